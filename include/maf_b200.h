@@ -1,0 +1,168 @@
+/*
+ * magnum.af B200 field / time-step library: C ABI.
+ *
+ * Drop-in boundary for magnum.af's effective-field and time-step hot path.
+ * Each entry point names the reference interface it replaces (paths relative
+ * to the magnum.af project root).  Conventions:
+ *   - every function returns an int status (MAF_OK on success); the message of
+ *     the last failure on the calling thread is returned by maf_last_error();
+ *   - vector fields are double [3][nz][ny][nx] (x fastest, component slowest),
+ *     the same bytes as ArrayFire's column-major [nx, ny, nz, 3] arrays that
+ *     the reference passes around; scalar fields are [nz][ny][nx];
+ *   - the library owns all device memory; one state = one CUDA stream (its own
+ *     unless maf_state_set_stream() installs the caller's); handles are not
+ *     thread-safe;
+ *   - the CUDA path is the only path: there is no CPU fallback, and without a
+ *     usable GPU every compute call fails with MAF_ERR_NODEVICE.
+ */
+#ifndef MAF_B200_H
+#define MAF_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct maf_state_s* maf_state;
+typedef struct maf_term_s* maf_term;
+typedef struct maf_llg_s* maf_llg;
+
+enum {
+    MAF_OK = 0,
+    MAF_ERR_BADARG = 1,      /* invalid argument / shape mismatch */
+    MAF_ERR_CUDA = 2,        /* CUDA runtime failure */
+    MAF_ERR_OOM = 3,         /* device allocation failed */
+    MAF_ERR_NAN = 4,         /* NaN/Inf detected in the RK error norm */
+    MAF_ERR_TIMEOUT = 5,     /* a bounded device wait gave up */
+    MAF_ERR_UNSUPPORTED = 6, /* e.g. an FFT length with a prime factor > 13 */
+    MAF_ERR_NODEVICE = 7     /* no CUDA device available */
+};
+
+enum {
+    MAF_FP64 = 0,      /* everything in FP64 (the reference's f64 path) */
+    MAF_FP32_FIELD = 1 /* field (demag FFT + stencils) in FP32; RK state, error norm, energies in FP64 */
+};
+
+/* Thread-local message of the last failure ("" when none). */
+const char* maf_last_error(void);
+/* Library version. */
+int maf_version(int* major, int* minor);
+/* Number of visible CUDA devices (0 without a GPU). */
+int maf_device_count(int* n);
+
+/* ---------------------------------------------------------------- State ---
+ * Replaces magnumaf::State(Mesh, double Ms, af::array m) and
+ * State(Mesh, af::array Ms_field, af::array m)
+ * (magnumaf/include/magnumaf/state.hpp:14-15, magnumaf/src/state.cpp:91-111).
+ * m is normalised on construction; with a scalar Ms and some |m| == 0 an
+ * Ms_field = Ms * (|m| != 0) is created (state.cpp:71-89).
+ * Ms_field_host may be NULL (scalar Ms). */
+int maf_state_create(maf_state* out, int nx, int ny, int nz, double dx, double dy, double dz, double Ms,
+                     const double* Ms_field_host, const double* m_host, int precision);
+int maf_state_destroy(maf_state s);
+/* copy m to the host: replaces State::m / get_m_addr (state.hpp:32, state.cpp:133) */
+int maf_state_get_m(maf_state s, double* m_host);
+/* State::set_m: normalises (state.cpp:131) */
+int maf_state_set_m(maf_state s, const double* m_host);
+int maf_state_get_t(maf_state s, double* t);
+int maf_state_set_t(maf_state s, double t);
+int maf_state_get_steps(maf_state s, unsigned long long* steps);
+/* State::mean_m (state.cpp:39-45): sum of m over cells / number of cells with |m| != 0 */
+int maf_state_mean_m(maf_state s, double out[3]);
+/* has_field = 1 and Ms_field copied to host (if non-NULL) when the state carries an Ms_field */
+int maf_state_get_Ms_field(maf_state s, double* Ms_field_host, int* has_field);
+int maf_state_get_Ms(maf_state s, double* Ms);
+/* Use the caller's cudaStream_t for all work on this state (NULL: back to the state's own stream). */
+int maf_state_set_stream(maf_state s, void* cuda_stream);
+/* Device pointer of m (double [3][N]); it changes after every accepted step. */
+int maf_state_device_m(maf_state s, void** m64_dev);
+int maf_state_precision(maf_state s, int* precision);
+
+/* ---------------------------------------------------------------- Terms ---
+ * Field terms; each replaces a FieldTerm subclass of
+ * magnumaf/include/magnumaf/field_terms/field_term.hpp:12-51 with its
+ * H_in_Apm(const State&) and Energy_in_J(const State&). */
+
+/* DemagField(Mesh mesh, ...) (magnumaf/src/field_terms/micro/demag_field.cpp:211-213):
+ * the Newell tensor is computed on the GPU in FP64 and transformed once. */
+int maf_term_demag_create(maf_term* out, int nx, int ny, int nz, double dx, double dy, double dz);
+/* ExchangeField(double A) (magnumaf/src/field_terms/micro/exchange_field.cpp:115-157) */
+int maf_term_exchange_create(maf_term* out, double A);
+/* DmiField(double D, std::array<double,3> D_axis) (magnumaf/src/field_terms/micro/dmi_field.cpp:15,41-110) */
+int maf_term_dmi_create(maf_term* out, double D, double axis_x, double axis_y, double axis_z);
+/* DmiField(af::array D_constants, D_axis) (dmi_field.cpp:17-19); D_field is [nz][ny][nx] */
+int maf_term_dmi_field_create(maf_term* out, int nx, int ny, int nz, const double* D_field_host, double axis_x,
+                              double axis_y, double axis_z);
+/* BulkDMIExchangeField(double D, double A) (magnumaf/src/field_terms/micro/bulk_dmi_exchange_field.cpp:9,95-119) */
+int maf_term_bulkdmi_exchange_create(maf_term* out, double D, double A);
+/* UniaxialAnisotropyField(double Ku1, std::array<double,3> axis)
+ * (magnumaf/src/field_terms/micro/uniaxial_anisotropy_field.cpp:11-12,58-89) */
+int maf_term_uniaxial_create(maf_term* out, double Ku1, double axis_x, double axis_y, double axis_z);
+/* UniaxialAnisotropyField with an Ku1 field and/or an axis field (uniaxial_anisotropy_field.cpp:14-31);
+ * Ku1_field [nz][ny][nx] or NULL (then Ku1 is used), axis_field [3][N] or NULL (then the axis is used) */
+int maf_term_uniaxial_field_create(maf_term* out, int nx, int ny, int nz, const double* Ku1_field_host, double Ku1,
+                                   const double* axis_field_host, double axis_x, double axis_y, double axis_z);
+/* CubicAnisotropyField(Kc1, Kc2, Kc3, c1, c2) (magnumaf/src/field_terms/micro/cubic_anisotropy_field.cpp:9-22,61-113);
+ * returns MAF_ERR_BADARG where the reference exits, i.e. when |c1.c2| > 1e-12 */
+int maf_term_cubic_create(maf_term* out, double Kc1, double Kc2, double Kc3, const double c1[3], const double c2[3]);
+/* ExternalField(af::array zee) (magnumaf/src/field_terms/micro/external_field.cpp:9,28-48); h is [3][N] */
+int maf_term_external_create(maf_term* out, int nx, int ny, int nz, const double* h_host);
+/* ExternalField with one field vector for every cell (set_homogeneous_field, external_field.cpp:19-25) */
+int maf_term_external_uniform_create(maf_term* out, double hx, double hy, double hz);
+int maf_term_destroy(maf_term t);
+/* FieldTerm::H_in_Apm (field_term.hpp:15,55-64); FP32-field states return their FP32 field widened */
+int maf_term_H(maf_term t, maf_state s, double* H_host);
+/* H_in_Apm of an FP32-field state in its native FP32 */
+int maf_term_H_f32(maf_term t, maf_state s, float* H_host);
+/* FieldTerm::Energy_in_J (field_term.hpp:19-20,66-86; micro_term.hpp:18-30) */
+int maf_term_E(maf_term t, maf_state s, double* E);
+/* DemagField only: the symmetry-reduced real spectral tensor, FP64,
+ * [ncomp][nz == 1 ? 1 : nz+1][ny+1][nx+1], ncomp = 6 (xx,xy,xz,yy,yz,zz) or 4 (xx,xy,yy,zz) when nz == 1 */
+int maf_term_demag_tensor(maf_term t, double* host);
+/* DemagField only: the real-space Newell tensor on the padded grid, [6][Pz][Py][Px]
+ * (replaces DemagField::calc_N, demag_field.cpp:207-209, in the x-fastest layout) */
+int maf_term_demag_real_tensor(maf_term t, double* host);
+
+/* ------------------------------------------------------------ Integrator ---
+ * LLGIntegrator(double alpha, vec_uptr_FieldTerm terms, std::string scheme = "RKF45",
+ *               Controller(hmin, hmax, atol, rtol), bool dissipation_term_only)
+ * (magnumaf/include/magnumaf/integrators/llg_integrator.hpp:28-44,
+ *  magnumaf/include/magnumaf/integrators/controller.hpp:16-17).
+ * scheme: "RKF45", "DP45" or "BS23".  alpha_field ([nz][ny][nx]) may be NULL.
+ * The integrator keeps its own reference to each term. */
+int maf_llg_create(maf_llg* out, double alpha, const double* alpha_field_host, int nx, int ny, int nz,
+                   const maf_term* terms, int nterms, const char* scheme, double hmin, double hmax, double atol,
+                   double rtol, int dissipation_term_only);
+int maf_llg_destroy(maf_llg l);
+/* Python add_terms() (python/magnumaf.pyx, LLGIntegrator.add_terms) */
+int maf_llg_add_term(maf_llg l, maf_term t);
+/* LLGIntegrator::alpha setter */
+int maf_llg_set_alpha(maf_llg l, double alpha);
+/* LLGIntegrator::step -> AdaptiveRungeKutta::step (adaptive_runge_kutta.cpp:39-71) */
+int maf_llg_step(maf_llg l, maf_state s);
+/* n consecutive steps */
+int maf_llg_steps(maf_llg l, maf_state s, int n);
+/* LLGIntegrator::E (llg_integrator.cpp:41) */
+int maf_llg_E(maf_llg l, maf_state s, double* E);
+/* Effective field of all terms (LLGIntegrator::h_addr / fheff, llg_integrator.cpp:11-16,112) */
+int maf_llg_heff(maf_llg l, maf_state s, double* H_host);
+int maf_llg_heff_f32(maf_llg l, maf_state s, float* H_host);
+/* Effective field from a device-resident m (float* for FP32-field states, double* for FP64 states)
+ * into a device-resident H of the same type, on the state's stream; no synchronisation. */
+int maf_llg_heff_device(maf_llg l, maf_state s, const void* m_dev, void* H_dev);
+/* dm/dt = LLGIntegrator::f(state) (llg_integrator.cpp:18-38) */
+int maf_llg_dmdt(maf_llg l, maf_state s, double* dmdt_host);
+/* LLGIntegrator::integrate_dense (llg_integrator.cpp:68-104): rows of (t, <mx>, <my>, <mz>),
+ * the first row being the initial state; at most max_rows rows are written. */
+int maf_llg_integrate_dense(maf_llg l, maf_state s, double time_in_s, double write_every_dt_in_s, double* rows,
+                            int max_rows, int* nrows);
+/* LLGIntegrator::relax (llg_integrator.cpp:43-66) */
+int maf_llg_relax(maf_llg l, maf_state s, double precision, int eval_E);
+/* current step size h and the controller counters {accepted, rejected, hmin, hmax}
+ * (controller.hpp:26-31) */
+int maf_llg_get_h(maf_llg l, double* h);
+int maf_llg_counters(maf_llg l, unsigned long long out[4]);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MAF_B200_H */

@@ -1,0 +1,964 @@
+// C ABI of the magnum.af B200 library (declared in include/maf_b200.h).
+#include <cmath>
+#include <cstring>
+#include <limits>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/maf_b200.h"
+#include "engine.hpp"
+#include "rk.hpp"
+
+using namespace mafb;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string& msg) {
+    g_last_error = msg;
+    return code;
+}
+
+template <typename F> int guarded(F&& f) {
+    try {
+        g_last_error.clear();
+        f();
+        return MAF_OK;
+    } catch (const Error& e) {
+        return fail(e.code, e.what());
+    } catch (const std::bad_alloc&) {
+        return fail(MAF_ERR_OOM, "host allocation failed");
+    } catch (const std::exception& e) {
+        return fail(MAF_ERR_CUDA, e.what());
+    }
+}
+
+void require_device() {
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n == 0) {
+        cudaGetLastError();
+        throw Error(MAF_ERR_NODEVICE, "no CUDA device available: the magnum.af B200 library has no CPU path");
+    }
+}
+
+void check(bool ok, const std::string& msg) {
+    if (!ok) throw Error(MAF_ERR_BADARG, msg);
+}
+
+// ---------------------------------------------------------------------------
+// Controller (magnumaf/include/magnumaf/integrators/controller.hpp:11-61,
+//             magnumaf/src/integrators/controller.cpp:36-95)
+// ---------------------------------------------------------------------------
+struct Controller {
+    double hmin = 1e-15, hmax = 3.5e-10, atol = 1e-6, rtol = 1e-6;
+    const double beta = 0.4 / 5.0;
+    const double alpha = 0.2 - 0.75 * beta;
+    const double headroom = 0.9;
+    const double minscale = 0.2;
+    const double maxscale = 10.;
+    bool reject = false;
+    double errold = 1.0e-4;
+    double hnext = 0.0;
+    unsigned long long n_reject = 0, n_accepted = 0, n_hmax = 0, n_hmin = 0;
+
+    bool success(double err, double& h) {
+        double scale;
+        if (err <= 1.0) {
+            if (err == 0.0) {
+                scale = maxscale;
+            } else {
+                scale = headroom * std::pow(err, -alpha) * std::pow(errold, beta);
+                if (scale < minscale) scale = minscale;
+                if (scale > maxscale) scale = maxscale;
+            }
+            hnext = reject ? h * std::min(scale, 1.0) : h * scale;
+            if (hnext <= hmin) {
+                hnext = hmin;
+                ++n_hmin;
+            } else if (hnext >= hmax) {
+                hnext = hmax;
+                ++n_hmax;
+            }
+            errold = std::max(err, 1.0e-4);
+            reject = false;
+            ++n_accepted;
+            return true;
+        }
+        scale = std::max(headroom * std::pow(err, -alpha), minscale);
+        h *= scale;
+        if (h <= hmin) {
+            h = hmin;
+            ++n_hmin;
+            return true;
+        }
+        if (h >= hmax) {
+            h = hmax;
+            ++n_hmax;
+            return true;
+        }
+        reject = true;
+        ++n_reject;
+        return false;
+    }
+};
+
+// Butcher tableaus (adaptive_runge_kutta.cpp:75-173, 496-529); coefficients
+// with dt_in_k == false are multiplied by dt at run time (BS23 keeps k = f).
+struct Scheme {
+    int stages = 0;
+    double a[8][8] = {};
+    double b[8] = {};
+    double e[8] = {};
+    int form = 0;  // 0: err = sum e_j k_j ; 1: err = sumbk - sum e_j k_j
+    bool dt_in_k = true;
+};
+
+Scheme make_scheme(const std::string& name) {
+    Scheme s;
+    if (name == "RKF45") {
+        s.stages = 6;
+        s.a[1][0] = 1. / 4.;
+        s.a[2][0] = 3. / 32.; s.a[2][1] = 9 / 32.;
+        s.a[3][0] = 1932. / 2197.; s.a[3][1] = -7200. / 2197.; s.a[3][2] = 7296. / 2197.;
+        s.a[4][0] = 439. / 216.; s.a[4][1] = -8.; s.a[4][2] = 3680. / 513.; s.a[4][3] = -845. / 4104.;
+        s.a[5][0] = -8. / 27.; s.a[5][1] = 2.; s.a[5][2] = -3544. / 2565.; s.a[5][3] = 1859. / 4104.;
+        s.a[5][4] = -11. / 40.;
+        const double b[6] = {16. / 135., 0, 6656. / 12825., 28561. / 56430., -9. / 50., 2. / 55.};
+        const double bh[6] = {25. / 216., 0, 1408. / 2565., 2197. / 4104., -1. / 5., 0};
+        for (int i = 0; i < 6; ++i) { s.b[i] = b[i]; s.e[i] = bh[i]; }
+        s.form = 1;
+    } else if (name == "DP45") {
+        s.stages = 7;
+        s.a[1][0] = 0.2;
+        s.a[2][0] = 3.0 / 40.0; s.a[2][1] = 9.0 / 40.0;
+        s.a[3][0] = 44.0 / 45.0; s.a[3][1] = -56.0 / 15.0; s.a[3][2] = 32.0 / 9.0;
+        s.a[4][0] = 19372.0 / 6561.0; s.a[4][1] = -25360.0 / 2187.0; s.a[4][2] = 64448.0 / 6561.0;
+        s.a[4][3] = -212.0 / 729.0;
+        s.a[5][0] = 9017.0 / 3168.0; s.a[5][1] = -355.0 / 33.0; s.a[5][2] = 46732.0 / 5247.0;
+        s.a[5][3] = 49.0 / 176.0; s.a[5][4] = -5103.0 / 18656.0;
+        s.a[6][0] = 35.0 / 384.0; s.a[6][2] = 500.0 / 1113.0; s.a[6][3] = 125.0 / 192.0;
+        s.a[6][4] = -2187.0 / 6784.0; s.a[6][5] = 11.0 / 84.0;
+        for (int j = 0; j < 6; ++j) s.b[j] = s.a[6][j];
+        const double e[7] = {71.0 / 57600.0, 0, -71.0 / 16695.0, 71.0 / 1920.0, -17253.0 / 339200.0, 22.0 / 525.0,
+                             -1.0 / 40.0};
+        for (int j = 0; j < 7; ++j) s.e[j] = e[j];
+        s.form = 0;
+    } else if (name == "BS23") {
+        s.stages = 4;
+        s.dt_in_k = false;
+        s.a[1][0] = 1. / 2.;
+        s.a[2][1] = 3. / 4.;
+        s.a[3][0] = 2. / 9.; s.a[3][1] = 1. / 3.; s.a[3][2] = 4. / 9.;
+        s.b[0] = 2. / 9.; s.b[1] = 1. / 3.; s.b[2] = 4. / 9.;
+        s.e[0] = 7. / 24.; s.e[1] = 1. / 4.; s.e[2] = 1. / 3.; s.e[3] = 1. / 8.;
+        s.form = 1;
+    } else {
+        throw Error(MAF_ERR_BADARG, "Integration method not found. Valid arguments are 'RKF45', 'DP45', 'BS23'");
+    }
+    return s;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// handle structs
+// ---------------------------------------------------------------------------
+struct maf_state_s {
+    StateD s;
+    DevBuf scratch;  // reductions
+    bool m32_valid = false;
+    ~maf_state_s() {
+        if (s.own_stream && s.stream) cudaStreamDestroy(s.stream);
+    }
+};
+
+struct maf_term_s {
+    std::shared_ptr<Term> t;
+};
+
+struct maf_llg_s {
+    double alpha = 0;
+    DevBuf alpha_field;
+    bool has_alpha_field = false;
+    int alpha_n = 0;
+    std::vector<std::shared_ptr<Term>> terms;
+    std::string scheme_name = "RKF45";
+    Scheme scheme;
+    Controller ctrl;
+    double h = 1.01e-15;
+    bool dissipation_only = false;
+    DevBuf k[8];
+    DevBuf mstage64, mstage32, mcand, partials, errbuf, h32out;
+    unsigned long long accumulated_steps = 0;
+};
+
+namespace {
+
+void ensure_m32(maf_state_s* st) {
+    StateD& s = st->s;
+    if (s.precision != PREC_FP32_FIELD) return;
+    s.m32.ensure(sizeof(float) * 3 * s.md.N());
+    if (!st->m32_valid) {
+        stage_m32(s.m64.as<double>(), s.m32.as<float>(), 3 * s.md.N(), s.stream);
+        st->m32_valid = true;
+    }
+}
+
+std::vector<Term*> raw_terms(const std::vector<std::shared_ptr<Term>>& v) {
+    std::vector<Term*> r;
+    for (auto& p : v) r.push_back(p.get());
+    return r;
+}
+
+// Field of `terms` on the state's current m with the given epilogue.
+void eval_on_state(maf_state_s* st, const std::vector<Term*>& terms, EpilogueArgs ep, double* energy = nullptr,
+                   const double* m64_for_llg = nullptr) {
+    StateD& s = st->s;
+    if (ep.kind == EPI_LLG && !ep.llg.m64) ep.llg.m64 = m64_for_llg ? m64_for_llg : s.m64.as<double>();
+    if (s.precision == PREC_FP32_FIELD) {
+        ensure_m32(st);
+        eval_terms<float>(terms, s.md, s.m32.as<float>(), s.msinfo(), ep, s.stream, st->scratch, energy);
+    } else {
+        eval_terms<double>(terms, s.md, s.m64.as<double>(), s.msinfo(), ep, s.stream, st->scratch, energy);
+    }
+}
+
+LLGParams llg_params(const maf_llg_s* l, double scale) {
+    LLGParams p;
+    const double a = l->alpha;
+    p.c_prec = -kGamma / (1. + a * a);
+    p.c_damp = -a * kGamma / (1. + a * a);
+    p.alpha = l->has_alpha_field ? l->alpha_field.as<double>() : nullptr;
+    p.dissipation_only = l->dissipation_only ? 1 : 0;
+    p.scale = scale;
+    return p;
+}
+
+// One RK attempt of `sch` with step dt; leaves m + sumbk (normalised per
+// norm_mode) in l->mcand and returns the error norm.
+double rk_attempt(maf_llg_s* l, maf_state_s* st, const Scheme& sch, double dt, int norm_mode) {
+    StateD& s = st->s;
+    const int64_t N = s.md.N();
+    const int64_t n3 = 3 * N;
+    const bool f32 = s.precision == PREC_FP32_FIELD;
+    for (int i = 0; i < sch.stages; ++i) l->k[i].ensure(sizeof(double) * n3);
+    l->mstage64.ensure(sizeof(double) * n3);
+    if (f32) l->mstage32.ensure(sizeof(float) * n3);
+    l->mcand.ensure(sizeof(double) * n3);
+    l->partials.ensure(sizeof(double) * 148 * 8 + 64);
+    l->errbuf.ensure(sizeof(double) * 4);
+    auto terms = raw_terms(l->terms);
+    const double kscale = sch.dt_in_k ? dt : 1.0;
+    const double cmul = sch.dt_in_k ? 1.0 : dt;
+    for (int stg = 0; stg < sch.stages; ++stg) {
+        EpilogueArgs ep;
+        ep.kind = EPI_LLG;
+        ep.out = l->k[stg].p;
+        ep.llg = llg_params(l, kscale);
+        if (stg == 0) {
+            ep.llg.m64 = s.m64.as<double>();
+            eval_on_state(st, terms, ep);
+        } else {
+            KList kl;
+            for (int j = 0; j < stg; ++j) {
+                if (sch.a[stg][j] == 0.0) continue;
+                kl.k[kl.n] = l->k[j].as<double>();
+                kl.c[kl.n] = sch.dt_in_k ? sch.a[stg][j] : dt * sch.a[stg][j];
+                ++kl.n;
+            }
+            rk_combine(s.m64.as<double>(), kl, l->mstage64.as<double>(), f32 ? l->mstage32.as<float>() : nullptr, n3,
+                       s.stream);
+            ep.llg.m64 = l->mstage64.as<double>();
+            if (f32)
+                eval_terms<float>(terms, s.md, l->mstage32.as<float>(), s.msinfo(), ep, s.stream, st->scratch, nullptr);
+            else
+                eval_terms<double>(terms, s.md, l->mstage64.as<double>(), s.msinfo(), ep, s.stream, st->scratch,
+                                   nullptr);
+        }
+    }
+    KList kb, ke;
+    for (int j = 0; j < sch.stages; ++j) {
+        if (sch.b[j] != 0.0) {
+            kb.k[kb.n] = l->k[j].as<double>();
+            kb.c[kb.n] = sch.b[j] * cmul;
+            ++kb.n;
+        }
+        if (sch.e[j] != 0.0) {
+            ke.k[ke.n] = l->k[j].as<double>();
+            ke.c[ke.n] = sch.e[j] * cmul;
+            ++ke.n;
+        }
+    }
+    rk_finalize(s.m64.as<double>(), kb, ke, sch.form, l->ctrl.atol, l->ctrl.rtol, l->mcand.as<double>(), norm_mode, N,
+                l->partials.as<double>(), l->errbuf.as<double>(), s.stream);
+    double err = 0;
+    MAF_CUDA(cudaMemcpyAsync(&err, l->errbuf.p, sizeof(double), cudaMemcpyDeviceToHost, s.stream));
+    MAF_CUDA(cudaStreamSynchronize(s.stream));
+    return err;
+}
+
+void accept_candidate(maf_llg_s* l, maf_state_s* st) {
+    std::swap(st->s.m64, l->mcand);
+    st->m32_valid = false;
+}
+
+void llg_step(maf_llg_s* l, maf_state_s* st) {
+    StateD& s = st->s;
+    const int norm_mode = s.has_Ms_field ? 2 : 1;
+    while (true) {
+        const double err = rk_attempt(l, st, l->scheme, l->h, norm_mode);
+        if (!(err == err) || std::isinf(err))
+            throw Error(MAF_ERR_NAN, "NaN/Inf in the Runge-Kutta error norm (t=" + std::to_string(s.t) + ")");
+        if (l->ctrl.success(err, l->h)) break;
+    }
+    s.t += l->h;
+    l->h = l->ctrl.hnext;
+    accept_candidate(l, st);
+    s.steps++;
+    l->accumulated_steps++;
+}
+
+void mean_m_host(maf_state_s* st, const double* m64, double out[3]) {
+    StateD& s = st->s;
+    st->scratch.ensure(sizeof(double) * (4 * 148 * 2 + 8));
+    double* scr = st->scratch.as<double>();
+    mean_m(m64, s.md.N(), scr, scr + 4 * 148 * 2, s.stream);
+    MAF_CUDA(cudaMemcpyAsync(out, scr + 4 * 148 * 2, 3 * sizeof(double), cudaMemcpyDeviceToHost, s.stream));
+    MAF_CUDA(cudaStreamSynchronize(s.stream));
+}
+
+double llg_energy(maf_llg_s* l, maf_state_s* st) {
+    EpilogueArgs ep;
+    ep.kind = EPI_EDENS;
+    double e = 0;
+    eval_on_state(st, raw_terms(l->terms), ep, &e);
+    return e;
+}
+
+void upload(DevBuf& b, const double* host, size_t n, cudaStream_t st) {
+    b.alloc(sizeof(double) * n);
+    MAF_CUDA(cudaMemcpyAsync(b.p, host, sizeof(double) * n, cudaMemcpyHostToDevice, st));
+    MAF_CUDA(cudaStreamSynchronize(st));
+}
+
+void H_to_host(maf_state_s* st, const std::vector<Term*>& terms, double* H_host, float* H32_host, DevBuf& tmp) {
+    StateD& s = st->s;
+    const int64_t n3 = 3 * s.md.N();
+    EpilogueArgs ep;
+    ep.kind = EPI_H;
+    if (s.precision == PREC_FP32_FIELD) {
+        // [float H32 | pad to 256 B | double H64]
+        const size_t off = (sizeof(float) * n3 + 255) / 256 * 256;
+        tmp.ensure(off + sizeof(double) * n3);
+        float* h32 = tmp.as<float>();
+        ep.out = h32;
+        eval_on_state(st, terms, ep);
+        if (H32_host) {
+            MAF_CUDA(cudaMemcpyAsync(H32_host, h32, sizeof(float) * n3, cudaMemcpyDeviceToHost, s.stream));
+        } else {
+            double* h64 = reinterpret_cast<double*>(static_cast<char*>(tmp.p) + off);
+            f32_to_f64(h32, h64, n3, s.stream);
+            MAF_CUDA(cudaMemcpyAsync(H_host, h64, sizeof(double) * n3, cudaMemcpyDeviceToHost, s.stream));
+        }
+    } else {
+        if (H32_host) throw Error(MAF_ERR_BADARG, "FP32 field output requested from an FP64 state");
+        tmp.ensure(sizeof(double) * n3);
+        ep.out = tmp.p;
+        eval_on_state(st, terms, ep);
+        MAF_CUDA(cudaMemcpyAsync(H_host, tmp.p, sizeof(double) * n3, cudaMemcpyDeviceToHost, s.stream));
+    }
+    MAF_CUDA(cudaStreamSynchronize(s.stream));
+}
+
+thread_local DevBuf g_tmp;  // host-copy staging for H outputs
+
+}  // namespace
+
+// ===========================================================================
+extern "C" {
+
+const char* maf_last_error(void) { return g_last_error.c_str(); }
+
+int maf_version(int* major, int* minor) {
+    if (major) *major = 0;
+    if (minor) *minor = 1;
+    return MAF_OK;
+}
+
+int maf_device_count(int* n) {
+    return guarded([&] {
+        int c = 0;
+        if (cudaGetDeviceCount(&c) != cudaSuccess) {
+            cudaGetLastError();
+            c = 0;
+        }
+        *n = c;
+    });
+}
+
+// ------------------------------------------------------------------ state
+int maf_state_create(maf_state* out, int nx, int ny, int nz, double dx, double dy, double dz, double Ms,
+                     const double* Ms_field_host, const double* m_host, int precision) {
+    return guarded([&] {
+        check(out && m_host, "maf_state_create: NULL argument");
+        check(nx > 0 && ny > 0 && nz > 0, "maf_state_create: mesh sizes must be positive");
+        check(precision == MAF_FP64 || precision == MAF_FP32_FIELD, "maf_state_create: bad precision");
+        require_device();
+        auto h = std::make_unique<maf_state_s>();
+        StateD& s = h->s;
+        s.md = MeshDims{nx, ny, nz, dx, dy, dz};
+        s.precision = precision;
+        MAF_CUDA(cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking));
+        s.own_stream = true;
+        const int64_t N = s.md.N();
+        upload(s.m64, m_host, 3 * N, s.stream);
+        // normalize (state.cpp:92) and count zero-norm cells
+        h->scratch.ensure(sizeof(unsigned long long) * 2);
+        MAF_CUDA(cudaMemsetAsync(h->scratch.p, 0, sizeof(unsigned long long), s.stream));
+        normalize_m(s.m64.as<double>(), N, 2, h->scratch.as<unsigned long long>(), s.stream);
+        unsigned long long zeros = 0;
+        MAF_CUDA(cudaMemcpyAsync(&zeros, h->scratch.p, sizeof(zeros), cudaMemcpyDeviceToHost, s.stream));
+        MAF_CUDA(cudaStreamSynchronize(s.stream));
+        if (Ms_field_host) {
+            s.Ms = std::numeric_limits<double>::quiet_NaN();
+            s.has_Ms_field = true;
+            upload(s.Msf64, Ms_field_host, N, s.stream);
+        } else {
+            s.Ms = Ms;
+            if (zeros > 0) {
+                s.has_Ms_field = true;
+                s.Msf64.alloc(sizeof(double) * N);
+            }
+        }
+        if (s.has_Ms_field) {
+            if (precision == PREC_FP32_FIELD) s.Msf32.alloc(sizeof(float) * N);
+            if (!Ms_field_host) {
+                ms_field_from_m(s.m64.as<double>(), Ms, s.Msf64.as<double>(),
+                                precision == PREC_FP32_FIELD ? s.Msf32.as<float>() : nullptr, N, s.stream);
+            } else if (precision == PREC_FP32_FIELD) {
+                stage_m32(s.Msf64.as<double>(), s.Msf32.as<float>(), N, s.stream);
+            }
+            MAF_CUDA(cudaStreamSynchronize(s.stream));
+        }
+        *out = h.release();
+    });
+}
+
+int maf_state_destroy(maf_state s) {
+    return guarded([&] { delete s; });
+}
+
+int maf_state_get_m(maf_state st, double* m_host) {
+    return guarded([&] {
+        check(st && m_host, "NULL argument");
+        StateD& s = st->s;
+        MAF_CUDA(cudaMemcpyAsync(m_host, s.m64.p, sizeof(double) * 3 * s.md.N(), cudaMemcpyDeviceToHost, s.stream));
+        MAF_CUDA(cudaStreamSynchronize(s.stream));
+    });
+}
+
+int maf_state_set_m(maf_state st, const double* m_host) {
+    return guarded([&] {
+        check(st && m_host, "NULL argument");
+        StateD& s = st->s;
+        MAF_CUDA(cudaMemcpyAsync(s.m64.p, m_host, sizeof(double) * 3 * s.md.N(), cudaMemcpyHostToDevice, s.stream));
+        normalize_m(s.m64.as<double>(), s.md.N(), 2, nullptr, s.stream);
+        st->m32_valid = false;
+    });
+}
+
+int maf_state_get_t(maf_state st, double* t) {
+    return guarded([&] { check(st && t, "NULL argument"); *t = st->s.t; });
+}
+int maf_state_set_t(maf_state st, double t) {
+    return guarded([&] { check(st, "NULL argument"); st->s.t = t; });
+}
+int maf_state_get_steps(maf_state st, unsigned long long* steps) {
+    return guarded([&] { check(st && steps, "NULL argument"); *steps = st->s.steps; });
+}
+int maf_state_mean_m(maf_state st, double out[3]) {
+    return guarded([&] {
+        check(st && out, "NULL argument");
+        mean_m_host(st, st->s.m64.as<double>(), out);
+    });
+}
+int maf_state_get_Ms_field(maf_state st, double* host, int* has_field) {
+    return guarded([&] {
+        check(st, "NULL argument");
+        if (has_field) *has_field = st->s.has_Ms_field ? 1 : 0;
+        if (host && st->s.has_Ms_field) {
+            MAF_CUDA(cudaMemcpyAsync(host, st->s.Msf64.p, sizeof(double) * st->s.md.N(), cudaMemcpyDeviceToHost,
+                                     st->s.stream));
+            MAF_CUDA(cudaStreamSynchronize(st->s.stream));
+        }
+    });
+}
+int maf_state_get_Ms(maf_state st, double* Ms) {
+    return guarded([&] { check(st && Ms, "NULL argument"); *Ms = st->s.Ms; });
+}
+int maf_state_set_stream(maf_state st, void* stream) {
+    return guarded([&] {
+        check(st, "NULL argument");
+        MAF_CUDA(cudaStreamSynchronize(st->s.stream));
+        if (stream) {
+            if (st->s.own_stream) cudaStreamDestroy(st->s.stream);
+            st->s.own_stream = false;
+            st->s.stream = static_cast<cudaStream_t>(stream);
+        } else if (!st->s.own_stream) {
+            MAF_CUDA(cudaStreamCreateWithFlags(&st->s.stream, cudaStreamNonBlocking));
+            st->s.own_stream = true;
+        }
+    });
+}
+int maf_state_device_m(maf_state st, void** p) {
+    return guarded([&] { check(st && p, "NULL argument"); *p = st->s.m64.p; });
+}
+int maf_state_precision(maf_state st, int* p) {
+    return guarded([&] { check(st && p, "NULL argument"); *p = st->s.precision; });
+}
+
+// ------------------------------------------------------------------ terms
+static maf_term new_term(std::shared_ptr<Term> t) {
+    auto* h = new maf_term_s;
+    h->t = std::move(t);
+    return h;
+}
+
+int maf_term_demag_create(maf_term* out, int nx, int ny, int nz, double dx, double dy, double dz) {
+    return guarded([&] {
+        check(out, "NULL argument");
+        check(nx > 0 && ny > 0 && nz > 0 && dx > 0 && dy > 0 && dz > 0, "DemagField: invalid mesh");
+        require_device();
+        auto t = std::make_shared<Term>();
+        t->kind = TK_DEMAG;
+        t->demag_mesh = MeshDims{nx, ny, nz, dx, dy, dz};
+        cudaStream_t st;
+        MAF_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        try {
+            t->demag = std::make_unique<Demag>(t->demag_mesh, st);
+        } catch (...) {
+            cudaStreamDestroy(st);
+            throw;
+        }
+        MAF_CUDA(cudaStreamSynchronize(st));
+        cudaStreamDestroy(st);
+        *out = new_term(t);
+    });
+}
+
+int maf_term_exchange_create(maf_term* out, double A) {
+    return guarded([&] {
+        check(out, "NULL argument");
+        auto t = std::make_shared<Term>();
+        t->kind = TK_EXCHANGE;
+        t->p[0] = A;
+        *out = new_term(t);
+    });
+}
+
+static void set_unit_axis(double* dst, double x, double y, double z, const char* who) {
+    const double n = std::sqrt(x * x + y * y + z * z);
+    check(n > 0, std::string(who) + ": zero axis");
+    dst[0] = x / n;
+    dst[1] = y / n;
+    dst[2] = z / n;
+}
+
+int maf_term_dmi_create(maf_term* out, double D, double ax, double ay, double az) {
+    return guarded([&] {
+        check(out, "NULL argument");
+        auto t = std::make_shared<Term>();
+        t->kind = TK_DMI;
+        t->p[0] = D;
+        // dmi_field.cpp:43-47: n = D_axis / |D_axis|
+        const double norm = std::sqrt(std::pow(ax, 2) + std::pow(ay, 2) + std::pow(az, 2));
+        check(norm > 0, "DmiField: zero axis");
+        t->p[1] = ax / norm;
+        t->p[2] = ay / norm;
+        t->p[3] = az / norm;
+        *out = new_term(t);
+    });
+}
+
+int maf_term_dmi_field_create(maf_term* out, int nx, int ny, int nz, const double* D_field, double ax, double ay,
+                              double az) {
+    return guarded([&] {
+        check(out && D_field, "NULL argument");
+        require_device();
+        auto t = std::make_shared<Term>();
+        t->kind = TK_DMI;
+        const double norm = std::sqrt(std::pow(ax, 2) + std::pow(ay, 2) + std::pow(az, 2));
+        check(norm > 0, "DmiField: zero axis");
+        t->p[1] = ax / norm;
+        t->p[2] = ay / norm;
+        t->p[3] = az / norm;
+        upload(t->f0, D_field, (size_t)nx * ny * nz, 0);
+        t->demag_mesh = MeshDims{nx, ny, nz, 0, 0, 0};
+        *out = new_term(t);
+    });
+}
+
+int maf_term_bulkdmi_exchange_create(maf_term* out, double D, double A) {
+    return guarded([&] {
+        check(out, "NULL argument");
+        auto t = std::make_shared<Term>();
+        t->kind = TK_BULKDMI;
+        t->p[0] = D;
+        t->p[1] = A;
+        *out = new_term(t);
+    });
+}
+
+int maf_term_uniaxial_create(maf_term* out, double Ku1, double ax, double ay, double az) {
+    return guarded([&] {
+        check(out, "NULL argument");
+        auto t = std::make_shared<Term>();
+        t->kind = TK_UNIAXIAL;
+        t->p[0] = Ku1;
+        set_unit_axis(t->p + 1, ax, ay, az, "UniaxialAnisotropyField");  // util::normalize_vector
+        *out = new_term(t);
+    });
+}
+
+int maf_term_uniaxial_field_create(maf_term* out, int nx, int ny, int nz, const double* Ku1_field, double Ku1,
+                                   const double* axis_field, double ax, double ay, double az) {
+    return guarded([&] {
+        check(out, "NULL argument");
+        require_device();
+        auto t = std::make_shared<Term>();
+        t->kind = TK_UNIAXIAL;
+        t->p[0] = Ku1;
+        const size_t N = (size_t)nx * ny * nz;
+        if (Ku1_field) upload(t->f0, Ku1_field, N, 0);
+        if (axis_field) {
+            // util::normalize on the axis field (uniaxial_anisotropy_field.cpp:24)
+            upload(t->f1, axis_field, 3 * N, 0);
+            normalize_m(t->f1.as<double>(), (int64_t)N, 2, nullptr, 0);
+            MAF_CUDA(cudaDeviceSynchronize());
+        } else {
+            set_unit_axis(t->p + 1, ax, ay, az, "UniaxialAnisotropyField");
+        }
+        *out = new_term(t);
+    });
+}
+
+int maf_term_cubic_create(maf_term* out, double Kc1, double Kc2, double Kc3, const double c1[3], const double c2[3]) {
+    return guarded([&] {
+        check(out && c1 && c2, "NULL argument");
+        auto t = std::make_shared<Term>();
+        t->kind = TK_CUBIC;
+        t->p[0] = Kc1;
+        t->p[1] = Kc2;
+        t->p[2] = Kc3;
+        double a[3], b[3];
+        set_unit_axis(a, c1[0], c1[1], c1[2], "CubicAnisotropyField c1");
+        set_unit_axis(b, c2[0], c2[1], c2[2], "CubicAnisotropyField c2");
+        const double dot = std::fabs(a[0] * b[0] + a[1] * b[1] + a[2] * b[2]);
+        check(dot <= 1e-12, "CubicAnisotropyField: provided c1 and c2 are not perpendicular, |c1.c2| = " +
+                                std::to_string(dot));
+        // c3 = normalize(c1 x c2), cross product of the given (unnormalised) axes
+        const double cx = c1[1] * c2[2] - c1[2] * c2[1];
+        const double cy = c1[2] * c2[0] - c1[0] * c2[2];
+        const double cz = c1[0] * c2[1] - c1[1] * c2[0];
+        double c[3];
+        set_unit_axis(c, cx, cy, cz, "CubicAnisotropyField c3");
+        for (int i = 0; i < 3; ++i) {
+            t->p[3 + i] = a[i];
+            t->p[6 + i] = b[i];
+            t->p[9 + i] = c[i];
+        }
+        *out = new_term(t);
+    });
+}
+
+int maf_term_external_create(maf_term* out, int nx, int ny, int nz, const double* h_host) {
+    return guarded([&] {
+        check(out && h_host, "NULL argument");
+        const size_t N = (size_t)nx * ny * nz;
+        auto t = std::make_shared<Term>();
+        t->kind = TK_ZEEMAN;
+        // a field that is the same in every cell is kept as one vector
+        bool uniform = true;
+        for (int c = 0; c < 3 && uniform; ++c)
+            for (size_t i = 1; i < N; ++i)
+                if (h_host[c * N + i] != h_host[c * N]) { uniform = false; break; }
+        if (uniform) {
+            t->p[0] = h_host[0];
+            t->p[1] = h_host[N];
+            t->p[2] = h_host[2 * N];
+        } else {
+            require_device();
+            upload(t->f0, h_host, 3 * N, 0);
+        }
+        t->demag_mesh = MeshDims{nx, ny, nz, 0, 0, 0};
+        *out = new_term(t);
+    });
+}
+
+int maf_term_external_uniform_create(maf_term* out, double hx, double hy, double hz) {
+    return guarded([&] {
+        check(out, "NULL argument");
+        auto t = std::make_shared<Term>();
+        t->kind = TK_ZEEMAN;
+        t->p[0] = hx;
+        t->p[1] = hy;
+        t->p[2] = hz;
+        *out = new_term(t);
+    });
+}
+
+int maf_term_destroy(maf_term t) {
+    return guarded([&] { delete t; });
+}
+
+static void check_term_state(maf_term t, maf_state s) {
+    check(t && s, "NULL argument");
+    if (t->t->f0.p || t->t->f1.p) {
+        check(t->t->demag_mesh.N() == s->s.md.N() || t->t->demag_mesh.N() == 0,
+              "field-term parameter array does not match the state's mesh");
+    }
+}
+
+int maf_term_H(maf_term t, maf_state s, double* H) {
+    return guarded([&] {
+        check_term_state(t, s);
+        check(H, "NULL argument");
+        H_to_host(s, {t->t.get()}, H, nullptr, g_tmp);
+    });
+}
+
+int maf_term_H_f32(maf_term t, maf_state s, float* H) {
+    return guarded([&] {
+        check_term_state(t, s);
+        check(H, "NULL argument");
+        H_to_host(s, {t->t.get()}, nullptr, H, g_tmp);
+    });
+}
+
+int maf_term_E(maf_term t, maf_state s, double* E) {
+    return guarded([&] {
+        check_term_state(t, s);
+        check(E, "NULL argument");
+        EpilogueArgs ep;
+        ep.kind = EPI_EDENS;
+        eval_on_state(s, {t->t.get()}, ep, E);
+    });
+}
+
+int maf_term_demag_tensor(maf_term t, double* host) {
+    return guarded([&] {
+        check(t && host && t->t->kind == TK_DEMAG, "maf_term_demag_tensor: not a DemagField");
+        t->t->demag->download_tensor(host, 0);
+    });
+}
+
+int maf_term_demag_real_tensor(maf_term t, double* host) {
+    return guarded([&] {
+        check(t && host && t->t->kind == TK_DEMAG, "maf_term_demag_real_tensor: not a DemagField");
+        t->t->demag->download_real_tensor(host, 0);
+    });
+}
+
+// ------------------------------------------------------------------ LLG
+int maf_llg_create(maf_llg* out, double alpha, const double* alpha_field, int nx, int ny, int nz, const maf_term* terms,
+                   int nterms, const char* scheme, double hmin, double hmax, double atol, double rtol,
+                   int dissipation_term_only) {
+    return guarded([&] {
+        check(out, "NULL argument");
+        check(nterms >= 0 && (nterms == 0 || terms), "maf_llg_create: bad term list");
+        auto l = std::make_unique<maf_llg_s>();
+        l->alpha = alpha;
+        if (alpha_field) {
+            require_device();
+            upload(l->alpha_field, alpha_field, (size_t)nx * ny * nz, 0);
+            l->has_alpha_field = true;
+            l->alpha_n = nx * ny * nz;
+        }
+        for (int i = 0; i < nterms; ++i) {
+            check(terms[i] != nullptr, "maf_llg_create: NULL term");
+            l->terms.push_back(terms[i]->t);
+        }
+        l->scheme_name = scheme ? scheme : "RKF45";
+        l->scheme = make_scheme(l->scheme_name);
+        l->ctrl.hmin = hmin;
+        l->ctrl.hmax = hmax;
+        l->ctrl.atol = atol;
+        l->ctrl.rtol = rtol;
+        l->dissipation_only = dissipation_term_only != 0;
+        *out = l.release();
+    });
+}
+
+int maf_llg_destroy(maf_llg l) {
+    return guarded([&] { delete l; });
+}
+
+int maf_llg_add_term(maf_llg l, maf_term t) {
+    return guarded([&] {
+        check(l && t, "NULL argument");
+        l->terms.push_back(t->t);
+    });
+}
+
+int maf_llg_set_alpha(maf_llg l, double alpha) {
+    return guarded([&] {
+        check(l, "NULL argument");
+        l->alpha = alpha;
+    });
+}
+
+static void check_llg_state(maf_llg l, maf_state s) {
+    check(l && s, "NULL argument");
+    check(!l->terms.empty(), "LLGIntegrator: no field terms");
+    if (l->has_alpha_field) check(l->alpha_n == s->s.md.N(), "alpha field does not match the state's mesh");
+}
+
+int maf_llg_step(maf_llg l, maf_state s) {
+    return guarded([&] {
+        check_llg_state(l, s);
+        llg_step(l, s);
+    });
+}
+
+int maf_llg_steps(maf_llg l, maf_state s, int n) {
+    return guarded([&] {
+        check_llg_state(l, s);
+        for (int i = 0; i < n; ++i) llg_step(l, s);
+    });
+}
+
+int maf_llg_E(maf_llg l, maf_state s, double* E) {
+    return guarded([&] {
+        check_llg_state(l, s);
+        check(E, "NULL argument");
+        *E = llg_energy(l, s);
+    });
+}
+
+int maf_llg_heff(maf_llg l, maf_state s, double* H) {
+    return guarded([&] {
+        check_llg_state(l, s);
+        check(H, "NULL argument");
+        H_to_host(s, raw_terms(l->terms), H, nullptr, g_tmp);
+    });
+}
+
+int maf_llg_heff_f32(maf_llg l, maf_state s, float* H) {
+    return guarded([&] {
+        check_llg_state(l, s);
+        check(H, "NULL argument");
+        H_to_host(s, raw_terms(l->terms), nullptr, H, g_tmp);
+    });
+}
+
+int maf_llg_heff_device(maf_llg l, maf_state s, const void* m_dev, void* H_dev) {
+    return guarded([&] {
+        check_llg_state(l, s);
+        check(m_dev && H_dev, "NULL argument");
+        EpilogueArgs ep;
+        ep.kind = EPI_H;
+        ep.out = H_dev;
+        StateD& st = s->s;
+        if (st.precision == PREC_FP32_FIELD)
+            eval_terms<float>(raw_terms(l->terms), st.md, static_cast<const float*>(m_dev), st.msinfo(), ep, st.stream,
+                              s->scratch, nullptr);
+        else
+            eval_terms<double>(raw_terms(l->terms), st.md, static_cast<const double*>(m_dev), st.msinfo(), ep,
+                               st.stream, s->scratch, nullptr);
+    });
+}
+
+int maf_llg_dmdt(maf_llg l, maf_state s, double* out) {
+    return guarded([&] {
+        check_llg_state(l, s);
+        check(out, "NULL argument");
+        const int64_t n3 = 3 * s->s.md.N();
+        l->k[0].ensure(sizeof(double) * n3);
+        EpilogueArgs ep;
+        ep.kind = EPI_LLG;
+        ep.out = l->k[0].p;
+        ep.llg = llg_params(l, 1.0);
+        eval_on_state(s, raw_terms(l->terms), ep);
+        MAF_CUDA(cudaMemcpyAsync(out, l->k[0].p, sizeof(double) * n3, cudaMemcpyDeviceToHost, s->s.stream));
+        MAF_CUDA(cudaStreamSynchronize(s->s.stream));
+    });
+}
+
+int maf_llg_integrate_dense(maf_llg l, maf_state s, double time_in_s, double write_every_dt_in_s, double* rows,
+                            int max_rows, int* nrows) {
+    return guarded([&] {
+        check_llg_state(l, s);
+        check(rows && nrows && max_rows > 0, "NULL argument");
+        check(write_every_dt_in_s > 0, "integrate_dense: write_every_dt_in_s must be > 0");
+        StateD& st = s->s;
+        int n = 0;
+        auto push = [&](double t, const double mm[3]) {
+            if (n < max_rows) {
+                rows[4 * n + 0] = t;
+                rows[4 * n + 1] = mm[0];
+                rows[4 * n + 2] = mm[1];
+                rows[4 * n + 3] = mm[2];
+                ++n;
+            }
+        };
+        double mm[3];
+        mean_m_host(s, st.m64.as<double>(), mm);
+        push(st.t, mm);
+        const Scheme rkf = make_scheme("RKF45");
+        const double time_init = st.t;
+        const double time_final = time_init + time_in_s;
+        double t_next = time_init + write_every_dt_in_s;
+        while (st.t < time_final) {
+            llg_step(l, s);
+            if (st.t >= t_next) {
+                const double backstep = t_next - st.t;  // negative
+                // RKF45 back-step from the overshooting state, no normalisation (llg_integrator.cpp:79-94)
+                rk_attempt(l, s, rkf, backstep, 0);
+                if (t_next >= time_final - 1e-20) {
+                    accept_candidate(l, s);
+                    st.t += backstep;
+                    mean_m_host(s, st.m64.as<double>(), mm);
+                    push(st.t, mm);
+                    break;
+                }
+                mean_m_host(s, l->mcand.as<double>(), mm);
+                push(st.t + backstep, mm);
+                t_next += write_every_dt_in_s;
+                while (t_next < st.t) t_next += write_every_dt_in_s;
+            }
+        }
+        *nrows = n;
+    });
+}
+
+int maf_llg_relax(maf_llg l, maf_state s, double precision, int eval_E) {
+    return guarded([&] {
+        check_llg_state(l, s);
+        double E_prev = 1e20;
+        double E = llg_energy(l, s);
+        while (std::fabs((E_prev - E) / E_prev) > precision) {
+            E_prev = E;
+            for (int i = 0; i < eval_E; ++i) llg_step(l, s);
+            E = llg_energy(l, s);
+        }
+    });
+}
+
+int maf_llg_get_h(maf_llg l, double* h) {
+    return guarded([&] { check(l && h, "NULL argument"); *h = l->h; });
+}
+
+int maf_llg_counters(maf_llg l, unsigned long long out[4]) {
+    return guarded([&] {
+        check(l && out, "NULL argument");
+        out[0] = l->ctrl.n_accepted;
+        out[1] = l->ctrl.n_reject;
+        out[2] = l->ctrl.n_hmin;
+        out[3] = l->ctrl.n_hmax;
+    });
+}
+
+}  // extern "C"

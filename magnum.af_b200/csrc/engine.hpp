@@ -1,0 +1,178 @@
+// Host-side engine objects behind the C ABI: device buffers, the demag plan,
+// the field evaluator and the adaptive Runge-Kutta integrator.
+#pragma once
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+#include "fft_engine.cuh"
+#include "local_terms.cuh"
+
+namespace mafb {
+
+enum Precision : int { PREC_FP64 = 0, PREC_FP32_FIELD = 1 };
+
+// Owning device allocation.
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    DevBuf() = default;
+    explicit DevBuf(size_t n) { alloc(n); }
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    DevBuf(DevBuf&& o) noexcept : p(o.p), bytes(o.bytes) { o.p = nullptr; o.bytes = 0; }
+    DevBuf& operator=(DevBuf&& o) noexcept {
+        if (this != &o) { release(); p = o.p; bytes = o.bytes; o.p = nullptr; o.bytes = 0; }
+        return *this;
+    }
+    ~DevBuf() { release(); }
+    void alloc(size_t n) {
+        release();
+        if (n) MAF_CUDA(cudaMalloc(&p, n));
+        bytes = n;
+    }
+    void ensure(size_t n) { if (bytes < n) alloc(n); }
+    void release() { if (p) cudaFree(p); p = nullptr; bytes = 0; }
+    template <typename T> T* as() const { return static_cast<T*>(p); }
+};
+
+struct MeshDims {
+    int nx = 0, ny = 0, nz = 0;
+    double dx = 0, dy = 0, dz = 0;
+    int64_t N() const { return (int64_t)nx * ny * nz; }
+    Geom geom() const { return Geom{nx, ny, nz, N(), dx, dy, dz}; }
+    bool operator==(const MeshDims& o) const {
+        return nx == o.nx && ny == o.ny && nz == o.nz && dx == o.dx && dy == o.dy && dz == o.dz;
+    }
+};
+
+// Twiddle tables W_L^k, k in [0, L), per length and precision.
+class Twiddles {
+  public:
+    const void* get(int L, bool fp64);
+  private:
+    std::map<std::pair<int, int>, DevBuf> tables_;
+};
+
+FFTPlan make_fft_plan(int L, const void* tw);  // throws MAF_ERR_UNSUPPORTED for primes > 13
+
+// Output handling of the last field pass.
+enum Epilogue : int {
+    EPI_H = 0,      // write H (precision R) to out[3][N]
+    EPI_LLG = 1,    // write k = scale * dm/dt (double) to out[3][N]
+    EPI_EDENS = 2,  // accumulate the energy of the term list (double partial sums per CTA)
+};
+
+struct LLGParams {
+    double c_prec = 0;             // -gamma/(1+alpha^2)
+    double c_damp = 0;             // -alpha*gamma/(1+alpha^2)
+    const double* alpha = nullptr; // optional alpha field [N]
+    int dissipation_only = 0;
+    double scale = 1.0;            // dt (RKF45/DP45) or 1 (BS23)
+    const double* m64 = nullptr;   // state m in FP64 for the cross products
+};
+
+struct EpilogueArgs {
+    int kind = EPI_H;
+    void* out = nullptr;           // H (R) or k (double)
+    double* partials = nullptr;    // EPI_EDENS: one double per CTA
+    LLGParams llg;
+    int edge_exchange = 1;         // EPI_EDENS: exchange energy uses h_withedges
+};
+
+struct MsInfo {
+    double Ms = 0;                 // scalar Ms (used when field == nullptr)
+    const double* field64 = nullptr;
+    const float* field32 = nullptr;
+};
+
+// Demag plan: the symmetry-reduced real spectral Newell tensor and the
+// spectral work buffers for one mesh.
+class Demag {
+  public:
+    explicit Demag(const MeshDims& md, cudaStream_t st);
+    const MeshDims& mesh() const { return md_; }
+    int Px() const { return 2 * md_.nx; }
+    int Py() const { return 2 * md_.ny; }
+    int Pz() const { return md_.nz == 1 ? 1 : 2 * md_.nz; }
+    int nxh() const { return md_.nx + 1; }
+    int ncomp() const { return md_.nz == 1 ? 4 : 6; }
+    // Passes 1..4: spectral convolution of Ms*m, result left in the half-spectrum
+    // buffer for the fused x-inverse epilogue.
+    template <typename R> void forward_conv(const R* m, const MsInfo& ms, cudaStream_t st);
+    // Pass 5: x-inverse + local terms + epilogue (called by the field evaluator).
+    template <typename R>
+    void inverse_x_epilogue(const R* m, const MsInfo& ms, const TermList& tl, const EpilogueArgs& ep,
+                            cudaStream_t st, int* nblocks_out);
+    // reduced real spectral tensor in FP64 [ncomp][kz][ky][kx] (host copy for tests)
+    void download_tensor(double* host, cudaStream_t st) const;
+    void download_real_tensor(double* host, cudaStream_t st);  // [6][Pz][Py][Px]
+    size_t tensor_elems() const { return (size_t)ncomp() * (md_.nz == 1 ? 1 : md_.nz + 1) * (md_.ny + 1) * nxh(); }
+    int pitch() const { return pitch_; }
+    template <typename R> int edens_blocks() const;
+
+  private:
+    template <typename R> const R* tensor() ;
+    template <typename R> cplx_t<R>* S1();
+    template <typename R> cplx_t<R>* S2();
+    void build_tensor(cudaStream_t st);
+
+    MeshDims md_;
+    int pitch_;  // complex row pitch of the half spectrum (>= nx+1)
+    DevBuf Nred64_, Nred32_;
+    DevBuf S1_64_, S2_64_, S1_32_, S2_32_;
+    Twiddles tw_;
+};
+
+// Field-term objects (the C ABI's maf_term).
+struct Term {
+    int kind = TK_DEMAG;
+    double p[12] = {};
+    DevBuf f0, f1;                   // optional parameter fields (FP64)
+    std::unique_ptr<Demag> demag;    // TK_DEMAG
+    MeshDims demag_mesh;
+    TermDesc desc() const {
+        TermDesc d;
+        d.kind = kind;
+        for (int i = 0; i < 12; ++i) d.p[i] = p[i];
+        d.f0 = f0.p ? f0.as<double>() : nullptr;
+        d.f1 = f1.p ? f1.as<double>() : nullptr;
+        return d;
+    }
+};
+
+// Device-resident State.
+struct StateD {
+    MeshDims md;
+    int precision = PREC_FP64;
+    double Ms = 0;
+    bool has_Ms_field = false;
+    DevBuf m64;        // double [3][N]
+    DevBuf m32;        // float  [3][N] staged copy (FP32-field form)
+    DevBuf Msf64, Msf32;
+    double t = 0;
+    unsigned long long steps = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    MsInfo msinfo() const {
+        MsInfo mi;
+        mi.Ms = Ms;
+        if (has_Ms_field) { mi.field64 = Msf64.as<double>(); mi.field32 = Msf32.as<float>(); }
+        return mi;
+    }
+};
+
+// Field evaluation of a list of terms on m (precision R), with one epilogue.
+template <typename R>
+void eval_terms(const std::vector<Term*>& terms, const MeshDims& md, const R* m, const MsInfo& ms,
+                const EpilogueArgs& ep, cudaStream_t st, DevBuf& scratch_partials, double* energy_out);
+
+// FP64 -> FP32 staging of m
+void stage_m32(const double* m64, float* m32, int64_t n, cudaStream_t st);
+
+// Newell tensor on the padded grid, one component [Pz][Py][Px] (newell.cu).
+void newell_component(double* out, int comp, const MeshDims& md, int Px, int Py, int Pz, cudaStream_t st);
+
+}  // namespace mafb

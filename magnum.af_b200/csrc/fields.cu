@@ -1,0 +1,821 @@
+// Effective-field kernels: the zero-padded demag FFT convolution in five (3-D)
+// or three (nz == 1) passes, with the local terms and the chosen epilogue
+// fused into the last pass.
+//
+// Reference: magnumaf/src/field_terms/micro/demag_field.cpp:215-264
+//   H = IFFT( N^ . FFT(pad(Ms m)) ) / (Px Py Pz), truncated to the mesh,
+// with P = (2nx, 2ny, nz == 1 ? 1 : 2nz) and the tensor of demag_field.cpp:104-147.
+//
+// HBM layout (x fastest everywhere):
+//   m, H            [3][nz][ny][nx]            real (FP32 or FP64)
+//   S1 half spectrum [3][nz][ny][pitch]         complex, kx in [0, nx]
+//   S2               [3][nz][Py][pitch]         complex (3-D meshes only)
+//   tensor (reduced) [ncomp][nz+1 or 1][ny+1][nx+1] real: the spectral Newell
+//                    tensor is real and even/odd in ky and kz, so only the
+//                    quadrant ky <= ny, kz <= nz is stored (6 components; 4
+//                    when nz == 1 because Nxz = Nyz = 0 in a single layer).
+//
+// Passes (3-D): x-fwd R2C (zero pad fused into the load) -> y-fwd (pad fused)
+//   -> z-fwd . tensor . z-inv (in place, truncation fused) -> y-inv (truncation
+//   fused into the store) -> x-inv C2R + local terms + epilogue.
+// Passes (nz == 1): x-fwd -> y-fwd . tensor . y-inv (in place) -> x-inv + epilogue.
+#include <algorithm>
+#include <cmath>
+
+#include "engine.hpp"
+
+namespace mafb {
+
+// ---------------------------------------------------------------------------
+// twiddles and plans
+// ---------------------------------------------------------------------------
+const void* Twiddles::get(int L, bool fp64) {
+    auto key = std::make_pair(L, fp64 ? 1 : 0);
+    auto it = tables_.find(key);
+    if (it != tables_.end()) return it->second.p;
+    // W_L^k = exp(-2 pi i k / L) in long double, reduced to the first octant
+    // so that the table is symmetric to the last bit.
+    std::vector<long double> c(L), s(L);
+    const long double pi = 3.141592653589793238462643383279502884L;
+    for (int k = 0; k < L; ++k) {
+        // angle = 2 pi k / L; use k/L in [0,1)
+        long double a = 2.0L * pi * (long double)k / (long double)L;
+        // symmetric evaluation about the quarter points
+        int64_t k4 = 4 * (int64_t)k;
+        long double cv, sv;
+        if (k4 == 0) { cv = 1; sv = 0; }
+        else if (k4 == L) { cv = 0; sv = 1; }
+        else if (k4 == 2 * (int64_t)L) { cv = -1; sv = 0; }
+        else if (k4 == 3 * (int64_t)L) { cv = 0; sv = -1; }
+        else { cv = cosl(a); sv = sinl(a); }
+        c[k] = cv;
+        s[k] = -sv;  // exp(-i a)
+    }
+    DevBuf buf;
+    if (fp64) {
+        std::vector<double2> h(L);
+        for (int k = 0; k < L; ++k) h[k] = make_double2((double)c[k], (double)s[k]);
+        buf.alloc(sizeof(double2) * L);
+        MAF_CUDA(cudaMemcpy(buf.p, h.data(), sizeof(double2) * L, cudaMemcpyHostToDevice));
+    } else {
+        std::vector<float2> h(L);
+        for (int k = 0; k < L; ++k) h[k] = make_float2((float)c[k], (float)s[k]);
+        buf.alloc(sizeof(float2) * L);
+        MAF_CUDA(cudaMemcpy(buf.p, h.data(), sizeof(float2) * L, cudaMemcpyHostToDevice));
+    }
+    const void* p = buf.p;
+    tables_.emplace(key, std::move(buf));
+    return p;
+}
+
+FFTPlan make_fft_plan(int L, const void* tw) {
+    FFTPlan p;
+    p.L = L;
+    p.tw = tw;
+    int n = L;
+    auto push = [&](int r) {
+        if (p.nstages >= kMaxStages) throw Error(6, "FFT plan: too many stages");
+        p.radix[p.nstages++] = r;
+    };
+    while (n % 8 == 0) { push(8); n /= 8; }
+    if (n % 4 == 0) { push(4); n /= 4; }
+    if (n % 2 == 0) { push(2); n /= 2; }
+    for (int r : {3, 5, 7, 11, 13}) {
+        while (n % r == 0) { push(r); n /= r; }
+    }
+    if (n != 1)
+        throw Error(6, "FFT length " + std::to_string(L) +
+                           " has a prime factor > 13; choose mesh sizes whose doubled sizes factor into 2,3,5,7,11,13");
+    return p;
+}
+
+// ---------------------------------------------------------------------------
+// pass kernels
+// ---------------------------------------------------------------------------
+// x-forward: rows of n_in reals (times Ms) zero-padded to Px = 2*Lc, real FFT by
+// packing even/odd samples into Lc complex values; writes kx in [0, Lc].
+template <typename R>
+__global__ void __launch_bounds__(kMaxFftThreads) k_xfwd(const R* __restrict__ in, int n_in, int64_t rows, int64_t rows_pc,
+                                               const R* __restrict__ msf, R ms, cplx_t<R>* __restrict__ out, int pitch,
+                                               FFTPlan plan, const cplx_t<R>* __restrict__ twP, int nb) {
+    using C = cplx_t<R>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C* s = reinterpret_cast<C*>(smem_raw);
+    const int Lc = plan.L;
+    const SLay<false> lay{nb, spad_len(Lc)};
+    const int64_t r0 = (int64_t)blockIdx.x * nb;
+    for (int idx = threadIdx.x; idx < nb * Lc; idx += blockDim.x) {
+        const int b = idx / Lc;
+        const int k = idx - b * Lc;
+        const int64_t row = r0 + b;
+        R a = 0, c = 0;
+        if (row < rows) {
+            const R* rp = in + row * n_in;
+            const int x0 = 2 * k, x1 = 2 * k + 1;
+            if (msf) {
+                const R* mp = msf + (row % rows_pc) * n_in;
+                if (x0 < n_in) a = mp[x0] * rp[x0];
+                if (x1 < n_in) c = mp[x1] * rp[x1];
+            } else {
+                if (x0 < n_in) a = ms * rp[x0];
+                if (x1 < n_in) c = ms * rp[x1];
+            }
+        }
+        s[lay.at(k, b)] = mk(a, c);
+    }
+    __syncthreads();
+    run_fft<R, -1, false>(s, lay, plan);
+    const R half = (R)0.5;
+    for (int idx = threadIdx.x; idx < nb * (Lc + 1); idx += blockDim.x) {
+        const int b = idx / (Lc + 1);
+        const int k = idx - b * (Lc + 1);
+        const int64_t row = r0 + b;
+        if (row >= rows) continue;
+        const C Zk = s[lay.at(k == Lc ? 0 : k, b)];
+        const C Zm = s[lay.at(k == 0 ? 0 : Lc - k, b)];
+        const C E = cscale(cadd(Zk, cconj(Zm)), half);
+        const C O = cscale(cmul_i<-1>(csub(Zk, cconj(Zm))), half);
+        const C w = twP[k];  // W_Px^k, k <= Lc < Px
+        out[row * pitch + k] = cadd(E, cmul(w, O));
+    }
+}
+
+// Strided batched column FFT: element i of column c of batch b at
+// base + b*sbat + i*si + c.  Loads n_in values (zero pad to L), stores n_out.
+template <typename R, int DIR>
+__global__ void __launch_bounds__(kMaxFftThreads) k_fft_cols(const cplx_t<R>* in, cplx_t<R>* out, FFTPlan plan, int n_in,
+                                                   int n_out, int ncols, int64_t in_si, int64_t out_si, int64_t in_sbat,
+                                                   int64_t out_sbat, int nb) {
+    using C = cplx_t<R>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C* s = reinterpret_cast<C*>(smem_raw);
+    const int L = plan.L;
+    const SLay<true> lay{nb, 0};
+    const int c0 = blockIdx.x * nb;
+    const C* ib = in + (int64_t)blockIdx.y * in_sbat + c0;
+    C* ob = out + (int64_t)blockIdx.y * out_sbat + c0;
+    const int ncv = min(nb, ncols - c0);
+    for (int idx = threadIdx.x; idx < L * nb; idx += blockDim.x) {
+        const int i = idx / nb;
+        const int b = idx - i * nb;
+        C v = mk((R)0, (R)0);
+        if (i < n_in && b < ncv) v = ib[i * in_si + b];
+        s[lay.at(i, b)] = v;
+    }
+    __syncthreads();
+    run_fft<R, DIR, true>(s, lay, plan);
+    for (int idx = threadIdx.x; idx < n_out * nb; idx += blockDim.x) {
+        const int i = idx / nb;
+        const int b = idx - i * nb;
+        if (b < ncv) ob[i * out_si + b] = s[lay.at(i, b)];
+    }
+}
+
+// Spectral convolution along the last transform axis (z for 3-D meshes, y for
+// nz == 1), in place: forward FFT of the three components (zero pad fused),
+// multiply by the symmetric tensor, inverse FFT, keep the first n_in values.
+template <typename R>
+__global__ void __launch_bounds__(kMaxFftThreads) k_conv(cplx_t<R>* S, const R* __restrict__ Nred, FFTPlan fplan, FFTPlan iplan,
+                                               int n_in, int64_t si, int64_t comp_stride, int64_t other_stride,
+                                               int ncols, int nb, int axis_is_z, int ny, int nz, int nxh) {
+    using C = cplx_t<R>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C* s = reinterpret_cast<C*>(smem_raw);
+    const int L = fplan.L;
+    const int nb3 = 3 * nb;
+    const SLay<true> lay{nb3, 0};
+    const int c0 = blockIdx.x * nb;
+    const int other = blockIdx.y;  // ky for the z convolution
+    C* base = S + (int64_t)other * other_stride + c0;
+    const int ncv = min(nb, ncols - c0);
+    for (int idx = threadIdx.x; idx < L * nb3; idx += blockDim.x) {
+        const int i = idx / nb3;
+        const int cb = idx - i * nb3;
+        const int comp = cb / nb;
+        const int b = cb - comp * nb;
+        C v = mk((R)0, (R)0);
+        if (i < n_in && b < ncv) v = base[comp * comp_stride + i * si + b];
+        s[lay.at(i, cb)] = v;
+    }
+    __syncthreads();
+    run_fft<R, -1, true>(s, lay, fplan);
+    // tensor multiply
+    const int Py = 2 * ny;
+    const int Pz = (nz == 1) ? 1 : 2 * nz;
+    const int Kz = (nz == 1) ? 1 : nz + 1;
+    const int64_t cs = (int64_t)Kz * (ny + 1) * nxh;  // component stride of Nred
+    for (int idx = threadIdx.x; idx < L * nb; idx += blockDim.x) {
+        const int kf = idx / nb;
+        const int b = idx - kf * nb;
+        if (b >= ncv) continue;
+        const int kx = c0 + b;
+        int ky, kz;
+        if (axis_is_z) { ky = other; kz = kf; } else { ky = kf; kz = 0; }
+        const int kyr = ky <= ny ? ky : Py - ky;
+        const R sy = ky <= ny ? (R)1 : (R)-1;
+        int kzr = 0;
+        R sz = (R)1;
+        if (nz > 1) { kzr = kz <= nz ? kz : Pz - kz; sz = kz <= nz ? (R)1 : (R)-1; }
+        const int64_t o = ((int64_t)kzr * (ny + 1) + kyr) * nxh + kx;
+        const C mx = s[lay.at(kf, b)];
+        const C my = s[lay.at(kf, nb + b)];
+        const C mz = s[lay.at(kf, 2 * nb + b)];
+        R Nxx, Nxy, Nxz, Nyy, Nyz, Nzz;
+        if (nz > 1) {
+            Nxx = Nred[o];
+            Nxy = sy * Nred[cs + o];
+            Nxz = sz * Nred[2 * cs + o];
+            Nyy = Nred[3 * cs + o];
+            Nyz = sy * sz * Nred[4 * cs + o];
+            Nzz = Nred[5 * cs + o];
+        } else {
+            Nxx = Nred[o];
+            Nxy = sy * Nred[cs + o];
+            Nxz = 0;
+            Nyy = Nred[2 * cs + o];
+            Nyz = 0;
+            Nzz = Nred[3 * cs + o];
+        }
+        const C hx = cadd(cadd(cscale(mx, Nxx), cscale(my, Nxy)), cscale(mz, Nxz));
+        const C hy = cadd(cadd(cscale(mx, Nxy), cscale(my, Nyy)), cscale(mz, Nyz));
+        const C hz = cadd(cadd(cscale(mx, Nxz), cscale(my, Nyz)), cscale(mz, Nzz));
+        s[lay.at(kf, b)] = hx;
+        s[lay.at(kf, nb + b)] = hy;
+        s[lay.at(kf, 2 * nb + b)] = hz;
+    }
+    __syncthreads();
+    run_fft<R, 1, true>(s, lay, iplan);
+    for (int idx = threadIdx.x; idx < n_in * nb3; idx += blockDim.x) {
+        const int i = idx / nb3;
+        const int cb = idx - i * nb3;
+        const int comp = cb / nb;
+        const int b = cb - comp * nb;
+        if (b < ncv) base[comp * comp_stride + i * si + b] = s[lay.at(i, cb)];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// epilogue shared by the fused x-inverse pass and the standalone local kernel
+// ---------------------------------------------------------------------------
+template <typename R>
+__device__ __forceinline__ R cell_Ms(const MsInfo& ms, int64_t cell) {
+    if (ms.field64) {
+        if constexpr (sizeof(R) == 4) return ms.field32[cell];
+        else return (R)ms.field64[cell];
+    }
+    return (R)ms.Ms;
+}
+
+template <typename R, int EPI>
+__device__ __forceinline__ void epilogue_cell(const Geom& g, int x, int y, int z, int64_t cell,
+                                              const R* __restrict__ m, const MsInfo& ms, const TermList& tl,
+                                              const EpilogueArgs& ep, const R hd[3], double& eacc) {
+    R mc[3];
+    mvec(m, g, cell, mc);
+    const bool msf = ms.field64 != nullptr;
+    const R Ms = cell_Ms<R>(ms, cell);
+    if constexpr (EPI == EPI_EDENS) {
+        const double Msd = msf ? ms.field64[cell] : ms.Ms;
+        for (int it = 0; it < tl.n; ++it) {
+            const TermDesc& t = tl.t[it];
+            R ht[3] = {0, 0, 0};
+            double w = -kMu0 / 2.0;
+            if (t.kind == TK_DEMAG) {
+                ht[0] = hd[0]; ht[1] = hd[1]; ht[2] = hd[2];
+            } else if (t.kind == TK_CUBIC) {
+                R h1[3], h2[3], h3[3];
+                cubic_h123(t, mc, Ms, h1, h2, h3);
+                double e = 0;
+                for (int c = 0; c < 3; ++c)
+                    e += (-1.0 / 4.0 * (double)h1[c] - 1.0 / 6.0 * (double)h2[c] - 1.0 / 8.0 * (double)h3[c]) *
+                         (double)mc[c];
+                eacc += kMu0 * Msd * e;
+                continue;
+            } else {
+                add_local_term(t, m, g, x, y, z, cell, mc, Ms, msf, ht);
+                if (t.kind == TK_ZEEMAN) w = -kMu0;
+                if (t.kind == TK_EXCHANGE && ep.edge_exchange && !(msf && Ms == (R)0)) {
+                    // h_withedges: + m/d^2 on each boundary face (exchange_field.cpp:42-51)
+                    const R coef = (R)(2.0 * t.p[0]) / ((R)kMu0 * Ms);
+                    R edge = 0;
+                    const R idx2 = (R)(1.0 / (g.dx * g.dx)), idy2 = (R)(1.0 / (g.dy * g.dy)),
+                            idz2 = (R)(1.0 / (g.dz * g.dz));
+                    R f = 0;
+                    if (x == 0) f += idx2;
+                    if (x == g.nx - 1) f += idx2;
+                    if (y == 0) f += idy2;
+                    if (y == g.ny - 1) f += idy2;
+                    if (z == 0) f += idz2;
+                    if (z == g.nz - 1) f += idz2;
+                    edge = f;
+                    for (int c = 0; c < 3; ++c) ht[c] += coef * (edge * mc[c]);
+                }
+            }
+            const double hm = (double)ht[0] * (double)mc[0] + (double)ht[1] * (double)mc[1] + (double)ht[2] * (double)mc[2];
+            eacc += w * Msd * hm;
+        }
+    } else {
+        R h[3] = {0, 0, 0};
+        for (int it = 0; it < tl.n; ++it) {
+            const TermDesc& t = tl.t[it];
+            if (t.kind == TK_DEMAG) {
+                h[0] += hd[0]; h[1] += hd[1]; h[2] += hd[2];
+            } else {
+                add_local_term(t, m, g, x, y, z, cell, mc, Ms, msf, h);
+            }
+        }
+        if constexpr (EPI == EPI_H) {
+            R* o = static_cast<R*>(ep.out);
+            o[cell] = h[0];
+            o[g.N + cell] = h[1];
+            o[2 * g.N + cell] = h[2];
+        } else {
+            const double* m64 = ep.llg.m64;
+            const double M0 = m64[cell], M1 = m64[g.N + cell], M2 = m64[2 * g.N + cell];
+            const double H0 = h[0], H1 = h[1], H2 = h[2];
+            const double x0 = M1 * H2 - M2 * H1;
+            const double x1 = M2 * H0 - M0 * H2;
+            const double x2 = M0 * H1 - M1 * H0;
+            const double d0 = M1 * x2 - M2 * x1;
+            const double d1 = M2 * x0 - M0 * x2;
+            const double d2 = M0 * x1 - M1 * x0;
+            double cp = ep.llg.c_prec, cd = ep.llg.c_damp;
+            if (ep.llg.alpha) {
+                const double a = ep.llg.alpha[cell];
+                cp = -kGamma / (1. + a * a);
+                cd = -a * kGamma / (1. + a * a);
+            }
+            double k0, k1, k2;
+            if (ep.llg.dissipation_only) {
+                k0 = cd * d0; k1 = cd * d1; k2 = cd * d2;
+            } else {
+                k0 = cp * x0 + cd * d0; k1 = cp * x1 + cd * d1; k2 = cp * x2 + cd * d2;
+            }
+            double* o = static_cast<double*>(ep.out);
+            const double sc = ep.llg.scale;
+            o[cell] = sc * k0;
+            o[g.N + cell] = sc * k1;
+            o[2 * g.N + cell] = sc * k2;
+        }
+    }
+}
+
+__device__ __forceinline__ void block_sum_store(double v, double* partials) {
+    __shared__ double red[32];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) red[wid] = v;
+    __syncthreads();
+    if (wid == 0) {
+        const int nw = (blockDim.x + 31) >> 5;
+        double s = lane < nw ? red[lane] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+        if (lane == 0) partials[blockIdx.x] = s;
+    }
+}
+
+// x-inverse C2R of the half spectrum (3 components of nbr rows), scale, then
+// the per-cell epilogue with the local terms.
+template <typename R, int EPI>
+__global__ void __launch_bounds__(kMaxFftThreads) k_xinv_epi(const cplx_t<R>* __restrict__ S1, int pitch, FFTPlan plan,
+                                                   const cplx_t<R>* __restrict__ twP, Geom g, R scale,
+                                                   const R* __restrict__ m, MsInfo ms, TermList tl, EpilogueArgs ep,
+                                                   int nbr) {
+    using C = cplx_t<R>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C* s = reinterpret_cast<C*>(smem_raw);
+    const int Lc = plan.L;
+    const int nb3 = 3 * nbr;
+    const SLay<false> lay{nb3, spad_len(Lc)};
+    const int64_t rows_pc = (int64_t)g.ny * g.nz;
+    const int64_t ry0 = (int64_t)blockIdx.x * nbr;
+    for (int idx = threadIdx.x; idx < nb3 * Lc; idx += blockDim.x) {
+        const int cb = idx / Lc;
+        const int k = idx - cb * Lc;
+        const int comp = cb / nbr;
+        const int b = cb - comp * nbr;
+        const int64_t ry = ry0 + b;
+        C Z = mk((R)0, (R)0);
+        if (ry < rows_pc) {
+            const C* rp = S1 + (comp * rows_pc + ry) * pitch;
+            const C Xk = rp[k];
+            const C Xm = rp[Lc - k];
+            const C E = cadd(Xk, cconj(Xm));
+            const C O = cmulc(csub(Xk, cconj(Xm)), twP[k]);  // times W_Px^{-k}
+            Z = cadd(E, cmul_i<1>(O));
+        }
+        s[lay.at(k, cb)] = Z;
+    }
+    __syncthreads();
+    run_fft<R, 1, false>(s, lay, plan);
+    double eacc = 0;
+    for (int idx = threadIdx.x; idx < nbr * g.nx; idx += blockDim.x) {
+        const int b = idx / g.nx;
+        const int x = idx - b * g.nx;
+        const int64_t ry = ry0 + b;
+        if (ry >= rows_pc) continue;
+        const int z = (int)(ry / g.ny);
+        const int y = (int)(ry - (int64_t)z * g.ny);
+        const int64_t cell = ry * g.nx + x;
+        R hd[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const C v = s[lay.at(x >> 1, c * nbr + b)];
+            hd[c] = scale * ((x & 1) ? v.y : v.x);
+        }
+        epilogue_cell<R, EPI>(g, x, y, z, cell, m, ms, tl, ep, hd, eacc);
+    }
+    if constexpr (EPI == EPI_EDENS) block_sum_store(eacc, ep.partials);
+}
+
+// Local terms only (no demag in the term list).
+template <typename R, int EPI>
+__global__ void __launch_bounds__(256) k_local_epi(Geom g, const R* __restrict__ m, MsInfo ms, TermList tl,
+                                                   EpilogueArgs ep) {
+    double eacc = 0;
+    const R hd[3] = {0, 0, 0};
+    for (int64_t cell = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; cell < g.N;
+         cell += (int64_t)gridDim.x * blockDim.x) {
+        const int x = (int)(cell % g.nx);
+        const int64_t r = cell / g.nx;
+        const int y = (int)(r % g.ny);
+        const int z = (int)(r / g.ny);
+        epilogue_cell<R, EPI>(g, x, y, z, cell, m, ms, tl, ep, hd, eacc);
+    }
+    if constexpr (EPI == EPI_EDENS) block_sum_store(eacc, ep.partials);
+}
+
+__global__ void k_sum_partials(const double* __restrict__ p, int n, double* out) {
+    double v = 0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) v += p[i];
+    __shared__ double red[32];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        double s = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+        if (threadIdx.x == 0) *out = s;
+    }
+}
+
+__global__ void k_stage32(const double* __restrict__ a, float* __restrict__ b, int64_t n) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        b[i] = (float)a[i];
+}
+
+void stage_m32(const double* m64, float* m32, int64_t n, cudaStream_t st) {
+    const int64_t blocks = std::min<int64_t>(ceil_div(n, 256), 148LL * 16);
+    k_stage32<<<(unsigned)blocks, 256, 0, st>>>(m64, m32, n);
+    MAF_LAUNCH_CHECK();
+}
+
+// Extract the real part of the spectral tensor on the stored quadrant.
+__global__ void k_reduce_tensor(const double2* __restrict__ spec, double* __restrict__ dst, int nxh, int pitch, int Py,
+                                int Kz, int Ky) {
+    const int64_t total = (int64_t)Kz * Ky * nxh;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+        const int kx = (int)(i % nxh);
+        const int ky = (int)((i / nxh) % Ky);
+        const int kz = (int)(i / ((int64_t)nxh * Ky));
+        dst[i] = spec[((int64_t)kz * Py + ky) * pitch + kx].x;
+    }
+}
+
+__global__ void k_d2f(const double* __restrict__ a, float* __restrict__ b, int64_t n) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        b[i] = (float)a[i];
+}
+
+// ---------------------------------------------------------------------------
+// launch helpers
+// ---------------------------------------------------------------------------
+template <typename K> static void set_smem(K kernel, size_t bytes) {
+    if (bytes > 48 * 1024) MAF_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+}
+
+static int round_threads(int t) {
+    t = std::max(t, 32);
+    t = (t + 31) / 32 * 32;
+    if (t > kMaxFftThreads) throw Error(6, "FFT tile needs more threads than one CTA has (transform length too large)");
+    return t;
+}
+
+// choose columns-per-tile so that the tile holds about `target` complex values
+static int pick_nb(int L, int target, int ncols, int nbmax) {
+    int nb = std::max(1, target / std::max(L, 1));
+    nb = std::min(nb, nbmax);
+    nb = std::min(nb, std::max(ncols, 1));
+    return nb;
+}
+
+template <typename R> static int tile_target() { return sizeof(R) == 4 ? 8192 : 4096; }
+
+template <typename R>
+static void launch_xfwd(const R* in, int n_in, int64_t rows, int64_t rows_pc, const R* msf, R ms, cplx_t<R>* out,
+                        int pitch, int Px, Twiddles& tw, cudaStream_t st) {
+    const bool f64 = sizeof(R) == 8;
+    const int Lc = Px / 2;
+    FFTPlan plan = make_fft_plan(Lc, tw.get(Lc, f64));
+    int nb = pick_nb(Lc, tile_target<R>(), (int)std::min<int64_t>(rows, 1 << 20), 64);
+    int threads;
+    while (true) {
+        threads = fft_threads_needed(plan, nb);
+        threads = std::max(threads, std::min(256, nb * Lc));
+        if (threads <= kMaxFftThreads || nb == 1) break;
+        nb = std::max(1, nb / 2);
+    }
+    threads = round_threads(threads);
+    const size_t smem = sizeof(cplx_t<R>) * (size_t)nb * spad_len(Lc);
+    set_smem(k_xfwd<R>, smem);
+    const int64_t blocks = ceil_div(rows, nb);
+    k_xfwd<R><<<(unsigned)blocks, threads, smem, st>>>(in, n_in, rows, rows_pc, msf, ms, out, pitch, plan,
+                                                       static_cast<const cplx_t<R>*>(tw.get(Px, f64)), nb);
+    MAF_LAUNCH_CHECK();
+}
+
+template <typename R, int DIR>
+static void launch_cols(const cplx_t<R>* in, cplx_t<R>* out, int L, int n_in, int n_out, int ncols, int64_t in_si,
+                        int64_t out_si, int64_t in_sbat, int64_t out_sbat, int nbat, Twiddles& tw, cudaStream_t st) {
+    const bool f64 = sizeof(R) == 8;
+    FFTPlan plan = make_fft_plan(L, tw.get(L, f64));
+    int nb = pick_nb(L, tile_target<R>(), ncols, 32);
+    int threads;
+    while (true) {
+        threads = fft_threads_needed(plan, nb);
+        threads = std::max(threads, std::min(256, nb * L));
+        if (threads <= kMaxFftThreads || nb == 1) break;
+        nb = std::max(1, nb / 2);
+    }
+    threads = round_threads(threads);
+    const size_t smem = sizeof(cplx_t<R>) * (size_t)nb * spad_len(L);
+    set_smem(k_fft_cols<R, DIR>, smem);
+    dim3 grid((unsigned)ceil_div(ncols, nb), (unsigned)nbat);
+    k_fft_cols<R, DIR><<<grid, threads, smem, st>>>(in, out, plan, n_in, n_out, ncols, in_si, out_si, in_sbat,
+                                                    out_sbat, nb);
+    MAF_LAUNCH_CHECK();
+}
+
+// ---------------------------------------------------------------------------
+// Demag
+// ---------------------------------------------------------------------------
+Demag::Demag(const MeshDims& md, cudaStream_t st) : md_(md) {
+    if (md.nx < 1 || md.ny < 1 || md.nz < 1) throw Error(1, "DemagField: empty mesh");
+    // complex pitch: multiple of 4 so that tiles of 4 complex values start on 32 B
+    pitch_ = (nxh() + 3) / 4 * 4;
+    // validate all FFT lengths early
+    make_fft_plan(Px() / 2, nullptr);
+    make_fft_plan(Py(), nullptr);
+    make_fft_plan(Pz(), nullptr);
+    build_tensor(st);
+}
+
+void Demag::build_tensor(cudaStream_t st) {
+    const int Px_ = Px(), Py_ = Py(), Pz_ = Pz();
+    const int64_t nreal = (int64_t)Px_ * Py_ * Pz_;
+    const int Ky = md_.ny + 1;
+    const int Kz = md_.nz == 1 ? 1 : md_.nz + 1;
+    const int64_t cstride = (int64_t)Kz * Ky * nxh();
+    Nred64_.alloc(sizeof(double) * cstride * ncomp());
+    DevBuf real(sizeof(double) * nreal);
+    DevBuf spec(sizeof(double2) * (int64_t)Pz_ * Py_ * pitch_);
+    const int comps6[6] = {0, 1, 2, 3, 4, 5};
+    const int comps4[4] = {0, 1, 3, 5};
+    const int* comps = md_.nz == 1 ? comps4 : comps6;
+    for (int ci = 0; ci < ncomp(); ++ci) {
+        newell_component(real.as<double>(), comps[ci], md_, Px_, Py_, Pz_, st);
+        // 3-D R2C of the real tensor component
+        launch_xfwd<double>(real.as<double>(), Px_, (int64_t)Py_ * Pz_, (int64_t)Py_ * Pz_, nullptr, 1.0,
+                            spec.as<double2>(), pitch_, Px_, tw_, st);
+        launch_cols<double, -1>(spec.as<double2>(), spec.as<double2>(), Py_, Py_, Py_, nxh(), pitch_, pitch_,
+                                (int64_t)Py_ * pitch_, (int64_t)Py_ * pitch_, Pz_, tw_, st);
+        if (Pz_ > 1)
+            launch_cols<double, -1>(spec.as<double2>(), spec.as<double2>(), Pz_, Pz_, Pz_, nxh(),
+                                    (int64_t)Py_ * pitch_, (int64_t)Py_ * pitch_, pitch_, pitch_, Py_, tw_, st);
+        const int64_t total = cstride;
+        const int64_t blocks = std::min<int64_t>(ceil_div(total, 256), 148LL * 16);
+        k_reduce_tensor<<<(unsigned)blocks, 256, 0, st>>>(spec.as<double2>(), Nred64_.as<double>() + ci * cstride,
+                                                           nxh(), pitch_, Py_, Kz, Ky);
+        MAF_LAUNCH_CHECK();
+    }
+    MAF_CUDA(cudaStreamSynchronize(st));
+}
+
+void Demag::download_tensor(double* host, cudaStream_t st) const {
+    MAF_CUDA(cudaMemcpyAsync(host, Nred64_.p, sizeof(double) * tensor_elems(), cudaMemcpyDeviceToHost, st));
+    MAF_CUDA(cudaStreamSynchronize(st));
+}
+
+void Demag::download_real_tensor(double* host, cudaStream_t st) {
+    const int64_t nreal = (int64_t)Px() * Py() * Pz();
+    DevBuf real(sizeof(double) * nreal);
+    for (int c = 0; c < 6; ++c) {
+        newell_component(real.as<double>(), c, md_, Px(), Py(), Pz(), st);
+        MAF_CUDA(cudaMemcpyAsync(host + c * nreal, real.p, sizeof(double) * nreal, cudaMemcpyDeviceToHost, st));
+    }
+    MAF_CUDA(cudaStreamSynchronize(st));
+}
+
+template <> const double* Demag::tensor<double>() { return Nred64_.as<double>(); }
+template <> const float* Demag::tensor<float>() {
+    if (!Nred32_.p) {
+        const int64_t n = (int64_t)tensor_elems();
+        Nred32_.alloc(sizeof(float) * n);
+        k_d2f<<<(unsigned)std::min<int64_t>(ceil_div(n, 256), 148LL * 16), 256>>>(Nred64_.as<double>(),
+                                                                                   Nred32_.as<float>(), n);
+        MAF_LAUNCH_CHECK();
+        MAF_CUDA(cudaDeviceSynchronize());
+    }
+    return Nred32_.as<float>();
+}
+
+template <> cplx_t<double>* Demag::S1<double>() {
+    S1_64_.ensure(sizeof(double2) * 3 * md_.N() / md_.nx * pitch_);
+    return S1_64_.as<double2>();
+}
+template <> cplx_t<float>* Demag::S1<float>() {
+    S1_32_.ensure(sizeof(float2) * 3 * md_.N() / md_.nx * pitch_);
+    return S1_32_.as<float2>();
+}
+template <> cplx_t<double>* Demag::S2<double>() {
+    S2_64_.ensure(sizeof(double2) * 3 * (int64_t)md_.nz * Py() * pitch_);
+    return S2_64_.as<double2>();
+}
+template <> cplx_t<float>* Demag::S2<float>() {
+    S2_32_.ensure(sizeof(float2) * 3 * (int64_t)md_.nz * Py() * pitch_);
+    return S2_32_.as<float2>();
+}
+
+template <typename R> void Demag::forward_conv(const R* m, const MsInfo& ms, cudaStream_t st) {
+    using C = cplx_t<R>;
+    const bool f64 = sizeof(R) == 8;
+    const int nx = md_.nx, ny = md_.ny, nz = md_.nz;
+    const int64_t rows_pc = (int64_t)ny * nz;
+    const R* msf = nullptr;
+    if (ms.field64) {
+        if constexpr (sizeof(R) == 4) msf = reinterpret_cast<const R*>(ms.field32);
+        else msf = reinterpret_cast<const R*>(ms.field64);
+    }
+    C* s1 = S1<R>();
+    const R* Nr = tensor<R>();
+    // pass 1: x forward (zero pad fused)
+    launch_xfwd<R>(m, nx, 3 * rows_pc, rows_pc, msf, (R)ms.Ms, s1, pitch_, Px(), tw_, st);
+    if (nz > 1) {
+        C* s2 = S2<R>();
+        // pass 2: y forward, S1 [3*nz][ny][pitch] -> S2 [3*nz][Py][pitch]
+        launch_cols<R, -1>(s1, s2, Py(), ny, Py(), nxh(), pitch_, pitch_, (int64_t)ny * pitch_,
+                           (int64_t)Py() * pitch_, 3 * nz, tw_, st);
+        // pass 3: z forward . tensor . z inverse, in place on S2
+        {
+            const int L = Pz();
+            FFTPlan fp = make_fft_plan(L, tw_.get(L, f64));
+            FFTPlan ip = fp;
+            int nb = pick_nb(3 * L, tile_target<R>(), nxh(), 64);
+            int threads;
+            while (true) {
+                threads = std::max(fft_threads_needed(fp, 3 * nb), std::min(256, 3 * nb * L));
+                if (threads <= kMaxFftThreads || nb == 1) break;
+                nb = std::max(1, nb / 2);
+            }
+            threads = round_threads(threads);
+            const size_t smem = sizeof(C) * (size_t)3 * nb * spad_len(L);
+            set_smem(k_conv<R>, smem);
+            dim3 grid((unsigned)ceil_div(nxh(), nb), (unsigned)Py());
+            k_conv<R><<<grid, threads, smem, st>>>(s2, Nr, fp, ip, nz, (int64_t)Py() * pitch_,
+                                                   (int64_t)nz * Py() * pitch_, pitch_, nxh(), nb, 1, ny, nz, nxh());
+            MAF_LAUNCH_CHECK();
+        }
+        // pass 4: y inverse, S2 -> S1, keep ky rows [0, ny)
+        launch_cols<R, 1>(s2, s1, Py(), Py(), ny, nxh(), pitch_, pitch_, (int64_t)Py() * pitch_,
+                          (int64_t)ny * pitch_, 3 * nz, tw_, st);
+    } else {
+        // pass 2 (2-D): y forward . tensor . y inverse, in place on S1
+        const int L = Py();
+        FFTPlan fp = make_fft_plan(L, tw_.get(L, f64));
+        int nb = pick_nb(3 * L, tile_target<R>(), nxh(), 64);
+        int threads;
+        while (true) {
+            threads = std::max(fft_threads_needed(fp, 3 * nb), std::min(256, 3 * nb * L));
+            if (threads <= kMaxFftThreads || nb == 1) break;
+            nb = std::max(1, nb / 2);
+        }
+        threads = round_threads(threads);
+        const size_t smem = sizeof(C) * (size_t)3 * nb * spad_len(L);
+        set_smem(k_conv<R>, smem);
+        dim3 grid((unsigned)ceil_div(nxh(), nb), 1);
+        k_conv<R><<<grid, threads, smem, st>>>(s1, Nr, fp, fp, ny, pitch_, (int64_t)ny * pitch_, 0, nxh(), nb, 0, ny,
+                                               nz, nxh());
+        MAF_LAUNCH_CHECK();
+    }
+}
+
+template <typename R> int Demag::edens_blocks() const { return 0; }
+
+template <typename R>
+void Demag::inverse_x_epilogue(const R* m, const MsInfo& ms, const TermList& tl, const EpilogueArgs& ep,
+                               cudaStream_t st, int* nblocks_out) {
+    const bool f64 = sizeof(R) == 8;
+    const int Lc = md_.nx;
+    FFTPlan plan = make_fft_plan(Lc, tw_.get(Lc, f64));
+    const int64_t rows_pc = (int64_t)md_.ny * md_.nz;
+    int nbr = pick_nb(3 * Lc, tile_target<R>(), (int)std::min<int64_t>(rows_pc, 1 << 20), 32);
+    int threads;
+    while (true) {
+        threads = std::max(fft_threads_needed(plan, 3 * nbr), std::min(256, 3 * nbr * Lc));
+        if (threads <= kMaxFftThreads || nbr == 1) break;
+        nbr = std::max(1, nbr / 2);
+    }
+    threads = round_threads(threads);
+    const size_t smem = sizeof(cplx_t<R>) * (size_t)3 * nbr * spad_len(Lc);
+    const int64_t blocks = ceil_div(rows_pc, nbr);
+    if (nblocks_out) *nblocks_out = (int)blocks;
+    const R scale = (R)(1.0 / ((double)Px() * Py() * Pz()));
+    const cplx_t<R>* tP = static_cast<const cplx_t<R>*>(tw_.get(Px(), f64));
+    const Geom g = md_.geom();
+    switch (ep.kind) {
+        case EPI_H:
+            set_smem(k_xinv_epi<R, EPI_H>, smem);
+            k_xinv_epi<R, EPI_H><<<(unsigned)blocks, threads, smem, st>>>(S1<R>(), pitch_, plan, tP, g, scale, m, ms,
+                                                                          tl, ep, nbr);
+            break;
+        case EPI_LLG:
+            set_smem(k_xinv_epi<R, EPI_LLG>, smem);
+            k_xinv_epi<R, EPI_LLG><<<(unsigned)blocks, threads, smem, st>>>(S1<R>(), pitch_, plan, tP, g, scale, m,
+                                                                            ms, tl, ep, nbr);
+            break;
+        default:
+            set_smem(k_xinv_epi<R, EPI_EDENS>, smem);
+            k_xinv_epi<R, EPI_EDENS><<<(unsigned)blocks, threads, smem, st>>>(S1<R>(), pitch_, plan, tP, g, scale, m,
+                                                                              ms, tl, ep, nbr);
+            break;
+    }
+    MAF_LAUNCH_CHECK();
+}
+
+template void Demag::forward_conv<float>(const float*, const MsInfo&, cudaStream_t);
+template void Demag::forward_conv<double>(const double*, const MsInfo&, cudaStream_t);
+template void Demag::inverse_x_epilogue<float>(const float*, const MsInfo&, const TermList&, const EpilogueArgs&,
+                                               cudaStream_t, int*);
+template void Demag::inverse_x_epilogue<double>(const double*, const MsInfo&, const TermList&, const EpilogueArgs&,
+                                                cudaStream_t, int*);
+
+// ---------------------------------------------------------------------------
+// field evaluation of a term list
+// ---------------------------------------------------------------------------
+template <typename R>
+void eval_terms(const std::vector<Term*>& terms, const MeshDims& md, const R* m, const MsInfo& ms,
+                const EpilogueArgs& ep_in, cudaStream_t st, DevBuf& scratch, double* energy_out) {
+    if (terms.empty()) throw Error(1, "no field terms");
+    if ((int)terms.size() > kMaxTerms) throw Error(1, "too many field terms (max 8)");
+    TermList tl;
+    Demag* demag = nullptr;
+    for (Term* t : terms) {
+        if (t->kind == TK_DEMAG) {
+            if (demag) throw Error(1, "at most one DemagField per term list");
+            if (!(t->demag_mesh == md)) throw Error(1, "DemagField mesh differs from the state's mesh");
+            demag = t->demag.get();
+        }
+        if (t->kind == TK_BULKDMI && (md.nx < 2 || md.ny < 2 || md.nz < 2))
+            throw Error(1, "BulkDMIExchangeField needs at least 2 cells along x, y and z");
+        tl.t[tl.n++] = t->desc();
+    }
+    EpilogueArgs ep = ep_in;
+    int nblocks = 0;
+    if (ep.kind == EPI_EDENS) {
+        // upper bound of CTAs for the partial sums
+        const int64_t maxb = std::max<int64_t>(md.N(), 148 * 8) + 1;
+        scratch.ensure(sizeof(double) * (maxb + 1));
+        ep.partials = scratch.as<double>();
+    }
+    if (demag) {
+        demag->forward_conv<R>(m, ms, st);
+        demag->inverse_x_epilogue<R>(m, ms, tl, ep, st, &nblocks);
+    } else {
+        const int threads = 256;
+        const int64_t blocks = std::min<int64_t>(ceil_div(md.N(), threads), 148LL * 8);
+        nblocks = (int)blocks;
+        const Geom g = md.geom();
+        switch (ep.kind) {
+            case EPI_H: k_local_epi<R, EPI_H><<<(unsigned)blocks, threads, 0, st>>>(g, m, ms, tl, ep); break;
+            case EPI_LLG: k_local_epi<R, EPI_LLG><<<(unsigned)blocks, threads, 0, st>>>(g, m, ms, tl, ep); break;
+            default: k_local_epi<R, EPI_EDENS><<<(unsigned)blocks, threads, 0, st>>>(g, m, ms, tl, ep); break;
+        }
+        MAF_LAUNCH_CHECK();
+    }
+    if (ep.kind == EPI_EDENS) {
+        double* dst = ep.partials + nblocks;
+        k_sum_partials<<<1, 256, 0, st>>>(ep.partials, nblocks, dst);
+        MAF_LAUNCH_CHECK();
+        double e = 0;
+        MAF_CUDA(cudaMemcpyAsync(&e, dst, sizeof(double), cudaMemcpyDeviceToHost, st));
+        MAF_CUDA(cudaStreamSynchronize(st));
+        if (energy_out) *energy_out = e * md.dx * md.dy * md.dz;
+    }
+}
+
+template void eval_terms<float>(const std::vector<Term*>&, const MeshDims&, const float*, const MsInfo&,
+                                const EpilogueArgs&, cudaStream_t, DevBuf&, double*);
+template void eval_terms<double>(const std::vector<Term*>&, const MeshDims&, const double*, const MsInfo&,
+                                 const EpilogueArgs&, cudaStream_t, DevBuf&, double*);
+
+}  // namespace mafb

@@ -1,0 +1,223 @@
+// Runge-Kutta stage combine, error norm / candidate update, normalisation and
+// small reductions for the adaptive LLG integrator.
+//
+// Reference: magnumaf/src/integrators/adaptive_runge_kutta.cpp:39-173,496-529
+//   stage s:     m_s = m + sum_j a_sj k_j                    (FP64)
+//   error norm:  err = max | rk_error / (atol + rtol |max(m, m + sumbk)|) |
+//   accept:      m <- normalise(m + sumbk)   (normalize_even_zero_vectors, or
+//                the zero-safe normalize when an Ms_field exists)
+// magnumaf/src/math.cpp:6-8 (max_4d_abs), magnumaf/src/util/util.cpp:34-42.
+#include "engine.hpp"
+#include "rk.hpp"
+
+namespace mafb {
+
+__global__ void k_combine(const double* __restrict__ m, KList kl, double* __restrict__ out64, float* __restrict__ out32,
+                          int64_t n) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        double acc = m[i];
+        for (int j = 0; j < kl.n; ++j) acc = acc + kl.c[j] * kl.k[j][i];
+        out64[i] = acc;
+        if (out32) out32[i] = (float)acc;
+    }
+}
+
+void rk_combine(const double* m, const KList& kl, double* out64, float* out32, int64_t n, cudaStream_t st) {
+    const int64_t blocks = std::min<int64_t>(ceil_div(n, 256), 148LL * 16);
+    k_combine<<<(unsigned)blocks, 256, 0, st>>>(m, kl, out64, out32, n);
+    MAF_LAUNCH_CHECK();
+}
+
+// max with NaN propagation (NaN wins)
+__device__ __forceinline__ double nanmax(double a, double b) {
+    if (a != a) return a;
+    if (b != b) return b;
+    return a > b ? a : b;
+}
+
+__device__ __forceinline__ void block_max_store(double v, double* partials) {
+    __shared__ double red[32];
+    for (int o = 16; o > 0; o >>= 1) v = nanmax(v, __shfl_down_sync(0xffffffffu, v, o));
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) red[wid] = v;
+    __syncthreads();
+    if (wid == 0) {
+        const int nw = (blockDim.x + 31) >> 5;
+        double s = lane < nw ? red[lane] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) s = nanmax(s, __shfl_down_sync(0xffffffffu, s, o));
+        if (lane == 0) partials[blockIdx.x] = s;
+    }
+}
+
+// sumbk = sum bs_j k_j ; rk_error = (form 0) sum e_j k_j  or (form 1) sumbk - sum e_j k_j
+__global__ void k_finalize(const double* __restrict__ m, KList kb, KList ke, int form, double atol, double rtol,
+                           double* __restrict__ mcand, int norm_mode, int64_t N, double* __restrict__ partials) {
+    double vmax = 0.0;
+    for (int64_t cell = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; cell < N;
+         cell += (int64_t)gridDim.x * blockDim.x) {
+        double out[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const int64_t i = c * N + cell;
+            double sumbk = kb.c[0] * kb.k[0][i];
+            for (int j = 1; j < kb.n; ++j) sumbk = sumbk + kb.c[j] * kb.k[j][i];
+            double e = ke.c[0] * ke.k[0][i];
+            for (int j = 1; j < ke.n; ++j) e = e + ke.c[j] * ke.k[j][i];
+            const double err = form == 0 ? e : sumbk - e;
+            const double mi = m[i];
+            const double mn = mi + sumbk;
+            const double mx = mi > mn ? mi : mn;  // af::max(m, m + sumbk)
+            const double sc = atol + rtol * fabs(mx);
+            vmax = nanmax(vmax, fabs(err / sc));
+            out[c] = mn;
+        }
+        if (norm_mode == 1) {
+            const double nrm = sqrt(out[0] * out[0] + out[1] * out[1] + out[2] * out[2]);
+            out[0] /= nrm; out[1] /= nrm; out[2] /= nrm;
+        } else if (norm_mode == 2) {
+            const double nrm = sqrt(out[0] * out[0] + out[1] * out[1] + out[2] * out[2]);
+            if (nrm != 0) { out[0] /= nrm; out[1] /= nrm; out[2] /= nrm; }
+            else { out[0] = 0; out[1] = 0; out[2] = 0; }
+        }
+        mcand[cell] = out[0];
+        mcand[N + cell] = out[1];
+        mcand[2 * N + cell] = out[2];
+    }
+    block_max_store(vmax, partials);
+}
+
+__global__ void k_max_partials(const double* __restrict__ p, int n, double* out) {
+    double v = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) v = nanmax(v, p[i]);
+    __shared__ double red[32];
+    for (int o = 16; o > 0; o >>= 1) v = nanmax(v, __shfl_down_sync(0xffffffffu, v, o));
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        double s = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) s = nanmax(s, __shfl_down_sync(0xffffffffu, s, o));
+        if (threadIdx.x == 0) *out = s;
+    }
+}
+
+int rk_finalize(const double* m, const KList& kb, const KList& ke, int form, double atol, double rtol, double* mcand,
+                int norm_mode, int64_t N, double* partials, double* err_dev, cudaStream_t st) {
+    const int threads = 256;
+    const int blocks = (int)std::min<int64_t>(ceil_div(N, threads), 148LL * 8);
+    k_finalize<<<blocks, threads, 0, st>>>(m, kb, ke, form, atol, rtol, mcand, norm_mode, N, partials);
+    MAF_LAUNCH_CHECK();
+    k_max_partials<<<1, 256, 0, st>>>(partials, blocks, err_dev);
+    MAF_LAUNCH_CHECK();
+    return blocks;
+}
+
+// normalize_handle_zero_vectors (util.cpp:37-42); counts cells of zero norm
+__global__ void k_normalize(double* __restrict__ m, int64_t N, int mode, unsigned long long* zero_count) {
+    unsigned long long z = 0;
+    for (int64_t cell = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; cell < N;
+         cell += (int64_t)gridDim.x * blockDim.x) {
+        double a = m[cell], b = m[N + cell], c = m[2 * N + cell];
+        const double nrm = sqrt(a * a + b * b + c * c);
+        if (mode == 1) {
+            a /= nrm; b /= nrm; c /= nrm;
+        } else if (nrm != 0) {
+            a /= nrm; b /= nrm; c /= nrm;
+        } else {
+            a = 0; b = 0; c = 0;
+            ++z;
+        }
+        m[cell] = a;
+        m[N + cell] = b;
+        m[2 * N + cell] = c;
+    }
+    if (zero_count && z) atomicAdd(zero_count, z);
+}
+
+void normalize_m(double* m, int64_t N, int mode, unsigned long long* zero_count_dev, cudaStream_t st) {
+    const int64_t blocks = std::min<int64_t>(ceil_div(N, 256), 148LL * 8);
+    k_normalize<<<(unsigned)blocks, 256, 0, st>>>(m, N, mode, zero_count_dev);
+    MAF_LAUNCH_CHECK();
+}
+
+// Ms_field = Ms * (|m| != 0)   (state.cpp:71-89)
+__global__ void k_ms_from_m(const double* __restrict__ m, double Ms, double* __restrict__ msf, float* __restrict__ msf32,
+                            int64_t N) {
+    for (int64_t cell = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; cell < N;
+         cell += (int64_t)gridDim.x * blockDim.x) {
+        const double a = m[cell], b = m[N + cell], c = m[2 * N + cell];
+        const double v = (sqrt(a * a + b * b + c * c) != 0) ? Ms : 0.0;
+        msf[cell] = v;
+        if (msf32) msf32[cell] = (float)v;
+    }
+}
+
+void ms_field_from_m(const double* m, double Ms, double* msf, float* msf32, int64_t N, cudaStream_t st) {
+    const int64_t blocks = std::min<int64_t>(ceil_div(N, 256), 148LL * 8);
+    k_ms_from_m<<<(unsigned)blocks, 256, 0, st>>>(m, Ms, msf, msf32, N);
+    MAF_LAUNCH_CHECK();
+}
+
+// <m>: per-block sums of the three components and of the nonzero-cell count,
+// then a fixed-order final pass (state.cpp:32-43).
+__global__ void k_mean_partials(const double* __restrict__ m, int64_t N, double* __restrict__ part) {
+    double s0 = 0, s1 = 0, s2 = 0, cnt = 0;
+    for (int64_t cell = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; cell < N;
+         cell += (int64_t)gridDim.x * blockDim.x) {
+        const double a = m[cell], b = m[N + cell], c = m[2 * N + cell];
+        s0 += a;
+        s1 += b;
+        s2 += c;
+        cnt += (sqrt(a * a + b * b + c * c) != 0) ? 1.0 : 0.0;
+    }
+    __shared__ double red[4][32];
+    double v[4] = {s0, s1, s2, cnt};
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        for (int o = 16; o > 0; o >>= 1) v[q] += __shfl_down_sync(0xffffffffu, v[q], o);
+        if (lane == 0) red[q][wid] = v[q];
+    }
+    __syncthreads();
+    if (wid == 0) {
+        const int nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            double s = lane < nw ? red[q][lane] : 0.0;
+            for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+            if (lane == 0) part[4 * blockIdx.x + q] = s;
+        }
+    }
+}
+
+__global__ void k_mean_final(const double* __restrict__ part, int nb, double* __restrict__ out) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        double s[4] = {0, 0, 0, 0};
+        for (int b = 0; b < nb; ++b)
+            for (int q = 0; q < 4; ++q) s[q] += part[4 * b + q];
+        out[0] = s[0] / s[3];
+        out[1] = s[1] / s[3];
+        out[2] = s[2] / s[3];
+    }
+}
+
+void mean_m(const double* m, int64_t N, double* scratch, double* out_dev, cudaStream_t st) {
+    const int blocks = (int)std::min<int64_t>(ceil_div(N, 256), 148LL * 2);
+    k_mean_partials<<<blocks, 256, 0, st>>>(m, N, scratch);
+    MAF_LAUNCH_CHECK();
+    k_mean_final<<<1, 32, 0, st>>>(scratch, blocks, out_dev);
+    MAF_LAUNCH_CHECK();
+}
+
+// (a - b) -> d, with sum of squares partials (for the string method's Frobenius norm)
+__global__ void k_f2d(const float* __restrict__ a, double* __restrict__ b, int64_t n) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        b[i] = (double)a[i];
+}
+
+void f32_to_f64(const float* a, double* b, int64_t n, cudaStream_t st) {
+    const int64_t blocks = std::min<int64_t>(ceil_div(n, 256), 148LL * 16);
+    k_f2d<<<(unsigned)blocks, 256, 0, st>>>(a, b, n);
+    MAF_LAUNCH_CHECK();
+}
+
+}  // namespace mafb

@@ -1,0 +1,22 @@
+// Launch wrappers of the Runge-Kutta / normalisation kernels (llg.cu).
+#pragma once
+#include "common.cuh"
+
+namespace mafb {
+
+struct KList {
+    const double* k[8] = {};
+    double c[8] = {};
+    int n = 0;
+};
+
+void rk_combine(const double* m, const KList& kl, double* out64, float* out32, int64_t n, cudaStream_t st);
+// returns the number of partial CTAs; err_dev receives the NaN-propagating max
+int rk_finalize(const double* m, const KList& kb, const KList& ke, int form, double atol, double rtol, double* mcand,
+                int norm_mode, int64_t N, double* partials, double* err_dev, cudaStream_t st);
+void normalize_m(double* m, int64_t N, int mode, unsigned long long* zero_count_dev, cudaStream_t st);
+void ms_field_from_m(const double* m, double Ms, double* msf, float* msf32, int64_t N, cudaStream_t st);
+void mean_m(const double* m, int64_t N, double* scratch, double* out_dev, cudaStream_t st);
+void f32_to_f64(const float* a, double* b, int64_t n, cudaStream_t st);
+
+}  // namespace mafb

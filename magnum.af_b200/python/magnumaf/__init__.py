@@ -1,0 +1,504 @@
+"""Python mirror of magnum.af's script API (python/magnumaf.pyx) over the
+B200 C ABI (include/maf_b200.h).
+
+Class and method names, argument meaning and defaults follow the reference's
+Cython module: ``Mesh``, ``State``, ``DemagField``, ``ExchangeField``,
+``DmiField``, ``BulkDMIExchangeField``, ``UniaxialAnisotropyField``,
+``CubicAnisotropyField``, ``ExternalField``, ``LLGIntegrator`` and
+``Constants``.  ArrayFire arrays are replaced by NumPy arrays of the same
+shape: a vector field is ``(nx, ny, nz, 3)``, a scalar field ``(nx, ny, nz)``
+(or ``(nx, ny, nz, 1)``).  Arrays returned by the library are Fortran-ordered,
+i.e. exactly the reference's column-major memory.
+
+The compute path is the CUDA library ``libmafb200.so`` only; importing this
+module fails loudly when the library is missing, and every compute call
+raises ``MafError`` when no GPU is available.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import os
+from typing import Optional, Sequence
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.normpath(os.path.join(_HERE, "..", "..", "lib", "libmafb200.so"))
+
+if not os.path.exists(_LIB_PATH):
+    raise ImportError(
+        "libmafb200.so not found at %s; build it with `python magnum.af_b200/build.py` "
+        "(there is no CPU fallback)" % _LIB_PATH)
+
+lib = C.CDLL(_LIB_PATH)
+
+_P = C.c_void_p
+_D = C.c_double
+_I = C.c_int
+_DP = C.POINTER(C.c_double)
+_FP = C.POINTER(C.c_float)
+
+# exported symbols and their signatures (include/maf_b200.h)
+_SIGS = {
+    "maf_last_error": (C.c_char_p, []),
+    "maf_version": (_I, [C.POINTER(_I), C.POINTER(_I)]),
+    "maf_device_count": (_I, [C.POINTER(_I)]),
+    "maf_state_create": (_I, [C.POINTER(_P), _I, _I, _I, _D, _D, _D, _D, _DP, _DP, _I]),
+    "maf_state_destroy": (_I, [_P]),
+    "maf_state_get_m": (_I, [_P, _DP]),
+    "maf_state_set_m": (_I, [_P, _DP]),
+    "maf_state_get_t": (_I, [_P, _DP]),
+    "maf_state_set_t": (_I, [_P, _D]),
+    "maf_state_get_steps": (_I, [_P, C.POINTER(C.c_ulonglong)]),
+    "maf_state_mean_m": (_I, [_P, _DP]),
+    "maf_state_get_Ms_field": (_I, [_P, _DP, C.POINTER(_I)]),
+    "maf_state_get_Ms": (_I, [_P, _DP]),
+    "maf_state_set_stream": (_I, [_P, _P]),
+    "maf_state_device_m": (_I, [_P, C.POINTER(_P)]),
+    "maf_state_precision": (_I, [_P, C.POINTER(_I)]),
+    "maf_term_demag_create": (_I, [C.POINTER(_P), _I, _I, _I, _D, _D, _D]),
+    "maf_term_exchange_create": (_I, [C.POINTER(_P), _D]),
+    "maf_term_dmi_create": (_I, [C.POINTER(_P), _D, _D, _D, _D]),
+    "maf_term_dmi_field_create": (_I, [C.POINTER(_P), _I, _I, _I, _DP, _D, _D, _D]),
+    "maf_term_bulkdmi_exchange_create": (_I, [C.POINTER(_P), _D, _D]),
+    "maf_term_uniaxial_create": (_I, [C.POINTER(_P), _D, _D, _D, _D]),
+    "maf_term_uniaxial_field_create": (_I, [C.POINTER(_P), _I, _I, _I, _DP, _D, _DP, _D, _D, _D]),
+    "maf_term_cubic_create": (_I, [C.POINTER(_P), _D, _D, _D, _DP, _DP]),
+    "maf_term_external_create": (_I, [C.POINTER(_P), _I, _I, _I, _DP]),
+    "maf_term_external_uniform_create": (_I, [C.POINTER(_P), _D, _D, _D]),
+    "maf_term_destroy": (_I, [_P]),
+    "maf_term_H": (_I, [_P, _P, _DP]),
+    "maf_term_H_f32": (_I, [_P, _P, _FP]),
+    "maf_term_E": (_I, [_P, _P, _DP]),
+    "maf_term_demag_tensor": (_I, [_P, _DP]),
+    "maf_term_demag_real_tensor": (_I, [_P, _DP]),
+    "maf_llg_create": (_I, [C.POINTER(_P), _D, _DP, _I, _I, _I, C.POINTER(_P), _I, C.c_char_p, _D, _D, _D, _D, _I]),
+    "maf_llg_destroy": (_I, [_P]),
+    "maf_llg_add_term": (_I, [_P, _P]),
+    "maf_llg_set_alpha": (_I, [_P, _D]),
+    "maf_llg_step": (_I, [_P, _P]),
+    "maf_llg_steps": (_I, [_P, _P, _I]),
+    "maf_llg_E": (_I, [_P, _P, _DP]),
+    "maf_llg_heff": (_I, [_P, _P, _DP]),
+    "maf_llg_heff_f32": (_I, [_P, _P, _FP]),
+    "maf_llg_heff_device": (_I, [_P, _P, _P, _P]),
+    "maf_llg_dmdt": (_I, [_P, _P, _DP]),
+    "maf_llg_integrate_dense": (_I, [_P, _P, _D, _D, _DP, _I, C.POINTER(_I)]),
+    "maf_llg_relax": (_I, [_P, _P, _D, _I]),
+    "maf_llg_get_h": (_I, [_P, _DP]),
+    "maf_llg_counters": (_I, [_P, C.POINTER(C.c_ulonglong)]),
+}
+for _name, (_res, _args) in _SIGS.items():
+    _f = getattr(lib, _name)
+    _f.restype = _res
+    _f.argtypes = _args
+
+MAF_FP64 = 0
+MAF_FP32_FIELD = 1
+_PRECISION = {"fp64": MAF_FP64, "f64": MAF_FP64, MAF_FP64: MAF_FP64,
+              "fp32_field": MAF_FP32_FIELD, "fp32": MAF_FP32_FIELD, MAF_FP32_FIELD: MAF_FP32_FIELD}
+ERROR_NAMES = {1: "BADARG", 2: "CUDA", 3: "OOM", 4: "NAN", 5: "TIMEOUT", 6: "UNSUPPORTED", 7: "NODEVICE"}
+
+
+class MafError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("[%s] %s" % (ERROR_NAMES.get(code, code), msg))
+        self.code = code
+
+
+def _ck(rc):
+    if rc != 0:
+        raise MafError(rc, lib.maf_last_error().decode())
+
+
+def _dptr(a: np.ndarray):
+    return a.ctypes.data_as(_DP)
+
+
+def _vec_soa(a, mesh=None) -> np.ndarray:
+    """(nx,ny,nz,3) -> bytes of [3][nz][ny][nx] (Fortran order of the 4-D array)."""
+    a = np.asarray(a, dtype=np.float64)
+    if a.ndim != 4 or a.shape[3] != 3:
+        raise ValueError("expected a vector field of shape (nx, ny, nz, 3), got %s" % (a.shape,))
+    if mesh is not None and a.shape[:3] != (mesh.nx, mesh.ny, mesh.nz):
+        raise ValueError("field shape %s does not match the mesh" % (a.shape,))
+    return np.asfortranarray(a)
+
+
+def _scalar_soa(a) -> np.ndarray:
+    a = np.asarray(a, dtype=np.float64)
+    if a.ndim == 4:
+        a = a[..., 0]
+    if a.ndim != 3:
+        raise ValueError("expected a scalar field of shape (nx, ny, nz[, 1])")
+    return np.asfortranarray(a)
+
+
+class Constants:
+    """magnumaf/include/magnumaf/constants.hpp:9-22"""
+    mu0 = 4e-7 * math.pi
+    gamma = 1.760859644e11 * mu0
+    mu_b = 9.274009994e-24
+    e = -1.6021766208e-19
+    kb = 1.38064852e-23
+    hbar = 1.0545718e-34
+
+
+class Mesh:
+    def __init__(self, nx, ny, nz, dx, dy, dz):
+        self.nx, self.ny, self.nz = int(nx), int(ny), int(nz)
+        self.dx, self.dy, self.dz = float(dx), float(dy), float(dz)
+
+    @property
+    def n(self):
+        return self.nx * self.ny * self.nz
+
+
+def device_count() -> int:
+    n = C.c_int(0)
+    _ck(lib.maf_device_count(C.byref(n)))
+    return n.value
+
+
+class State:
+    """State(mesh, Ms, m): Ms is a float or an (nx,ny,nz[,1]) array; m is (nx,ny,nz,3).
+    ``precision`` selects the FP64 form (default) or the FP32-field form."""
+
+    def __init__(self, mesh: Mesh, Ms, m, verbose=True, mute_warning=False, precision="fp64"):
+        self.mesh = mesh
+        self._h = _P()
+        mf = _vec_soa(m, mesh)
+        prec = _PRECISION[precision]
+        if np.ndim(Ms) == 0:
+            _ck(lib.maf_state_create(C.byref(self._h), mesh.nx, mesh.ny, mesh.nz, mesh.dx, mesh.dy, mesh.dz,
+                                     float(Ms), None, _dptr(mf), prec))
+        else:
+            msf = _scalar_soa(Ms)
+            _ck(lib.maf_state_create(C.byref(self._h), mesh.nx, mesh.ny, mesh.nz, mesh.dx, mesh.dy, mesh.dz,
+                                     float("nan"), _dptr(msf), _dptr(mf), prec))
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib.maf_state_destroy(self._h)
+            self._h = None
+
+    def __str__(self):
+        mx, my, mz = self.mean_m()
+        return str(self.t) + " " + str(mx) + " " + str(my) + " " + str(mz)
+
+    @property
+    def m(self) -> np.ndarray:
+        out = np.empty((self.mesh.nx, self.mesh.ny, self.mesh.nz, 3), order="F")
+        _ck(lib.maf_state_get_m(self._h, _dptr(out)))
+        return out
+
+    @m.setter
+    def m(self, m_in):
+        mf = _vec_soa(m_in, self.mesh)
+        _ck(lib.maf_state_set_m(self._h, _dptr(mf)))
+
+    @property
+    def t(self) -> float:
+        v = C.c_double()
+        _ck(lib.maf_state_get_t(self._h, C.byref(v)))
+        return v.value
+
+    @t.setter
+    def t(self, value):
+        _ck(lib.maf_state_set_t(self._h, float(value)))
+
+    @property
+    def steps(self) -> int:
+        v = C.c_ulonglong()
+        _ck(lib.maf_state_get_steps(self._h, C.byref(v)))
+        return v.value
+
+    @property
+    def Ms(self) -> float:
+        v = C.c_double()
+        _ck(lib.maf_state_get_Ms(self._h, C.byref(v)))
+        return v.value
+
+    @property
+    def Ms_field(self) -> Optional[np.ndarray]:
+        has = C.c_int()
+        _ck(lib.maf_state_get_Ms_field(self._h, None, C.byref(has)))
+        if not has.value:
+            return None
+        out = np.empty((self.mesh.nx, self.mesh.ny, self.mesh.nz), order="F")
+        _ck(lib.maf_state_get_Ms_field(self._h, _dptr(out), C.byref(has)))
+        return out
+
+    @property
+    def precision(self) -> int:
+        v = C.c_int()
+        _ck(lib.maf_state_precision(self._h, C.byref(v)))
+        return v.value
+
+    def mean_m(self, i=None):
+        out = np.empty(3)
+        _ck(lib.maf_state_mean_m(self._h, _dptr(out)))
+        if i is None:
+            return float(out[0]), float(out[1]), float(out[2])
+        return float(out[i])
+
+    def mean_mx(self):
+        return self.mean_m(0)
+
+    def mean_my(self):
+        return self.mean_m(1)
+
+    def mean_mz(self):
+        return self.mean_m(2)
+
+    def normalize(self):
+        self.m = self.m
+
+    def set_stream(self, stream_handle: int):
+        _ck(lib.maf_state_set_stream(self._h, C.c_void_p(stream_handle)))
+
+    def device_m(self) -> int:
+        p = _P()
+        _ck(lib.maf_state_device_m(self._h, C.byref(p)))
+        return p.value
+
+
+class FieldTerm:
+    _h = None
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib.maf_term_destroy(self._h)
+            self._h = None
+
+    def H_in_Apm(self, state: State) -> np.ndarray:
+        out = np.empty((state.mesh.nx, state.mesh.ny, state.mesh.nz, 3), order="F")
+        _ck(lib.maf_term_H(self._h, state._h, _dptr(out)))
+        return out
+
+    def H_in_Apm_f32(self, state: State) -> np.ndarray:
+        out = np.empty((state.mesh.nx, state.mesh.ny, state.mesh.nz, 3), dtype=np.float32, order="F")
+        _ck(lib.maf_term_H_f32(self._h, state._h, out.ctypes.data_as(_FP)))
+        return out
+
+    def H_in_T(self, state: State) -> np.ndarray:
+        return self.H_in_Apm(state) * Constants.mu0
+
+    def Energy_in_J(self, state: State) -> float:
+        v = C.c_double()
+        _ck(lib.maf_term_E(self._h, state._h, C.byref(v)))
+        return v.value
+
+    def Energy_in_eV(self, state: State) -> float:
+        return self.Energy_in_J(state) / 1.6021766208e-19
+
+
+class DemagField(FieldTerm):
+    """DemagField(mesh, verbose=False, caching=False, nthreads=4): the tensor is
+    always assembled on the GPU; ``caching`` and ``nthreads`` are accepted for
+    signature compatibility."""
+
+    def __init__(self, mesh: Mesh, verbose=False, caching=False, nthreads=4):
+        self.mesh = mesh
+        self._h = _P()
+        _ck(lib.maf_term_demag_create(C.byref(self._h), mesh.nx, mesh.ny, mesh.nz, mesh.dx, mesh.dy, mesh.dz))
+
+    def spectral_tensor(self) -> np.ndarray:
+        """Reduced real spectral tensor [ncomp][kz][ky][kx] (C order)."""
+        m = self.mesh
+        ncomp = 4 if m.nz == 1 else 6
+        kz = 1 if m.nz == 1 else m.nz + 1
+        out = np.empty((ncomp, kz, m.ny + 1, m.nx + 1))
+        _ck(lib.maf_term_demag_tensor(self._h, _dptr(out)))
+        return out
+
+    def get_N(self) -> np.ndarray:
+        """Real-space Newell tensor [Px, Py, Pz, 6] (the reference's setup_N layout)."""
+        m = self.mesh
+        Px, Py, Pz = 2 * m.nx, 2 * m.ny, (1 if m.nz == 1 else 2 * m.nz)
+        out = np.empty((6, Pz, Py, Px))
+        _ck(lib.maf_term_demag_real_tensor(self._h, _dptr(out)))
+        return out.transpose(3, 2, 1, 0)
+
+
+class ExchangeField(FieldTerm):
+    def __init__(self, A, mesh: Mesh = None, verbose=False):
+        self.A = float(A)
+        self._h = _P()
+        _ck(lib.maf_term_exchange_create(C.byref(self._h), self.A))
+
+
+class DmiField(FieldTerm):
+    def __init__(self, D, D_axis=(0.0, 0.0, 1.0)):
+        self._h = _P()
+        ax = [float(v) for v in D_axis]
+        if np.ndim(D) == 0:
+            self.D = float(D)
+            _ck(lib.maf_term_dmi_create(C.byref(self._h), self.D, *ax))
+        else:
+            d = _scalar_soa(D)
+            nx, ny, nz = d.shape
+            _ck(lib.maf_term_dmi_field_create(C.byref(self._h), nx, ny, nz, _dptr(d), *ax))
+
+
+class BulkDMIExchangeField(FieldTerm):
+    def __init__(self, D, A):
+        self._h = _P()
+        _ck(lib.maf_term_bulkdmi_exchange_create(C.byref(self._h), float(D), float(A)))
+
+
+class UniaxialAnisotropyField(FieldTerm):
+    def __init__(self, Ku1, Ku1_axis=(0.0, 0.0, 1.0)):
+        self._h = _P()
+        scalar_axis = np.ndim(Ku1_axis) == 1
+        if np.ndim(Ku1) == 0 and scalar_axis:
+            self.Ku1 = float(Ku1)
+            ax = np.asarray(Ku1_axis, dtype=np.float64)
+            self.Ku1_axis = list(ax / math.sqrt(float(np.sum(ax * ax))))
+            _ck(lib.maf_term_uniaxial_create(C.byref(self._h), self.Ku1, *[float(v) for v in Ku1_axis]))
+            return
+        kf = None if np.ndim(Ku1) == 0 else _scalar_soa(Ku1)
+        af = None if scalar_axis else _vec_soa(Ku1_axis)
+        shape = (kf if kf is not None else af).shape[:3]
+        ax = [0.0, 0.0, 1.0] if not scalar_axis else [float(v) for v in Ku1_axis]
+        self.Ku1 = Ku1
+        _ck(lib.maf_term_uniaxial_field_create(C.byref(self._h), shape[0], shape[1], shape[2],
+                                               None if kf is None else _dptr(kf),
+                                               float(Ku1) if kf is None else 0.0,
+                                               None if af is None else _dptr(af), *ax))
+
+
+class CubicAnisotropyField(FieldTerm):
+    def __init__(self, Kc1, Kc2=0.0, Kc3=0.0, c1=(1.0, 0.0, 0.0), c2=(0.0, 1.0, 0.0)):
+        self._h = _P()
+        a = np.asarray(c1, dtype=np.float64)
+        b = np.asarray(c2, dtype=np.float64)
+        _ck(lib.maf_term_cubic_create(C.byref(self._h), float(Kc1), float(Kc2), float(Kc3), _dptr(a), _dptr(b)))
+
+
+class ExternalField(FieldTerm):
+    def __init__(self, array_in):
+        self._h = _P()
+        h = _vec_soa(array_in)
+        self.shape = h.shape
+        nx, ny, nz, _ = h.shape
+        _ck(lib.maf_term_external_create(C.byref(self._h), nx, ny, nz, _dptr(h)))
+
+    @staticmethod
+    def uniform(hx, hy, hz):
+        t = ExternalField.__new__(ExternalField)
+        t._h = _P()
+        _ck(lib.maf_term_external_uniform_create(C.byref(t._h), float(hx), float(hy), float(hz)))
+        return t
+
+    def set_homogeneous_field(self, x, y, z):
+        nx, ny, nz, _ = self.shape
+        h = np.empty((nx, ny, nz, 3), order="F")
+        h[..., 0], h[..., 1], h[..., 2] = x, y, z
+        old = self._h
+        self._h = _P()
+        _ck(lib.maf_term_external_create(C.byref(self._h), nx, ny, nz, _dptr(h)))
+        lib.maf_term_destroy(old)
+
+
+class LLGIntegrator:
+    """LLGIntegrator(alpha, terms, mode="RKF45", hmin=1e-15, hmax=3.5e-10,
+    atol=1e-6, rtol=1e-6, dissipation_term_only=False)"""
+
+    def __init__(self, alpha, terms: Sequence[FieldTerm], mode="RKF45", hmin=1e-15, hmax=3.5e-10, atol=1e-6,
+                 rtol=1e-6, dissipation_term_only=False):
+        self._h = _P()
+        self._terms = list(terms)  # keep the Python objects alive
+        arr = (_P * max(1, len(self._terms)))(*[t._h for t in self._terms])
+        if np.ndim(alpha) == 0:
+            self._alpha = float(alpha)
+            _ck(lib.maf_llg_create(C.byref(self._h), self._alpha, None, 0, 0, 0, arr, len(self._terms),
+                                   mode.encode(), hmin, hmax, atol, rtol, int(bool(dissipation_term_only))))
+        else:
+            af = _scalar_soa(alpha)
+            self._alpha = af
+            nx, ny, nz = af.shape
+            _ck(lib.maf_llg_create(C.byref(self._h), 0.0, _dptr(af), nx, ny, nz, arr, len(self._terms),
+                                   mode.encode(), hmin, hmax, atol, rtol, int(bool(dissipation_term_only))))
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib.maf_llg_destroy(self._h)
+            self._h = None
+
+    def step(self, state: State):
+        _ck(lib.maf_llg_step(self._h, state._h))
+
+    def steps(self, state: State, n: int):
+        _ck(lib.maf_llg_steps(self._h, state._h, int(n)))
+
+    def Eeff_in_J(self, state: State) -> float:
+        v = C.c_double()
+        _ck(lib.maf_llg_E(self._h, state._h, C.byref(v)))
+        return v.value
+
+    E = Eeff_in_J
+
+    def H_in_Apm(self, state: State) -> np.ndarray:
+        out = np.empty((state.mesh.nx, state.mesh.ny, state.mesh.nz, 3), order="F")
+        _ck(lib.maf_llg_heff(self._h, state._h, _dptr(out)))
+        return out
+
+    def H_in_Apm_f32(self, state: State) -> np.ndarray:
+        out = np.empty((state.mesh.nx, state.mesh.ny, state.mesh.nz, 3), dtype=np.float32, order="F")
+        _ck(lib.maf_llg_heff_f32(self._h, state._h, out.ctypes.data_as(_FP)))
+        return out
+
+    def dmdt(self, state: State) -> np.ndarray:
+        out = np.empty((state.mesh.nx, state.mesh.ny, state.mesh.nz, 3), order="F")
+        _ck(lib.maf_llg_dmdt(self._h, state._h, _dptr(out)))
+        return out
+
+    def add_terms(self, *args):
+        for t in args:
+            _ck(lib.maf_llg_add_term(self._h, t._h))
+            self._terms.append(t)
+
+    def relax(self, state: State, precision=1e-10, ncalcE=100, nprint=1000, verbose=True):
+        _ck(lib.maf_llg_relax(self._h, state._h, float(precision), int(ncalcE)))
+
+    def integrate_dense(self, state: State, time_in_s, write_every_dt_in_s, filename=None, verbose=False,
+                        append=False) -> np.ndarray:
+        """Returns the rows (t, <mx>, <my>, <mz>) and, like the reference, writes
+        them to `filename` when one is given."""
+        max_rows = int(math.ceil(time_in_s / write_every_dt_in_s)) + 4
+        rows = np.zeros((max_rows, 4))
+        n = C.c_int()
+        _ck(lib.maf_llg_integrate_dense(self._h, state._h, float(time_in_s), float(write_every_dt_in_s),
+                                        _dptr(rows), max_rows, C.byref(n)))
+        rows = rows[: n.value]
+        if filename:
+            with open(filename, "a" if append else "w") as f:
+                for r in rows:
+                    f.write("%r\t%r\t%r\t%r\n" % tuple(r))
+        return rows
+
+    @property
+    def alpha(self):
+        return self._alpha
+
+    @alpha.setter
+    def alpha(self, value):
+        self._alpha = float(value)
+        _ck(lib.maf_llg_set_alpha(self._h, self._alpha))
+
+    @property
+    def h(self) -> float:
+        v = C.c_double()
+        _ck(lib.maf_llg_get_h(self._h, C.byref(v)))
+        return v.value
+
+    def counters(self):
+        out = (C.c_ulonglong * 4)()
+        _ck(lib.maf_llg_counters(self._h, out))
+        return {"accepted": out[0], "rejected": out[1], "hmin": out[2], "hmax": out[3]}
+
+    def heff_device(self, state: State, m_dev_ptr: int, H_dev_ptr: int):
+        """Field of a device-resident m into a device-resident H (no sync)."""
+        _ck(lib.maf_llg_heff_device(self._h, state._h, C.c_void_p(m_dev_ptr), C.c_void_p(H_dev_ptr)))
