@@ -1,0 +1,394 @@
+"""Benchmark: effective-field evaluations per second at 1024 x 1024 x 16 cells.
+
+Workload (one "step" = one H_eff evaluation of the full mesh): 1024 x 1024 x 16
+cells of 3 nm, Ms = 8.6e5 A/m, terms demag (open boundaries, zero-padded FFT
+convolution) + exchange (A = 1.3e-11 J/m) + cubic anisotropy (K1 = -1e4 J/m^3,
+lab axes) + a uniform Zeeman field drawn from a 50 mT ball; m uniform random on
+the unit sphere.  Inputs are synthetic and seeded.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+value      FP32-field form, H_eff evals/s with m resident in HBM (the field pipeline
+           alone), summed over all ranks (independent replicas, "weak" scaling).
+e2e        the same metric through the public C ABI with host buffers: every step
+           copies m (FP64) host->device from pinned memory and H (FP32) back.
+fp64_form  the FP64 form on the same mesh; rel_err_fp32_vs_fp64 checks the metric's
+           condition (FP32-field error <= 1e-5 relative to the FP64 form).
+roofline   the dominant pass: algorithmic bytes per launch / its mean CUDA-event
+           duration, against the measured HBM copy bandwidth.
+--impl reference  the FP64 CPU oracle (the reference algorithm restated in NumPy/SciPy)
+           on all host cores; each step evaluates a 2-layer slab of the workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+for _p in (os.path.join(ROOT, "magnum.af_b200", "python"), os.path.join(ROOT, "oracle")):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+METRIC = "Heff evals/s at 1024²×16; FP32-field vs FP64 form, rel. err ≤1e-5 vs FP64"
+NX, NY, NZ = 1024, 1024, 16  # the metric's mesh (--mesh overrides it for small profiling runs)
+DX = 3e-9
+MS = 8.6e5
+A_EX = 1.3e-11
+K1 = -1.0e4
+SEED = 1234
+MU0 = 4e-7 * math.pi
+
+
+def workload(seed=SEED, nz=None):
+    nz = NZ if nz is None else nz
+    rng = np.random.default_rng(seed)
+    m = rng.normal(size=(NX, NY, nz, 3))
+    m /= np.linalg.norm(m, axis=3, keepdims=True)
+    # uniform in a 50 mT ball
+    v = rng.normal(size=3)
+    v /= np.linalg.norm(v)
+    r = 0.05 * rng.uniform() ** (1.0 / 3.0)
+    h_ext = v * r / MU0
+    return np.asfortranarray(m), h_ext
+
+
+# algorithmic bytes per pass at the metric's mesh: the five-pass padded-FFT model
+# (r = 4 B FP32 / 8 B FP64, c = 2r, nxh = nx+1, Py = 2 ny, tensor stored on the
+# (nx+1)(ny+1)(nz+1) quadrant with 6 components)
+def pass_bytes(r, nx=None, ny=None, nz=None):
+    nx, ny, nz = (NX if nx is None else nx), (NY if ny is None else ny), (NZ if nz is None else nz)
+    c = 2 * r
+    N = nx * ny * nz
+    nxh = nx + 1
+    Py = 2 * ny
+    T = 6 * nxh * (ny + 1) * (nz + 1) * r
+    return {
+        "x_fwd": 3 * N * r + 3 * nxh * ny * nz * c,
+        "y_fwd": 3 * nxh * ny * nz * c + 3 * nxh * Py * nz * c,
+        "z_conv": 3 * nxh * Py * nz * c + T + 3 * nxh * Py * nz * c,
+        "y_inv": 3 * nxh * Py * nz * c + 3 * nxh * ny * nz * c,
+        "x_inv_local": 3 * nxh * ny * nz * c + 3 * N * r + 3 * N * r,
+    }
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def ncu_traffic():
+    """Per-launch DRAM bytes of the dominant pass from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "traffic_1024x1024x16.txt")
+    out = {}
+    try:
+        with open(p) as f:
+            for line in f:
+                if line.startswith("#") or "=" not in line:
+                    continue
+                k, v = line.split("=", 1)
+                out[k.strip()] = float(v.split()[0])
+    except OSError:
+        pass
+    return out
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = os.path.join("/tmp", "maf_clocks_%d_%d.csv" % (os.getpid(), gpu_index))
+
+    def start(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sm.append(float(parts[1]))
+                    mx.append(float(parts[2]))
+                except ValueError:
+                    continue
+                for n, v in zip(names, parts[5:9]):
+                    if v.lower() == "active":
+                        reasons.add(n)
+        os.unlink(self.path)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_oracle_sample(nz_sample=2, reps=1):
+    """FP64 oracle H_eff on a 1024 x 1024 x nz_sample slab of the workload, FFTs on all
+    host cores (scipy.fft workers), tensor assembled by the oracle (untimed).
+    Returns (seconds per sample evaluation, threads)."""
+    import maf_oracle as O
+
+    threads = os.cpu_count() or 1
+    O.FFT_WORKERS = threads
+    mesh = O.Mesh(NX, NY, nz_sample, DX, DX, DX)
+    m, h_ext = workload(nz=nz_sample)
+    state = O.State(mesh, MS, m)
+    N = O.demag_tensor_symmetric(mesh, workers=threads)
+    demag = O.DemagField(mesh, N_real=N)
+    del N
+    terms = [demag, O.ExchangeField(A_EX), O.CubicAnisotropyField(K1), O.ExternalField(h_ext)]
+    times = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        O.Heff_in_Apm(terms, state)
+        times.append(time.perf_counter() - t0)
+    return min(times), threads
+
+
+def run_reference(args):
+    """--impl reference: the FP64 CPU oracle on the host cores, rank 0 only."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import maf_oracle as O
+
+    threads = os.cpu_count() or 1
+    O.FFT_WORKERS = threads
+    nzs = 2
+    mesh = O.Mesh(NX, NY, nzs, DX, DX, DX)
+    m, h_ext = workload(nz=nzs)
+    state = O.State(mesh, MS, m)
+    demag = O.DemagField(mesh, N_real=O.demag_tensor_symmetric(mesh, workers=threads))
+    terms = [demag, O.ExchangeField(A_EX), O.CubicAnisotropyField(K1), O.ExternalField(h_ext)]
+    for _ in range(args.warmup):
+        O.Heff_in_Apm(terms, state)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        O.Heff_in_Apm(terms, state)
+    dt = (time.perf_counter() - t0) / max(args.steps, 1)
+    # a full evaluation covers NZ/nzs slabs (cost measured linear in the layer count)
+    per_eval = dt * NZ / nzs
+    value = 1.0 / per_eval
+    sample = ("FP64 oracle H_eff (numpy/scipy, FFTs on %d threads) on a 1024x1024x%d slab of the workload per "
+              "step; full-mesh evals/s = slab rate x %d/%d" % (threads, nzs, nzs, NZ))
+    line = {
+        "metric": METRIC, "value": value, "unit": "evals/s", "impl": "reference", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+        "config": {"workload": "H_eff demag+exchange+cubic+Zeeman, 1024x1024x16 cells of 3 nm",
+                   "cells": NX * NY * NZ, "sample_layers": nzs},
+        "cpu_baseline": {"value": value, "unit": "evals/s", "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": "evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args):
+    import ctypes as C
+
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    import magnumaf as M
+
+    lib = M.lib
+    dev = torch.device("cuda", local)
+    mesh = M.Mesh(NX, NY, NZ, DX, DX, DX)
+    m, h_ext = workload(seed=SEED + rank)
+    stream = torch.cuda.Stream(device=dev)
+    demag = M.DemagField(mesh)
+    terms = [demag, M.ExchangeField(A_EX), M.CubicAnisotropyField(K1), M.ExternalField.uniform(*h_ext)]
+    llg = M.LLGIntegrator(0.01, terms, "DP45")
+    s32 = M.State(mesh, MS, m, precision="fp32_field")
+    s64 = M.State(mesh, MS, m, precision="fp64")
+    s32.set_stream(stream.cuda_stream)
+    s64.set_stream(stream.cuda_stream)
+    n3 = 3 * NX * NY * NZ
+    m_norm = np.asarray(s64.m, order="F").ravel(order="F")  # normalised m, [3][nz][ny][nx]
+    m64_dev = torch.from_numpy(m_norm).to(dev)
+    m32_dev = m64_dev.float()
+    H32 = torch.empty(n3, dtype=torch.float32, device=dev)
+    H64 = torch.empty(n3, dtype=torch.float64, device=dev)
+    torch.cuda.synchronize()
+
+    def barrier():
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def timed(fn, steps, warmup):
+        with torch.cuda.stream(stream):
+            for _ in range(warmup):
+                fn()
+        barrier()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        with torch.cuda.stream(stream):
+            for _ in range(steps):
+                fn()
+        ev1.record(stream)
+        ev1.synchronize()
+        barrier()
+        ms = ev0.elapsed_time(ev1)
+        if dist:
+            t = torch.tensor([ms], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms
+
+    f32 = lambda: llg.heff_device(s32, m32_dev.data_ptr(), H32.data_ptr())
+    f64 = lambda: llg.heff_device(s64, m64_dev.data_ptr(), H64.data_ptr())
+
+    clk = ClockSampler(local)
+    clk.start()
+    ms32 = timed(f32, args.steps, args.warmup)
+    clocks = clk.stop()
+    ms64 = timed(f64, args.steps, args.warmup)
+
+    # accuracy of the FP32-field form against the FP64 form on the full mesh
+    f32()
+    f64()
+    torch.cuda.synchronize()
+    d = (H32.double() - H64)
+    rel_err = float(torch.linalg.vector_norm(d) / torch.linalg.vector_norm(H64))
+    rel_max = float(d.abs().max() / H64.abs().max())
+
+    # per-pass timing (CUDA events between the pass kernels on the launching stream)
+    passes = {}
+    nprof = max(3, min(args.steps, 10))
+    for _ in range(nprof):
+        for name, ms in llg.heff_device_profile(s32, m32_dev.data_ptr(), H32.data_ptr()):
+            passes.setdefault(name, []).append(ms)
+    pass_ms = {k: float(np.mean(v)) for k, v in passes.items()}
+    bytes32 = pass_bytes(4)
+    dominant = max(pass_ms, key=pass_ms.get)
+    peak, peak_kind = peaks()
+    achieved = bytes32[dominant] / (pass_ms[dominant] * 1e-3) / 1e9
+    traffic = ncu_traffic().get(dominant)
+    eval_bytes = sum(bytes32.values())
+    eval_gbs = eval_bytes / (ms32 / args.steps * 1e-3) / 1e9
+
+    # end to end through the C ABI with pinned host buffers
+    m_host = torch.from_numpy(m_norm.copy()).pin_memory()
+    H_host = torch.empty(n3, dtype=torch.float32).pin_memory()
+    mp = C.cast(C.c_void_p(m_host.data_ptr()), C.POINTER(C.c_double))
+    hp = C.cast(C.c_void_p(H_host.data_ptr()), C.POINTER(C.c_float))
+
+    def e2e_step():
+        M._ck(lib.maf_state_set_m(s32._h, mp))
+        M._ck(lib.maf_llg_heff_f32(llg._h, s32._h, hp))
+
+    e2e_steps = max(1, min(args.steps, 20))
+    ms_e2e = timed(e2e_step, e2e_steps, max(1, min(args.warmup, 3)))
+
+    npass = len(pass_ms)
+    value = world * args.steps / (ms32 * 1e-3)
+    line = {
+        "metric": METRIC,
+        "value": value,
+        "unit": "evals/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms32 / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic (seeded random m on the unit sphere, random 50 mT-ball Zeeman field)",
+        "config": {"workload": "H_eff demag+exchange+cubic+Zeeman, 1024x1024x16 cells of 3 nm (FP32-field form)",
+                   "cells": NX * NY * NZ, "parallelism": "replicas x%d" % world,
+                   "l2": "inputs larger than L2 (m 201 MB, spectra 403-806 MB per pass)"},
+        "fp64_form": {"value": world * args.steps / (ms64 * 1e-3), "ms_per_step": ms64 / args.steps,
+                      "fp32_speedup": ms64 / ms32},
+        "rel_err_fp32_vs_fp64": {"l2": rel_err, "max": rel_max},
+        "passes_ms": pass_ms,
+        "eval_roofline": {"bytes": eval_bytes, "achieved_gbs": eval_gbs, "frac": eval_gbs / peak},
+        "roofline": {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
+                     "algorithmic_bytes": bytes32[dominant]},
+        "e2e": {"value": world * e2e_steps / (ms_e2e * 1e-3), "unit": "evals/s", "h2d_bytes_per_step": n3 * 8,
+                "d2h_bytes_per_step": n3 * 4},
+        "gpu_launches": npass * args.steps,
+        "clocks": clocks,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        t, threads = cpu_oracle_sample(nz_sample=2)
+        per_eval = t * NZ / 2
+        line["cpu_baseline"] = {
+            "value": 1.0 / per_eval, "unit": "evals/s", "cores": threads, "kind": "port",
+            "sample": "one FP64 oracle H_eff of a 1024x1024x2 slab of the workload (FFTs on %d threads), "
+                      "scaled x1/8 to the 16-layer mesh" % threads}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    del s32, s64
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--mesh", type=int, nargs=3, default=None, metavar=("NX", "NY", "NZ"),
+                    help="smaller mesh for profiling captures (the reported metric is defined at 1024 1024 16)")
+    args = ap.parse_args()
+    if args.mesh:
+        global NX, NY, NZ
+        NX, NY, NZ = args.mesh
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

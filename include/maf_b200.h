@@ -118,9 +118,12 @@ int maf_term_E(maf_term t, maf_state s, double* E);
 /* DemagField only: the symmetry-reduced real spectral tensor, FP64,
  * [ncomp][nz == 1 ? 1 : nz+1][ny+1][nx+1], ncomp = 6 (xx,xy,xz,yy,yz,zz) or 4 (xx,xy,yy,zz) when nz == 1 */
 int maf_term_demag_tensor(maf_term t, double* host);
-/* DemagField only: the real-space Newell tensor on the padded grid, [6][Pz][Py][Px]
- * (replaces DemagField::calc_N, demag_field.cpp:207-209, in the x-fastest layout) */
-int maf_term_demag_real_tensor(maf_term t, double* host);
+/* DemagField only: the real-space Newell tensor on the padded grid, [6][Pz][Py][Px].
+ * symmetric == 0: the reference's setup_N values (DemagField::calc_N, demag_field.cpp:104-121,207-209,
+ *                 in the x-fastest layout);
+ * symmetric == 1: the parity-exact tensor the spectral pipeline transforms: values at (|j0|,|j1|,|j2|)
+ *                 with each component's parity sign, odd components zero on their Nyquist planes. */
+int maf_term_demag_real_tensor(maf_term t, double* host, int symmetric);
 
 /* ------------------------------------------------------------ Integrator ---
  * LLGIntegrator(double alpha, vec_uptr_FieldTerm terms, std::string scheme = "RKF45",
@@ -149,12 +152,24 @@ int maf_llg_heff_f32(maf_llg l, maf_state s, float* H_host);
 /* Effective field from a device-resident m (float* for FP32-field states, double* for FP64 states)
  * into a device-resident H of the same type, on the state's stream; no synchronisation. */
 int maf_llg_heff_device(maf_llg l, maf_state s, const void* m_dev, void* H_dev);
+/* maf_llg_heff_device with a CUDA event after every pass kernel: synchronises and
+ * returns each pass's duration in ms (the instrumentation LLGIntegrator::time_heff,
+ * llg_integrator.cpp:11-16, and the per-term timers of field_term.hpp:49-86 provide,
+ * at pass granularity).  Pass names come from maf_llg_pass_name. */
+int maf_llg_heff_device_profile(maf_llg l, maf_state s, const void* m_dev, void* H_dev, double* pass_ms,
+                                int max_passes, int* npasses);
+int maf_llg_pass_name(maf_llg l, maf_state s, int index, char* buf, int buflen);
 /* dm/dt = LLGIntegrator::f(state) (llg_integrator.cpp:18-38) */
 int maf_llg_dmdt(maf_llg l, maf_state s, double* dmdt_host);
 /* LLGIntegrator::integrate_dense (llg_integrator.cpp:68-104): rows of (t, <mx>, <my>, <mz>),
  * the first row being the initial state; at most max_rows rows are written. */
 int maf_llg_integrate_dense(maf_llg l, maf_state s, double time_in_s, double write_every_dt_in_s, double* rows,
                             int max_rows, int* nrows);
+/* One Runge-Kutta attempt of `scheme` ("RKF45", "DP45", "BS23") with step dt from the
+ * state's m, without the step controller: AdaptiveRungeKutta::RKF45/DP45/BS23(state, dt, err)
+ * (adaptive_runge_kutta.cpp:75-173, 496-529).  Writes m + sumbk (not normalised) and the
+ * scaled error norm; the state is not changed. */
+int maf_llg_rk_attempt(maf_llg l, maf_state s, const char* scheme, double dt, double* m_new_host, double* err);
 /* LLGIntegrator::relax (llg_integrator.cpp:43-66) */
 int maf_llg_relax(maf_llg l, maf_state s, double precision, int eval_E);
 /* current step size h and the controller counters {accepted, rejected, hmin, hmax}

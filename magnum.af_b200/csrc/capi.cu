@@ -755,10 +755,10 @@ int maf_term_demag_tensor(maf_term t, double* host) {
     });
 }
 
-int maf_term_demag_real_tensor(maf_term t, double* host) {
+int maf_term_demag_real_tensor(maf_term t, double* host, int symmetric) {
     return guarded([&] {
         check(t && host && t->t->kind == TK_DEMAG, "maf_term_demag_real_tensor: not a DemagField");
-        t->t->demag->download_real_tensor(host, 0);
+        t->t->demag->download_real_tensor(host, symmetric != 0, 0);
     });
 }
 
@@ -871,6 +871,49 @@ int maf_llg_heff_device(maf_llg l, maf_state s, const void* m_dev, void* H_dev) 
     });
 }
 
+int maf_llg_heff_device_profile(maf_llg l, maf_state s, const void* m_dev, void* H_dev, double* pass_ms,
+                                int max_passes, int* npasses) {
+    return guarded([&] {
+        check_llg_state(l, s);
+        check(m_dev && H_dev && pass_ms && npasses, "NULL argument");
+        EpilogueArgs ep;
+        ep.kind = EPI_H;
+        ep.out = H_dev;
+        StateD& st = s->s;
+        PassMarks marks;
+        if (st.precision == PREC_FP32_FIELD)
+            eval_terms<float>(raw_terms(l->terms), st.md, static_cast<const float*>(m_dev), st.msinfo(), ep, st.stream,
+                              s->scratch, nullptr, &marks);
+        else
+            eval_terms<double>(raw_terms(l->terms), st.md, static_cast<const double*>(m_dev), st.msinfo(), ep,
+                               st.stream, s->scratch, nullptr, &marks);
+        MAF_CUDA(cudaStreamSynchronize(st.stream));
+        int n = 0;
+        for (size_t i = 1; i < marks.ev.size() && n < max_passes; ++i, ++n) {
+            float ms = 0;
+            MAF_CUDA(cudaEventElapsedTime(&ms, marks.ev[i - 1], marks.ev[i]));
+            pass_ms[n] = ms;
+        }
+        *npasses = n;
+    });
+}
+
+int maf_llg_pass_name(maf_llg l, maf_state s, int index, char* buf, int buflen) {
+    return guarded([&] {
+        check_llg_state(l, s);
+        check(buf && buflen > 0, "NULL argument");
+        bool demag = false;
+        for (auto& t : l->terms) demag = demag || t->kind == TK_DEMAG;
+        static const char* n3[] = {"x_fwd", "y_fwd", "z_conv", "y_inv", "x_inv_local"};
+        static const char* n2[] = {"x_fwd", "y_conv", "x_inv_local"};
+        static const char* n0[] = {"local"};
+        const char** names = !demag ? n0 : (s->s.md.nz > 1 ? n3 : n2);
+        const int count = !demag ? 1 : (s->s.md.nz > 1 ? 5 : 3);
+        check(index >= 0 && index < count, "pass index out of range");
+        std::snprintf(buf, (size_t)buflen, "%s", names[index]);
+    });
+}
+
 int maf_llg_dmdt(maf_llg l, maf_state s, double* out) {
     return guarded([&] {
         check_llg_state(l, s);
@@ -931,6 +974,18 @@ int maf_llg_integrate_dense(maf_llg l, maf_state s, double time_in_s, double wri
             }
         }
         *nrows = n;
+    });
+}
+
+int maf_llg_rk_attempt(maf_llg l, maf_state s, const char* scheme, double dt, double* m_new_host, double* err) {
+    return guarded([&] {
+        check_llg_state(l, s);
+        check(scheme && m_new_host && err, "NULL argument");
+        const Scheme sch = make_scheme(scheme);
+        *err = rk_attempt(l, s, sch, dt, 0);
+        MAF_CUDA(cudaMemcpyAsync(m_new_host, l->mcand.p, sizeof(double) * 3 * s->s.md.N(), cudaMemcpyDeviceToHost,
+                                 s->s.stream));
+        MAF_CUDA(cudaStreamSynchronize(s->s.stream));
     });
 }
 

@@ -82,6 +82,23 @@ struct EpilogueArgs {
     int edge_exchange = 1;         // EPI_EDENS: exchange energy uses h_withedges
 };
 
+// Optional CUDA-event marks recorded after every pass kernel of a field
+// evaluation (used to time the passes individually).
+struct PassMarks {
+    std::vector<cudaEvent_t> ev;
+    std::vector<const char*> names;
+    void mark(cudaStream_t st, const char* name) {
+        cudaEvent_t e;
+        MAF_CUDA(cudaEventCreate(&e));
+        MAF_CUDA(cudaEventRecord(e, st));
+        ev.push_back(e);
+        names.push_back(name);
+    }
+    ~PassMarks() {
+        for (auto e : ev) cudaEventDestroy(e);
+    }
+};
+
 struct MsInfo {
     double Ms = 0;                 // scalar Ms (used when field == nullptr)
     const double* field64 = nullptr;
@@ -101,14 +118,14 @@ class Demag {
     int ncomp() const { return md_.nz == 1 ? 4 : 6; }
     // Passes 1..4: spectral convolution of Ms*m, result left in the half-spectrum
     // buffer for the fused x-inverse epilogue.
-    template <typename R> void forward_conv(const R* m, const MsInfo& ms, cudaStream_t st);
+    template <typename R> void forward_conv(const R* m, const MsInfo& ms, cudaStream_t st, PassMarks* marks = nullptr);
     // Pass 5: x-inverse + local terms + epilogue (called by the field evaluator).
     template <typename R>
     void inverse_x_epilogue(const R* m, const MsInfo& ms, const TermList& tl, const EpilogueArgs& ep,
-                            cudaStream_t st, int* nblocks_out);
+                            cudaStream_t st, int* nblocks_out, PassMarks* marks = nullptr);
     // reduced real spectral tensor in FP64 [ncomp][kz][ky][kx] (host copy for tests)
     void download_tensor(double* host, cudaStream_t st) const;
-    void download_real_tensor(double* host, cudaStream_t st);  // [6][Pz][Py][Px]
+    void download_real_tensor(double* host, bool symmetric, cudaStream_t st);  // [6][Pz][Py][Px]
     size_t tensor_elems() const { return (size_t)ncomp() * (md_.nz == 1 ? 1 : md_.nz + 1) * (md_.ny + 1) * nxh(); }
     int pitch() const { return pitch_; }
     template <typename R> int edens_blocks() const;
@@ -167,12 +184,15 @@ struct StateD {
 // Field evaluation of a list of terms on m (precision R), with one epilogue.
 template <typename R>
 void eval_terms(const std::vector<Term*>& terms, const MeshDims& md, const R* m, const MsInfo& ms,
-                const EpilogueArgs& ep, cudaStream_t st, DevBuf& scratch_partials, double* energy_out);
+                const EpilogueArgs& ep, cudaStream_t st, DevBuf& scratch_partials, double* energy_out,
+                PassMarks* marks = nullptr);
 
 // FP64 -> FP32 staging of m
 void stage_m32(const double* m64, float* m32, int64_t n, cudaStream_t st);
 
-// Newell tensor on the padded grid, one component [Pz][Py][Px] (newell.cu).
-void newell_component(double* out, int comp, const MeshDims& md, int Px, int Py, int Pz, cudaStream_t st);
+// Newell tensor on the padded grid, one component [Pz][Py][Px] (newell.cu);
+// symmetric = true gives the parity-exact tensor the spectral pipeline uses.
+void newell_component(double* out, int comp, const MeshDims& md, int Px, int Py, int Pz, bool symmetric,
+                      cudaStream_t st);
 
 }  // namespace mafb

@@ -291,25 +291,17 @@ __device__ __forceinline__ void epilogue_cell(const Geom& g, int x, int y, int z
                          (double)mc[c];
                 eacc += kMu0 * Msd * e;
                 continue;
+            } else if (t.kind == TK_EXCHANGE && ep.edge_exchange) {
+                // h_withedges (exchange_field.cpp:28-60): the zero-padded stencil plus
+                // m/d^2 on each boundary face, i.e. the Neumann Laplacian
+                if (!(msf && Ms == (R)0)) {
+                    const R coef = (R)(2.0 * t.p[0]) / ((R)kMu0 * Ms);
+                    h_exchange_add(m, g, x, y, z, mc, coef, (R)(1.0 / (g.dx * g.dx)), (R)(1.0 / (g.dy * g.dy)),
+                                   (R)(1.0 / (g.dz * g.dz)), true, ht);
+                }
             } else {
                 add_local_term(t, m, g, x, y, z, cell, mc, Ms, msf, ht);
                 if (t.kind == TK_ZEEMAN) w = -kMu0;
-                if (t.kind == TK_EXCHANGE && ep.edge_exchange && !(msf && Ms == (R)0)) {
-                    // h_withedges: + m/d^2 on each boundary face (exchange_field.cpp:42-51)
-                    const R coef = (R)(2.0 * t.p[0]) / ((R)kMu0 * Ms);
-                    R edge = 0;
-                    const R idx2 = (R)(1.0 / (g.dx * g.dx)), idy2 = (R)(1.0 / (g.dy * g.dy)),
-                            idz2 = (R)(1.0 / (g.dz * g.dz));
-                    R f = 0;
-                    if (x == 0) f += idx2;
-                    if (x == g.nx - 1) f += idx2;
-                    if (y == 0) f += idy2;
-                    if (y == g.ny - 1) f += idy2;
-                    if (z == 0) f += idz2;
-                    if (z == g.nz - 1) f += idz2;
-                    edge = f;
-                    for (int c = 0; c < 3; ++c) ht[c] += coef * (edge * mc[c]);
-                }
             }
             const double hm = (double)ht[0] * (double)mc[0] + (double)ht[1] * (double)mc[1] + (double)ht[2] * (double)mc[2];
             eacc += w * Msd * hm;
@@ -583,7 +575,7 @@ void Demag::build_tensor(cudaStream_t st) {
     const int comps4[4] = {0, 1, 3, 5};
     const int* comps = md_.nz == 1 ? comps4 : comps6;
     for (int ci = 0; ci < ncomp(); ++ci) {
-        newell_component(real.as<double>(), comps[ci], md_, Px_, Py_, Pz_, st);
+        newell_component(real.as<double>(), comps[ci], md_, Px_, Py_, Pz_, true, st);
         // 3-D R2C of the real tensor component
         launch_xfwd<double>(real.as<double>(), Px_, (int64_t)Py_ * Pz_, (int64_t)Py_ * Pz_, nullptr, 1.0,
                             spec.as<double2>(), pitch_, Px_, tw_, st);
@@ -606,11 +598,11 @@ void Demag::download_tensor(double* host, cudaStream_t st) const {
     MAF_CUDA(cudaStreamSynchronize(st));
 }
 
-void Demag::download_real_tensor(double* host, cudaStream_t st) {
+void Demag::download_real_tensor(double* host, bool symmetric, cudaStream_t st) {
     const int64_t nreal = (int64_t)Px() * Py() * Pz();
     DevBuf real(sizeof(double) * nreal);
     for (int c = 0; c < 6; ++c) {
-        newell_component(real.as<double>(), c, md_, Px(), Py(), Pz(), st);
+        newell_component(real.as<double>(), c, md_, Px(), Py(), Pz(), symmetric, st);
         MAF_CUDA(cudaMemcpyAsync(host + c * nreal, real.p, sizeof(double) * nreal, cudaMemcpyDeviceToHost, st));
     }
     MAF_CUDA(cudaStreamSynchronize(st));
@@ -646,7 +638,7 @@ template <> cplx_t<float>* Demag::S2<float>() {
     return S2_32_.as<float2>();
 }
 
-template <typename R> void Demag::forward_conv(const R* m, const MsInfo& ms, cudaStream_t st) {
+template <typename R> void Demag::forward_conv(const R* m, const MsInfo& ms, cudaStream_t st, PassMarks* marks) {
     using C = cplx_t<R>;
     const bool f64 = sizeof(R) == 8;
     const int nx = md_.nx, ny = md_.ny, nz = md_.nz;
@@ -660,11 +652,13 @@ template <typename R> void Demag::forward_conv(const R* m, const MsInfo& ms, cud
     const R* Nr = tensor<R>();
     // pass 1: x forward (zero pad fused)
     launch_xfwd<R>(m, nx, 3 * rows_pc, rows_pc, msf, (R)ms.Ms, s1, pitch_, Px(), tw_, st);
+    if (marks) marks->mark(st, "x_fwd");
     if (nz > 1) {
         C* s2 = S2<R>();
         // pass 2: y forward, S1 [3*nz][ny][pitch] -> S2 [3*nz][Py][pitch]
         launch_cols<R, -1>(s1, s2, Py(), ny, Py(), nxh(), pitch_, pitch_, (int64_t)ny * pitch_,
                            (int64_t)Py() * pitch_, 3 * nz, tw_, st);
+        if (marks) marks->mark(st, "y_fwd");
         // pass 3: z forward . tensor . z inverse, in place on S2
         {
             const int L = Pz();
@@ -684,10 +678,12 @@ template <typename R> void Demag::forward_conv(const R* m, const MsInfo& ms, cud
             k_conv<R><<<grid, threads, smem, st>>>(s2, Nr, fp, ip, nz, (int64_t)Py() * pitch_,
                                                    (int64_t)nz * Py() * pitch_, pitch_, nxh(), nb, 1, ny, nz, nxh());
             MAF_LAUNCH_CHECK();
+            if (marks) marks->mark(st, "z_conv");
         }
         // pass 4: y inverse, S2 -> S1, keep ky rows [0, ny)
         launch_cols<R, 1>(s2, s1, Py(), Py(), ny, nxh(), pitch_, pitch_, (int64_t)Py() * pitch_,
                           (int64_t)ny * pitch_, 3 * nz, tw_, st);
+        if (marks) marks->mark(st, "y_inv");
     } else {
         // pass 2 (2-D): y forward . tensor . y inverse, in place on S1
         const int L = Py();
@@ -706,6 +702,7 @@ template <typename R> void Demag::forward_conv(const R* m, const MsInfo& ms, cud
         k_conv<R><<<grid, threads, smem, st>>>(s1, Nr, fp, fp, ny, pitch_, (int64_t)ny * pitch_, 0, nxh(), nb, 0, ny,
                                                nz, nxh());
         MAF_LAUNCH_CHECK();
+        if (marks) marks->mark(st, "y_conv");
     }
 }
 
@@ -713,7 +710,7 @@ template <typename R> int Demag::edens_blocks() const { return 0; }
 
 template <typename R>
 void Demag::inverse_x_epilogue(const R* m, const MsInfo& ms, const TermList& tl, const EpilogueArgs& ep,
-                               cudaStream_t st, int* nblocks_out) {
+                               cudaStream_t st, int* nblocks_out, PassMarks* marks) {
     const bool f64 = sizeof(R) == 8;
     const int Lc = md_.nx;
     FFTPlan plan = make_fft_plan(Lc, tw_.get(Lc, f64));
@@ -750,21 +747,23 @@ void Demag::inverse_x_epilogue(const R* m, const MsInfo& ms, const TermList& tl,
             break;
     }
     MAF_LAUNCH_CHECK();
+    if (marks) marks->mark(st, "x_inv_local");
 }
 
-template void Demag::forward_conv<float>(const float*, const MsInfo&, cudaStream_t);
-template void Demag::forward_conv<double>(const double*, const MsInfo&, cudaStream_t);
+template void Demag::forward_conv<float>(const float*, const MsInfo&, cudaStream_t, PassMarks*);
+template void Demag::forward_conv<double>(const double*, const MsInfo&, cudaStream_t, PassMarks*);
 template void Demag::inverse_x_epilogue<float>(const float*, const MsInfo&, const TermList&, const EpilogueArgs&,
-                                               cudaStream_t, int*);
+                                               cudaStream_t, int*, PassMarks*);
 template void Demag::inverse_x_epilogue<double>(const double*, const MsInfo&, const TermList&, const EpilogueArgs&,
-                                                cudaStream_t, int*);
+                                                cudaStream_t, int*, PassMarks*);
 
 // ---------------------------------------------------------------------------
 // field evaluation of a term list
 // ---------------------------------------------------------------------------
 template <typename R>
 void eval_terms(const std::vector<Term*>& terms, const MeshDims& md, const R* m, const MsInfo& ms,
-                const EpilogueArgs& ep_in, cudaStream_t st, DevBuf& scratch, double* energy_out) {
+                const EpilogueArgs& ep_in, cudaStream_t st, DevBuf& scratch, double* energy_out,
+                PassMarks* marks) {
     if (terms.empty()) throw Error(1, "no field terms");
     if ((int)terms.size() > kMaxTerms) throw Error(1, "too many field terms (max 8)");
     TermList tl;
@@ -788,19 +787,22 @@ void eval_terms(const std::vector<Term*>& terms, const MeshDims& md, const R* m,
         ep.partials = scratch.as<double>();
     }
     if (demag) {
-        demag->forward_conv<R>(m, ms, st);
-        demag->inverse_x_epilogue<R>(m, ms, tl, ep, st, &nblocks);
+        if (marks) marks->mark(st, "start");
+        demag->forward_conv<R>(m, ms, st, marks);
+        demag->inverse_x_epilogue<R>(m, ms, tl, ep, st, &nblocks, marks);
     } else {
         const int threads = 256;
         const int64_t blocks = std::min<int64_t>(ceil_div(md.N(), threads), 148LL * 8);
         nblocks = (int)blocks;
         const Geom g = md.geom();
+        if (marks) marks->mark(st, "start");
         switch (ep.kind) {
             case EPI_H: k_local_epi<R, EPI_H><<<(unsigned)blocks, threads, 0, st>>>(g, m, ms, tl, ep); break;
             case EPI_LLG: k_local_epi<R, EPI_LLG><<<(unsigned)blocks, threads, 0, st>>>(g, m, ms, tl, ep); break;
             default: k_local_epi<R, EPI_EDENS><<<(unsigned)blocks, threads, 0, st>>>(g, m, ms, tl, ep); break;
         }
         MAF_LAUNCH_CHECK();
+        if (marks) marks->mark(st, "local");
     }
     if (ep.kind == EPI_EDENS) {
         double* dst = ep.partials + nblocks;
@@ -814,8 +816,8 @@ void eval_terms(const std::vector<Term*>& terms, const MeshDims& md, const R* m,
 }
 
 template void eval_terms<float>(const std::vector<Term*>&, const MeshDims&, const float*, const MsInfo&,
-                                const EpilogueArgs&, cudaStream_t, DevBuf&, double*);
+                                const EpilogueArgs&, cudaStream_t, DevBuf&, double*, PassMarks*);
 template void eval_terms<double>(const std::vector<Term*>&, const MeshDims&, const double*, const MsInfo&,
-                                 const EpilogueArgs&, cudaStream_t, DevBuf&, double*);
+                                 const EpilogueArgs&, cudaStream_t, DevBuf&, double*, PassMarks*);
 
 }  // namespace mafb

@@ -101,6 +101,28 @@ __device__ __forceinline__ void bulk_neighbour(const R* __restrict__ m, const Ge
     }
 }
 
+// Exchange Laplacian of one cell, added as coef * lap to h.  neumann = false:
+// neighbours outside the mesh are zero (exchange_field.cpp:115-126);
+// neumann = true: they are absent, i.e. the h_withedges field of the exchange
+// energy (exchange_field.cpp:28-51, which adds m/d^2 back on each boundary face).
+template <typename R>
+__device__ __forceinline__ void h_exchange_add(const R* __restrict__ m, const Geom& g, int x, int y, int z,
+                                               const R mc[3], R coef, R idx2, R idy2, R idz2, bool neumann, R h[3]) {
+    const int64_t cell = ((int64_t)z * g.ny + y) * g.nx + x;
+    const bool xm = x > 0, xp = x < g.nx - 1, ym = y > 0, yp = y < g.ny - 1, zm = z > 0, zp = z < g.nz - 1;
+    const int64_t sy = g.nx, sz = (int64_t)g.nx * g.ny;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        const R* mcmp = m + c * g.N + cell;
+        const R v = mc[c];
+        const R ab = neumann ? (R)0 : -v;  // contribution of a neighbour outside the mesh
+        const R ax = (xm ? mcmp[-1] - v : ab) + (xp ? mcmp[1] - v : ab);
+        const R ay = (ym ? mcmp[-sy] - v : ab) + (yp ? mcmp[sy] - v : ab);
+        const R az = (zm ? mcmp[-sz] - v : ab) + (zp ? mcmp[sz] - v : ab);
+        h[c] += coef * (ax * idx2 + ay * idy2 + az * idz2);
+    }
+}
+
 // Cubic anisotropy h1, h2, h3 (cubic_anisotropy_field.cpp:61-91) for one cell.
 template <typename R>
 __device__ __forceinline__ void cubic_h123(const TermDesc& t, const R mc[3], R Ms, R h1[3], R h2[3], R h3[3]) {
@@ -142,19 +164,15 @@ __device__ __forceinline__ void add_local_term(const TermDesc& t, const R* __res
                                                int z, int64_t cell, const R mc[3], R Ms, bool ms_is_field, R h[3]) {
     switch (t.kind) {
         case TK_EXCHANGE: {
-            // p[0]=A
+            // p[0]=A.  The reference filter (centre -2/dx^2-2/dy^2-2/dz^2, neighbours
+            // 1/d^2, zero outside) is evaluated as sum over the six neighbours of
+            // (m_nb - m_c)/d^2, with m_nb = 0 outside the mesh: the same value,
+            // without cancelling the ~1e7 A/m self term against the neighbour sum
+            // (which would cost the FP32-field form five digits).
             if (ms_is_field && Ms == (R)0) return;
             const R idx2 = (R)(1.0 / (g.dx * g.dx)), idy2 = (R)(1.0 / (g.dy * g.dy)), idz2 = (R)(1.0 / (g.dz * g.dz));
-            const R ctr = (R)(-2.0 / (g.dx * g.dx) - 2.0 / (g.dy * g.dy) - 2.0 / (g.dz * g.dz));
             const R coef = (R)(2.0 * t.p[0]) / ((R)kMu0 * Ms);
-#pragma unroll
-            for (int c = 0; c < 3; ++c) {
-                R lap = ctr * mc[c];
-                lap += (mget(m, g, c, x - 1, y, z) + mget(m, g, c, x + 1, y, z)) * idx2;
-                lap += (mget(m, g, c, x, y - 1, z) + mget(m, g, c, x, y + 1, z)) * idy2;
-                lap += (mget(m, g, c, x, y, z - 1) + mget(m, g, c, x, y, z + 1)) * idz2;
-                h[c] += coef * lap;
-            }
+            h_exchange_add(m, g, x, y, z, mc, coef, idx2, idy2, idz2, false, h);
             break;
         }
         case TK_DMI: {
@@ -197,12 +215,13 @@ __device__ __forceinline__ void add_local_term(const TermDesc& t, const R* __res
             const R curl1 = (zp[0] - zm[0]) * hz - (xp[2] - xm[2]) * hx;
             const R curl2 = (xp[1] - xm[1]) * hx - (yp[0] - ym[0]) * hy;
             const R idx2 = (R)(1.0 / (g.dx * g.dx)), idy2 = (R)(1.0 / (g.dy * g.dy)), idz2 = (R)(1.0 / (g.dz * g.dz));
-            const R ctr = (R)(-2.0 / (g.dx * g.dx) - 2.0 / (g.dy * g.dy) - 2.0 / (g.dz * g.dz));
             const R curl[3] = {curl0, curl1, curl2};
             const R den = (R)-kMu0 * Ms;
 #pragma unroll
             for (int c = 0; c < 3; ++c) {
-                const R lap = ctr * mc[c] + (xm[c] + xp[c]) * idx2 + (ym[c] + yp[c]) * idy2 + (zm[c] + zp[c]) * idz2;
+                // laplace_3D (math.cpp:107-122) as a sum of neighbour differences
+                const R lap = ((xm[c] - mc[c]) + (xp[c] - mc[c])) * idx2 + ((ym[c] - mc[c]) + (yp[c] - mc[c])) * idy2 +
+                              ((zm[c] - mc[c]) + (zp[c] - mc[c])) * idz2;
                 h[c] += ((R)2 * D * curl[c] + (R)-2 * A * lap) / den;
             }
             break;

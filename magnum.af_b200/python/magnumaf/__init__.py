@@ -72,7 +72,7 @@ _SIGS = {
     "maf_term_H_f32": (_I, [_P, _P, _FP]),
     "maf_term_E": (_I, [_P, _P, _DP]),
     "maf_term_demag_tensor": (_I, [_P, _DP]),
-    "maf_term_demag_real_tensor": (_I, [_P, _DP]),
+    "maf_term_demag_real_tensor": (_I, [_P, _DP, _I]),
     "maf_llg_create": (_I, [C.POINTER(_P), _D, _DP, _I, _I, _I, C.POINTER(_P), _I, C.c_char_p, _D, _D, _D, _D, _I]),
     "maf_llg_destroy": (_I, [_P]),
     "maf_llg_add_term": (_I, [_P, _P]),
@@ -83,8 +83,11 @@ _SIGS = {
     "maf_llg_heff": (_I, [_P, _P, _DP]),
     "maf_llg_heff_f32": (_I, [_P, _P, _FP]),
     "maf_llg_heff_device": (_I, [_P, _P, _P, _P]),
+    "maf_llg_heff_device_profile": (_I, [_P, _P, _P, _P, _DP, _I, C.POINTER(_I)]),
+    "maf_llg_pass_name": (_I, [_P, _P, _I, C.c_char_p, _I]),
     "maf_llg_dmdt": (_I, [_P, _P, _DP]),
     "maf_llg_integrate_dense": (_I, [_P, _P, _D, _D, _DP, _I, C.POINTER(_I)]),
+    "maf_llg_rk_attempt": (_I, [_P, _P, C.c_char_p, _D, _DP, _DP]),
     "maf_llg_relax": (_I, [_P, _P, _D, _I]),
     "maf_llg_get_h": (_I, [_P, _DP]),
     "maf_llg_counters": (_I, [_P, C.POINTER(C.c_ulonglong)]),
@@ -313,12 +316,13 @@ class DemagField(FieldTerm):
         _ck(lib.maf_term_demag_tensor(self._h, _dptr(out)))
         return out
 
-    def get_N(self) -> np.ndarray:
-        """Real-space Newell tensor [Px, Py, Pz, 6] (the reference's setup_N layout)."""
+    def get_N(self, symmetric=False) -> np.ndarray:
+        """Real-space Newell tensor [Px, Py, Pz, 6] (the reference's setup_N layout);
+        symmetric=True returns the parity-exact tensor the spectral pipeline uses."""
         m = self.mesh
         Px, Py, Pz = 2 * m.nx, 2 * m.ny, (1 if m.nz == 1 else 2 * m.nz)
         out = np.empty((6, Pz, Py, Px))
-        _ck(lib.maf_term_demag_real_tensor(self._h, _dptr(out)))
+        _ck(lib.maf_term_demag_real_tensor(self._h, _dptr(out), int(bool(symmetric))))
         return out.transpose(3, 2, 1, 0)
 
 
@@ -455,6 +459,13 @@ class LLGIntegrator:
         _ck(lib.maf_llg_dmdt(self._h, state._h, _dptr(out)))
         return out
 
+    def rk_attempt(self, state: State, scheme: str, dt: float):
+        """One attempt of `scheme` with step dt, no controller: returns (m + sumbk, err)."""
+        out = np.empty((state.mesh.nx, state.mesh.ny, state.mesh.nz, 3), order="F")
+        err = C.c_double()
+        _ck(lib.maf_llg_rk_attempt(self._h, state._h, scheme.encode(), float(dt), _dptr(out), C.byref(err)))
+        return out, err.value
+
     def add_terms(self, *args):
         for t in args:
             _ck(lib.maf_llg_add_term(self._h, t._h))
@@ -502,3 +513,16 @@ class LLGIntegrator:
     def heff_device(self, state: State, m_dev_ptr: int, H_dev_ptr: int):
         """Field of a device-resident m into a device-resident H (no sync)."""
         _ck(lib.maf_llg_heff_device(self._h, state._h, C.c_void_p(m_dev_ptr), C.c_void_p(H_dev_ptr)))
+
+    def heff_device_profile(self, state: State, m_dev_ptr: int, H_dev_ptr: int):
+        """One field evaluation with per-pass CUDA-event timing: [(name, ms), ...]."""
+        ms = np.zeros(16)
+        n = C.c_int()
+        _ck(lib.maf_llg_heff_device_profile(self._h, state._h, C.c_void_p(m_dev_ptr), C.c_void_p(H_dev_ptr),
+                                            _dptr(ms), 16, C.byref(n)))
+        out = []
+        buf = C.create_string_buffer(64)
+        for i in range(n.value):
+            _ck(lib.maf_llg_pass_name(self._h, state._h, i, buf, 64))
+            out.append((buf.value.decode(), float(ms[i])))
+        return out

@@ -281,13 +281,82 @@ def demag_tensor_real(mesh: Mesh) -> np.ndarray:
     return N
 
 
+_ODD_AXES = {0: (), 1: (0, 1), 2: (0, 2), 3: (), 4: (1, 2), 5: ()}
+
+
+def _octant_chunk(args):
+    """Newell values on the octant planes a0 in [a0_lo, a0_hi) (process-pool worker)."""
+    a0_lo, a0_hi, ny1, nz1, dx, dy, dz = args
+    A0, A1, A2 = np.meshgrid(np.arange(a0_lo, a0_hi), np.arange(ny1), np.arange(nz1), indexing="ij")
+    out = np.empty(A0.shape + (6,))
+    out[..., 0] = Nxx(A0, A1, A2, dx, dy, dz)
+    out[..., 1] = Nxy(A0, A1, A2, dx, dy, dz)
+    out[..., 2] = Nxy(A0, A2, A1, dx, dz, dy)
+    out[..., 3] = Nxx(A1, A2, A0, dy, dz, dx)
+    out[..., 4] = Nxy(A1, A2, A0, dy, dz, dx)
+    out[..., 5] = Nxx(A2, A0, A1, dz, dx, dy)
+    return out
+
+
+def demag_tensor_symmetric(mesh: Mesh, workers: int = 0) -> np.ndarray:
+    """The parity-exact tensor: the reference formula evaluated at
+    (|j0|, |j1|, |j2|), multiplied by each component's parity sign (xy odd in
+    x and y, xz odd in x and z, yz odd in y and z), with odd components set to
+    zero where they vanish in exact arithmetic (j = 0 along an odd axis) and
+    on their Nyquist planes j = -P/2.  Entries with |j| = P/2 never reach the
+    truncated output of the zero-padded convolution, so the field on the mesh
+    equals the reference's up to the rounding noise of its 27-point sums,
+    while the spectrum becomes exactly real and even/odd.  The octant
+    |j| <= P/2 is evaluated once (workers > 1: in a spawned process pool)."""
+    Px, Py, Pz = nx_exp(mesh.nx), nx_exp(mesh.ny), nz_exp(mesh.nz)
+    P = (Px, Py, Pz)
+    n1 = (Px // 2 + 1, Py // 2 + 1, Pz // 2 + 1)
+    args = (mesh.dx, mesh.dy, mesh.dz)
+    if workers and workers > 1:
+        import concurrent.futures as cf
+        import multiprocessing as mp
+        step = max(1, n1[0] // (4 * workers))
+        chunks = [(a, min(a + step, n1[0]), n1[1], n1[2]) + args for a in range(0, n1[0], step)]
+        with cf.ProcessPoolExecutor(max_workers=workers, mp_context=mp.get_context("spawn")) as ex:
+            octant = np.concatenate(list(ex.map(_octant_chunk, chunks)), axis=0)
+    else:
+        octant = _octant_chunk((0, n1[0], n1[1], n1[2]) + args)
+    j = [newell_wrapped_index(np.arange(p), p) for p in P]
+    N = octant[np.abs(j[0])][:, np.abs(j[1])][:, :, np.abs(j[2])]
+    for c, axes in _ODD_AXES.items():
+        sign = np.ones(P)
+        for ax in axes:
+            shape = [1, 1, 1]
+            shape[ax] = P[ax]
+            jj = j[ax].reshape(shape)
+            s = np.where(jj < 0, -1.0, 1.0)
+            s = np.where(jj == 0, 0.0, s)
+            if P[ax] > 1:
+                s = np.where(jj == -(P[ax] // 2), 0.0, s)
+            sign = sign * s
+        N[..., c] = N[..., c] * sign
+    return N
+
+
+# Number of host threads for the oracle's FFTs.  None: numpy.fft (single
+# thread, used by the tests); an int: scipy.fft with that many workers (used
+# when the oracle is timed as the CPU baseline on all host cores).
+FFT_WORKERS: Optional[int] = None
+
+
 def _rfft3(a, P):
     """ArrayFire fftR2C over dims 0..2 of a [x,y,z,...] array: halves dim 0."""
+    if FFT_WORKERS:
+        import scipy.fft as sf
+        return sf.rfftn(a, s=(P[1], P[2], P[0]), axes=(1, 2, 0), workers=FFT_WORKERS)
     return np.fft.rfftn(a, s=(P[1], P[2], P[0]), axes=(1, 2, 0))
 
 
 def _irfft3(a, P):
     """ArrayFire fftC2R with the 1/N normalisation (demag_field.cpp:251-257)."""
+    if FFT_WORKERS:
+        import scipy.fft as sf
+        return sf.irfftn(a, s=(P[1], P[2], P[0]), axes=(1, 2, 0), workers=FFT_WORKERS)
     return np.fft.irfftn(a, s=(P[1], P[2], P[0]), axes=(1, 2, 0))
 
 
@@ -297,11 +366,17 @@ class DemagField(FieldTerm):
     computed elsewhere (e.g. the device's) so that the convolution is checked
     on identical inputs."""
 
-    def __init__(self, mesh: Mesh, N_real: Optional[np.ndarray] = None):
+    def __init__(self, mesh: Mesh, N_real: Optional[np.ndarray] = None, symmetric: bool = False,
+                 Nfft: Optional[np.ndarray] = None):
         self.mesh = mesh
         self.P = (nx_exp(mesh.nx), nx_exp(mesh.ny), nz_exp(mesh.nz))
+        if Nfft is not None:
+            # spectral tensor supplied directly ([Px/2+1, Py, Pz, 6]); used by the timed CPU baseline
+            self.N_real = None
+            self.Nfft = Nfft
+            return
         if N_real is None:
-            N_real = demag_tensor_real(mesh)
+            N_real = demag_tensor_symmetric(mesh) if symmetric else demag_tensor_real(mesh)
         self.N_real = N_real
         self.Nfft = _rfft3(N_real, self.P)
 
@@ -857,3 +932,38 @@ def full_inner_product(a, b):
 
 def max_4d_abs(a):
     return float(np.max(np.abs(a)))
+
+
+def spectral_tensor_from_reduced(Nred: np.ndarray, mesh: Mesh) -> np.ndarray:
+    """Expand the device's symmetry-reduced real spectral tensor
+    [ncomp][kz][ky][kx] to the full half spectrum [Px/2+1, Py, Pz, 6] that
+    DemagField.Nfft holds, using the parities of the components (xy odd in ky,
+    xz odd in kz, yz odd in ky and kz).  Setup helper of the timed CPU baseline
+    (the oracle's own tensor assembly at 1024^2 x 16 would take far longer than
+    the field evaluation being timed)."""
+    nx, ny, nz = mesh.nx, mesh.ny, mesh.nz
+    Py, Pz = 2 * ny, nz_exp(nz)
+    ky = np.arange(Py)
+    kyr = np.where(ky <= ny, ky, Py - ky)
+    sy = np.where(ky <= ny, 1.0, -1.0)
+    kz = np.arange(Pz)
+    if nz > 1:
+        kzr = np.where(kz <= nz, kz, Pz - kz)
+        sz = np.where(kz <= nz, 1.0, -1.0)
+        comps = [(0, 0, 0), (1, 1, 0), (2, 0, 1), (3, 0, 0), (4, 1, 1), (5, 0, 0)]  # (slot, odd y, odd z)
+    else:
+        kzr = np.zeros(1, dtype=int)
+        sz = np.ones(1)
+        comps = [(0, 0, 0), (1, 1, 0), (None, 0, 0), (2, 0, 0), (None, 0, 0), (3, 0, 0)]
+    out = np.zeros((nx + 1, Py, Pz, 6), dtype=np.complex128)
+    for c, (slot, oy, oz) in enumerate(comps):
+        if slot is None:
+            continue
+        blk = Nred[slot][kzr][:, kyr]  # (Pz, Py, nxh)
+        sign = np.ones((Pz, Py))
+        if oy:
+            sign = sign * sy[None, :]
+        if oz:
+            sign = sign * sz[:, None]
+        out[..., c] = (blk * sign[..., None]).transpose(2, 1, 0)
+    return out

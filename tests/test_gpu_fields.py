@@ -57,7 +57,11 @@ def test_local_term_fp64(name, mesh_args):
     ref = ot.H_in_Apm(os_)
     assert rel_l2(h, ref) < 1e-12 and rel_max(h, ref) < 1e-12
     e, eref = gt.Energy_in_J(gs), ot.Energy_in_J(os_)
-    assert abs(e - eref) <= 1e-12 * max(abs(eref), 1e-300)
+    # energy scale: sum of |h.m| contributions (the exchange energy of a single cell
+    # is an exact cancellation, so |eref| alone is no scale)
+    dV = om.dx * om.dy * om.dz
+    scale = O.mu0 * 8e5 * float(np.sum(np.abs(ref * os_.m))) * dV
+    assert abs(e - eref) <= 1e-12 * max(abs(eref), scale)
 
 
 @pytest.mark.parametrize("name", list(LOCAL_TERMS))
@@ -147,12 +151,13 @@ def test_ms_field_zero_cells():
 @pytest.mark.parametrize("mesh_args", [(6, 5, 4, 2e-9, 3e-9, 4e-9), (3, 5, 7, 1e-9, 1e-9, 1e-9),
                                        (8, 6, 1, 1e-9, 1e-9, 1e-9), (1, 1, 1, 1e-9, 1e-9, 1e-9)])
 def test_newell_real_tensor(mesh_args):
+    """The device's FP64 Newell tensor (raw reference layout and the parity-exact
+    one the spectral pipeline uses) against the oracle's, entry by entry."""
     gm, om = mesh_pair(*mesh_args)
-    N = M.DemagField(gm).get_N()
-    ref = O.demag_tensor_real(om)
-    # near field: well conditioned
-    scale = np.abs(ref).max()
-    assert np.abs(N - ref).max() < 1e-12 * scale
+    d = M.DemagField(gm)
+    for N, ref in ((d.get_N(), O.demag_tensor_real(om)), (d.get_N(symmetric=True), O.demag_tensor_symmetric(om))):
+        scale = np.abs(ref).max()
+        assert np.abs(N - ref).max() < 1e-12 * scale
 
 
 @pytest.mark.parametrize("mesh_args", [(12, 10, 6, 2e-9, 2e-9, 3e-9), (30, 20, 1, 3e-9, 3e-9, 3e-9),
@@ -163,17 +168,20 @@ def test_demag_fp64_same_tensor(mesh_args):
     gm, om, gs, os_ = _pair_state(mesh_args, seed=9)
     d = M.DemagField(gm)
     h = d.H_in_Apm(gs)
-    ref = O.DemagField(om, N_real=d.get_N()).H_in_Apm(os_)
+    ref = O.DemagField(om, N_real=d.get_N(symmetric=True)).H_in_Apm(os_)
     assert rel_l2(h, ref) < 1e-12 and rel_max(h, ref) < 1e-12
 
 
 @pytest.mark.parametrize("mesh_args,tol", [((8, 6, 2, 2e-9, 2e-9, 3e-9), 1e-12),
-                                           ((16, 12, 1, 2e-9, 2e-9, 1e-9), 1e-12),
-                                           ((20, 16, 4, 3e-9, 3e-9, 3e-9), 1e-10)])
+                                           ((16, 12, 1, 2e-9, 2e-9, 1e-9), 1e-11),
+                                           ((20, 16, 4, 3e-9, 3e-9, 3e-9), 1e-11)])
 def test_demag_fp64_independent(mesh_args, tol):
+    """Device and oracle each assemble the tensor (CUDA vs host libm asinh/atan);
+    the tolerance is the measured rounding noise of the 27-point Newell sums at
+    these sizes (it grows roughly as the fourth power of the mesh side)."""
     gm, om, gs, os_ = _pair_state(mesh_args, seed=10)
     h = M.DemagField(gm).H_in_Apm(gs)
-    ref = O.DemagField(om).H_in_Apm(os_)
+    ref = O.DemagField(om, symmetric=True).H_in_Apm(os_)
     assert rel_l2(h, ref) < tol
 
 
@@ -221,7 +229,7 @@ def test_heff_sum_and_energy_fp64():
     d = M.DemagField(gm)
     hz = (0.01 / O.mu0, -0.02 / O.mu0, 0.005 / O.mu0)
     gterms = [d, M.ExchangeField(1.3e-11), M.CubicAnisotropyField(-1e4), M.ExternalField.uniform(*hz)]
-    oterms = [O.DemagField(om, N_real=d.get_N()), O.ExchangeField(1.3e-11), O.CubicAnisotropyField(-1e4),
+    oterms = [O.DemagField(om, N_real=d.get_N(symmetric=True)), O.ExchangeField(1.3e-11), O.CubicAnisotropyField(-1e4),
               O.ExternalField(np.broadcast_to(np.array(hz), (20, 16, 4, 3)))]
     llg = M.LLGIntegrator(0.01, gterms, "DP45")
     h = llg.H_in_Apm(gs)
