@@ -27,6 +27,7 @@ COMMON = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler",
           "--expt-relaxed-constexpr", "-I" + CSRC, "-I" + INCLUDE]
 SOURCES = {
     "fields.cu": [],
+    "fields_ct.cu": [],
     "llg.cu": [],
     "newell.cu": ["-fmad=false"],
     "capi.cu": [],

@@ -1,0 +1,139 @@
+// Compile-time specialised FFT stages for power-of-two lengths.
+//
+// The transform length, the radix sequence, the number of columns in the tile
+// and the CTA size are template parameters, so every index is a constant
+// expression (shifts and masks), each thread holds exactly kE = 16 complex
+// values in registers per stage, and nothing spills.  Same Stockham
+// formulation as fft_engine.cuh (inputs j + r L/R, twiddle W_{Ns R}^{r (j mod
+// Ns)}, outputs (j - j mod Ns) R + j mod Ns + r Ns), radix 16 as 4 x 4.
+#pragma once
+#include "fft_engine.cuh"
+
+namespace mafb {
+
+constexpr int kE = 16;
+
+template <int... Rs> struct Radices {};
+
+// 16-point DFT as two layers of radix 4 with the W16 twiddles in between.
+template <int DIR, typename R> __host__ __device__ __forceinline__ void bfly16(cplx_t<R>* v) {
+    using C = cplx_t<R>;
+    const R c1 = (R)0.92387953251128675613, s1 = (R)0.38268343236508977173;  // cos, sin (pi/8)
+    const R h = (R)0.70710678118654752440;
+    C a[4][4];
+#pragma unroll
+    for (int n2 = 0; n2 < 4; ++n2) {
+        C t[4] = {v[n2], v[4 + n2], v[8 + n2], v[12 + n2]};
+        bfly4<DIR>(t);
+#pragma unroll
+        for (int k1 = 0; k1 < 4; ++k1) a[n2][k1] = t[k1];
+    }
+    // a[n2][k1] *= W16^(n2 k1), W16 = exp(DIR 2 pi i / 16)
+    const R sd = (R)DIR;
+    const C w1 = mk(c1, sd * s1), w2 = mk(h, sd * h), w3 = mk(s1, sd * c1);
+    a[1][1] = cmul(a[1][1], w1);
+    a[1][2] = cmul(a[1][2], w2);
+    a[1][3] = cmul(a[1][3], w3);
+    a[2][1] = cmul(a[2][1], w2);
+    a[2][2] = cmul_i<DIR>(a[2][2]);
+    a[2][3] = cmul(a[2][3], mk(-h, sd * h));  // W16^6
+    a[3][1] = cmul(a[3][1], w3);
+    a[3][2] = cmul(a[3][2], mk(-h, sd * h));  // W16^6
+    a[3][3] = cmul(a[3][3], mk(-c1, -sd * s1));  // W16^9 = -W16^1
+#pragma unroll
+    for (int k1 = 0; k1 < 4; ++k1) {
+        C t[4] = {a[0][k1], a[1][k1], a[2][k1], a[3][k1]};
+        bfly4<DIR>(t);
+#pragma unroll
+        for (int k2 = 0; k2 < 4; ++k2) v[k1 + 4 * k2] = t[k2];
+    }
+}
+
+template <int RAD, int DIR, typename R> __device__ __forceinline__ void bfly_ct(cplx_t<R>* v) {
+    if constexpr (RAD == 2) {
+        bfly2<DIR>(v[0], v[1]);
+    } else if constexpr (RAD == 4) {
+        bfly4<DIR>(v);
+    } else if constexpr (RAD == 8) {
+        bfly8<DIR, R>(v);
+    } else {
+        static_assert(RAD == 16, "power-of-two radix");
+        bfly16<DIR, R>(v);
+    }
+}
+
+// One stage over NB columns of length L with NT threads.
+template <typename R, int RAD, int DIR, bool BFAST, int L, int NS, int NB, int NT>
+__device__ __forceinline__ void ct_stage(cplx_t<R>* s, int sb, const cplx_t<R>* __restrict__ tw) {
+    using C = cplx_t<R>;
+    constexpr int NBF = L / RAD;
+    constexpr int TOTAL = NBF * NB;
+    constexpr int BPT = (TOTAL + NT - 1) / NT;
+    constexpr int TWST = L / (NS * RAD);
+    C v[BPT][RAD];
+#pragma unroll
+    for (int k = 0; k < BPT; ++k) {
+        const int q = threadIdx.x + k * NT;
+        if (TOTAL % NT == 0 || q < TOTAL) {
+            const int b = BFAST ? q % NB : q / NBF;
+            const int j = BFAST ? q / NB : q % NBF;
+            const int jm = j % NS;
+#pragma unroll
+            for (int r = 0; r < RAD; ++r) {
+                const int i = j + r * NBF;
+                C x = s[BFAST ? spad(i) * NB + b : spad(i) + b * sb];
+                if (NS > 1 && r > 0) {
+                    const C w = tw[r * jm * TWST];
+                    x = DIR < 0 ? cmul(x, w) : cmulc(x, w);
+                }
+                v[k][r] = x;
+            }
+            bfly_ct<RAD, DIR, R>(v[k]);
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < BPT; ++k) {
+        const int q = threadIdx.x + k * NT;
+        if (TOTAL % NT == 0 || q < TOTAL) {
+            const int b = BFAST ? q % NB : q / NBF;
+            const int j = BFAST ? q / NB : q % NBF;
+            const int jm = j % NS;
+            const int d = (j - jm) * RAD + jm;
+#pragma unroll
+            for (int r = 0; r < RAD; ++r) {
+                const int i = d + r * NS;
+                s[BFAST ? spad(i) * NB + b : spad(i) + b * sb] = v[k][r];
+            }
+        }
+    }
+    __syncthreads();
+}
+
+template <typename R, int DIR, bool BFAST, int L, int NS, int NB, int NT, int RAD, int... REST>
+__device__ __forceinline__ void ct_run(cplx_t<R>* s, int sb, const cplx_t<R>* __restrict__ tw) {
+    ct_stage<R, RAD, DIR, BFAST, L, NS, NB, NT>(s, sb, tw);
+    if constexpr (sizeof...(REST) > 0) ct_run<R, DIR, BFAST, L, NS * RAD, NB, NT, REST...>(s, sb, tw);
+}
+
+template <typename R, int DIR, bool BFAST, int L, int NB, int NT, int... RS>
+__device__ __forceinline__ void ct_fft(cplx_t<R>* s, int sb, const cplx_t<R>* __restrict__ tw, Radices<RS...>) {
+    ct_run<R, DIR, BFAST, L, 1, NB, NT, RS...>(s, sb, tw);
+}
+
+// radix sequence per power-of-two length (16 first, smaller radices last)
+template <int L> struct CtPlan;
+template <> struct CtPlan<2> { using T = Radices<2>; };
+template <> struct CtPlan<4> { using T = Radices<4>; };
+template <> struct CtPlan<8> { using T = Radices<8>; };
+template <> struct CtPlan<16> { using T = Radices<16>; };
+template <> struct CtPlan<32> { using T = Radices<16, 2>; };
+template <> struct CtPlan<64> { using T = Radices<16, 4>; };
+template <> struct CtPlan<128> { using T = Radices<16, 8>; };
+template <> struct CtPlan<256> { using T = Radices<16, 16>; };
+template <> struct CtPlan<512> { using T = Radices<16, 16, 2>; };
+template <> struct CtPlan<1024> { using T = Radices<16, 16, 4>; };
+template <> struct CtPlan<2048> { using T = Radices<16, 16, 8>; };
+template <> struct CtPlan<4096> { using T = Radices<16, 16, 16>; };
+
+}  // namespace mafb

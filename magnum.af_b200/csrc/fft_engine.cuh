@@ -52,13 +52,13 @@ template <bool BFAST> struct SLay {
 // ---------------------------------------------------------------------------
 // butterflies: y[k] = sum_r v[r] W_R^{r k}, W_R = exp(DIR*2*pi*i/R)
 // ---------------------------------------------------------------------------
-template <int DIR, typename C> __device__ __forceinline__ void bfly2(C& a, C& b) {
+template <int DIR, typename C> __host__ __device__ __forceinline__ void bfly2(C& a, C& b) {
     C t = a;
     a = cadd(t, b);
     b = csub(t, b);
 }
 
-template <int DIR, typename C> __device__ __forceinline__ void bfly4(C* v) {
+template <int DIR, typename C> __host__ __device__ __forceinline__ void bfly4(C* v) {
     C t0 = cadd(v[0], v[2]);
     C t1 = csub(v[0], v[2]);
     C t2 = cadd(v[1], v[3]);
@@ -69,7 +69,7 @@ template <int DIR, typename C> __device__ __forceinline__ void bfly4(C* v) {
     v[3] = csub(t1, t3);
 }
 
-template <int DIR, typename R> __device__ __forceinline__ void bfly8(cplx_t<R>* v) {
+template <int DIR, typename R> __host__ __device__ __forceinline__ void bfly8(cplx_t<R>* v) {
     using C = cplx_t<R>;
     C e[4] = {v[0], v[2], v[4], v[6]};
     C o[4] = {v[1], v[3], v[5], v[7]};

@@ -23,6 +23,8 @@
 #include <cmath>
 
 #include "engine.hpp"
+#include "epilogue.cuh"
+#include "ct_dispatch.hpp"
 
 namespace mafb {
 
@@ -254,118 +256,6 @@ __global__ void __launch_bounds__(kMaxFftThreads) k_conv(cplx_t<R>* S, const R* 
     }
 }
 
-// ---------------------------------------------------------------------------
-// epilogue shared by the fused x-inverse pass and the standalone local kernel
-// ---------------------------------------------------------------------------
-template <typename R>
-__device__ __forceinline__ R cell_Ms(const MsInfo& ms, int64_t cell) {
-    if (ms.field64) {
-        if constexpr (sizeof(R) == 4) return ms.field32[cell];
-        else return (R)ms.field64[cell];
-    }
-    return (R)ms.Ms;
-}
-
-template <typename R, int EPI>
-__device__ __forceinline__ void epilogue_cell(const Geom& g, int x, int y, int z, int64_t cell,
-                                              const R* __restrict__ m, const MsInfo& ms, const TermList& tl,
-                                              const EpilogueArgs& ep, const R hd[3], double& eacc) {
-    R mc[3];
-    mvec(m, g, cell, mc);
-    const bool msf = ms.field64 != nullptr;
-    const R Ms = cell_Ms<R>(ms, cell);
-    if constexpr (EPI == EPI_EDENS) {
-        const double Msd = msf ? ms.field64[cell] : ms.Ms;
-        for (int it = 0; it < tl.n; ++it) {
-            const TermDesc& t = tl.t[it];
-            R ht[3] = {0, 0, 0};
-            double w = -kMu0 / 2.0;
-            if (t.kind == TK_DEMAG) {
-                ht[0] = hd[0]; ht[1] = hd[1]; ht[2] = hd[2];
-            } else if (t.kind == TK_CUBIC) {
-                R h1[3], h2[3], h3[3];
-                cubic_h123(t, mc, Ms, h1, h2, h3);
-                double e = 0;
-                for (int c = 0; c < 3; ++c)
-                    e += (-1.0 / 4.0 * (double)h1[c] - 1.0 / 6.0 * (double)h2[c] - 1.0 / 8.0 * (double)h3[c]) *
-                         (double)mc[c];
-                eacc += kMu0 * Msd * e;
-                continue;
-            } else if (t.kind == TK_EXCHANGE && ep.edge_exchange) {
-                // h_withedges (exchange_field.cpp:28-60): the zero-padded stencil plus
-                // m/d^2 on each boundary face, i.e. the Neumann Laplacian
-                if (!(msf && Ms == (R)0)) {
-                    const R coef = (R)(2.0 * t.p[0]) / ((R)kMu0 * Ms);
-                    h_exchange_add(m, g, x, y, z, mc, coef, (R)(1.0 / (g.dx * g.dx)), (R)(1.0 / (g.dy * g.dy)),
-                                   (R)(1.0 / (g.dz * g.dz)), true, ht);
-                }
-            } else {
-                add_local_term(t, m, g, x, y, z, cell, mc, Ms, msf, ht);
-                if (t.kind == TK_ZEEMAN) w = -kMu0;
-            }
-            const double hm = (double)ht[0] * (double)mc[0] + (double)ht[1] * (double)mc[1] + (double)ht[2] * (double)mc[2];
-            eacc += w * Msd * hm;
-        }
-    } else {
-        R h[3] = {0, 0, 0};
-        for (int it = 0; it < tl.n; ++it) {
-            const TermDesc& t = tl.t[it];
-            if (t.kind == TK_DEMAG) {
-                h[0] += hd[0]; h[1] += hd[1]; h[2] += hd[2];
-            } else {
-                add_local_term(t, m, g, x, y, z, cell, mc, Ms, msf, h);
-            }
-        }
-        if constexpr (EPI == EPI_H) {
-            R* o = static_cast<R*>(ep.out);
-            o[cell] = h[0];
-            o[g.N + cell] = h[1];
-            o[2 * g.N + cell] = h[2];
-        } else {
-            const double* m64 = ep.llg.m64;
-            const double M0 = m64[cell], M1 = m64[g.N + cell], M2 = m64[2 * g.N + cell];
-            const double H0 = h[0], H1 = h[1], H2 = h[2];
-            const double x0 = M1 * H2 - M2 * H1;
-            const double x1 = M2 * H0 - M0 * H2;
-            const double x2 = M0 * H1 - M1 * H0;
-            const double d0 = M1 * x2 - M2 * x1;
-            const double d1 = M2 * x0 - M0 * x2;
-            const double d2 = M0 * x1 - M1 * x0;
-            double cp = ep.llg.c_prec, cd = ep.llg.c_damp;
-            if (ep.llg.alpha) {
-                const double a = ep.llg.alpha[cell];
-                cp = -kGamma / (1. + a * a);
-                cd = -a * kGamma / (1. + a * a);
-            }
-            double k0, k1, k2;
-            if (ep.llg.dissipation_only) {
-                k0 = cd * d0; k1 = cd * d1; k2 = cd * d2;
-            } else {
-                k0 = cp * x0 + cd * d0; k1 = cp * x1 + cd * d1; k2 = cp * x2 + cd * d2;
-            }
-            double* o = static_cast<double*>(ep.out);
-            const double sc = ep.llg.scale;
-            o[cell] = sc * k0;
-            o[g.N + cell] = sc * k1;
-            o[2 * g.N + cell] = sc * k2;
-        }
-    }
-}
-
-__device__ __forceinline__ void block_sum_store(double v, double* partials) {
-    __shared__ double red[32];
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    if (lane == 0) red[wid] = v;
-    __syncthreads();
-    if (wid == 0) {
-        const int nw = (blockDim.x + 31) >> 5;
-        double s = lane < nw ? red[lane] : 0.0;
-        for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-        if (lane == 0) partials[blockIdx.x] = s;
-    }
-}
-
 // x-inverse C2R of the half spectrum (3 components of nbr rows), scale, then
 // the per-cell epilogue with the local terms.
 template <typename R, int EPI>
@@ -506,6 +396,7 @@ template <typename R> static int tile_target() { return sizeof(R) == 4 ? 8192 : 
 template <typename R>
 static void launch_xfwd(const R* in, int n_in, int64_t rows, int64_t rows_pc, const R* msf, R ms, cplx_t<R>* out,
                         int pitch, int Px, Twiddles& tw, cudaStream_t st) {
+    if (ct_xfwd<R>(in, n_in, rows, rows_pc, msf, ms, out, pitch, Px, tw, st)) return;
     const bool f64 = sizeof(R) == 8;
     const int Lc = Px / 2;
     FFTPlan plan = make_fft_plan(Lc, tw.get(Lc, f64));
@@ -529,6 +420,7 @@ static void launch_xfwd(const R* in, int n_in, int64_t rows, int64_t rows_pc, co
 template <typename R, int DIR>
 static void launch_cols(const cplx_t<R>* in, cplx_t<R>* out, int L, int n_in, int n_out, int ncols, int64_t in_si,
                         int64_t out_si, int64_t in_sbat, int64_t out_sbat, int nbat, Twiddles& tw, cudaStream_t st) {
+    if (ct_cols<R, DIR>(in, out, L, n_in, n_out, ncols, in_si, out_si, in_sbat, out_sbat, nbat, tw, st)) return;
     const bool f64 = sizeof(R) == 8;
     FFTPlan plan = make_fft_plan(L, tw.get(L, f64));
     int nb = pick_nb(L, tile_target<R>(), ncols, 32);
@@ -660,7 +552,7 @@ template <typename R> void Demag::forward_conv(const R* m, const MsInfo& ms, cud
                            (int64_t)Py() * pitch_, 3 * nz, tw_, st);
         if (marks) marks->mark(st, "y_fwd");
         // pass 3: z forward . tensor . z inverse, in place on S2
-        {
+        if (!ct_convz<R>(s2, Nr, nz, ny, nxh(), pitch_, tw_, st)) {
             const int L = Pz();
             FFTPlan fp = make_fft_plan(L, tw_.get(L, f64));
             FFTPlan ip = fp;
@@ -686,6 +578,10 @@ template <typename R> void Demag::forward_conv(const R* m, const MsInfo& ms, cud
         if (marks) marks->mark(st, "y_inv");
     } else {
         // pass 2 (2-D): y forward . tensor . y inverse, in place on S1
+        if (ct_convy<R>(s1, Nr, ny, nxh(), pitch_, tw_, st)) {
+            if (marks) marks->mark(st, "y_conv");
+            return;
+        }
         const int L = Py();
         FFTPlan fp = make_fft_plan(L, tw_.get(L, f64));
         int nb = pick_nb(3 * L, tile_target<R>(), nxh(), 64);
@@ -713,6 +609,13 @@ void Demag::inverse_x_epilogue(const R* m, const MsInfo& ms, const TermList& tl,
                                cudaStream_t st, int* nblocks_out, PassMarks* marks) {
     const bool f64 = sizeof(R) == 8;
     const int Lc = md_.nx;
+    {
+        const R scale = (R)(1.0 / ((double)Px() * Py() * Pz()));
+        if (ct_xinv<R>(S1<R>(), pitch_, Px(), tw_, md_.geom(), scale, m, ms, tl, ep, st, nblocks_out)) {
+            if (marks) marks->mark(st, "x_inv_local");
+            return;
+        }
+    }
     FFTPlan plan = make_fft_plan(Lc, tw_.get(Lc, f64));
     const int64_t rows_pc = (int64_t)md_.ny * md_.nz;
     int nbr = pick_nb(3 * Lc, tile_target<R>(), (int)std::min<int64_t>(rows_pc, 1 << 20), 32);

@@ -1,0 +1,525 @@
+// Demag pass kernels specialised at compile time for power-of-two transform
+// lengths 8..4096 (every configuration of the benchmarks).  Same data flow and
+// arithmetic as the generic kernels in fields.cu; the transform length, radix
+// sequence, tile width and CTA size are constants, each thread keeps 16
+// complex values in registers per FFT stage, global loads are issued as a
+// batch into registers before they are written to shared memory, and the
+// z convolution handles the rows ky and Py - ky in one CTA so that the stored
+// tensor quadrant is read from HBM once.
+#include "ct_dispatch.hpp"
+#include "epilogue.cuh"
+#include "fft_ct.cuh"
+
+namespace mafb {
+
+// ------------------------------------------------------------------ x forward
+template <typename R, int LC, int NB, int NT>
+__global__ void __launch_bounds__(NT) k_xfwd_ct(const R* __restrict__ in, int n_in, int64_t rows, int64_t rows_pc,
+                                                const R* __restrict__ msf, R ms, cplx_t<R>* __restrict__ out,
+                                                int pitch, const cplx_t<R>* __restrict__ tw,
+                                                const cplx_t<R>* __restrict__ twP) {
+    using C = cplx_t<R>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C* s = reinterpret_cast<C*>(smem_raw);
+    constexpr int SB = (LC - 1) + ((LC - 1) >> 4) + 1;
+    constexpr int E = LC * NB / NT;
+    static_assert(LC * NB % NT == 0, "tile");
+    const int64_t r0 = (int64_t)blockIdx.x * NB;
+    C v[E];
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+        const int idx = threadIdx.x + e * NT;
+        const int b = idx / LC;
+        const int k = idx % LC;
+        const int64_t row = r0 + b;
+        R a = 0, c = 0;
+        if (row < rows) {
+            const R* rp = in + row * n_in;
+            const int x0 = 2 * k, x1 = 2 * k + 1;
+            if (x0 < n_in) a = rp[x0];
+            if (x1 < n_in) c = rp[x1];
+            if (msf) {
+                const R* mp = msf + (row % rows_pc) * n_in;
+                if (x0 < n_in) a *= mp[x0];
+                if (x1 < n_in) c *= mp[x1];
+            } else {
+                a *= ms;
+                c *= ms;
+            }
+        }
+        v[e] = mk(a, c);
+    }
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+        const int idx = threadIdx.x + e * NT;
+        s[spad(idx % LC) + (idx / LC) * SB] = v[e];
+    }
+    __syncthreads();
+    ct_fft<R, -1, false, LC, NB, NT>(s, SB, tw, typename CtPlan<LC>::T());
+    const R half = (R)0.5;
+    for (int idx = threadIdx.x; idx < NB * (LC + 1); idx += NT) {
+        const int b = idx / (LC + 1);
+        const int k = idx - b * (LC + 1);
+        const int64_t row = r0 + b;
+        if (row >= rows) continue;
+        const C Zk = s[spad(k == LC ? 0 : k) + b * SB];
+        const C Zm = s[spad(k == 0 ? 0 : LC - k) + b * SB];
+        const C E_ = cscale(cadd(Zk, cconj(Zm)), half);
+        const C O = cscale(cmul_i<-1>(csub(Zk, cconj(Zm))), half);
+        out[row * pitch + k] = cadd(E_, cmul(twP[k], O));
+    }
+}
+
+// ------------------------------------------------------------ strided columns
+template <typename R, int DIR, int L, int NB, int NT>
+__global__ void __launch_bounds__(NT) k_cols_ct(const cplx_t<R>* in, cplx_t<R>* out, int n_in, int n_out, int ncols,
+                                                int64_t in_si, int64_t out_si, int64_t in_sbat, int64_t out_sbat,
+                                                const cplx_t<R>* __restrict__ tw) {
+    using C = cplx_t<R>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C* s = reinterpret_cast<C*>(smem_raw);
+    constexpr int E = L * NB / NT;
+    static_assert(L * NB % NT == 0, "tile");
+    const int c0 = blockIdx.x * NB;
+    const C* ib = in + (int64_t)blockIdx.y * in_sbat + c0;
+    C* ob = out + (int64_t)blockIdx.y * out_sbat + c0;
+    const int ncv = min(NB, ncols - c0);
+    C v[E];
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+        const int idx = threadIdx.x + e * NT;
+        const int i = idx / NB;
+        const int b = idx % NB;
+        C x = mk((R)0, (R)0);
+        if (i < n_in && b < ncv) x = ib[i * in_si + b];
+        v[e] = x;
+    }
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+        const int idx = threadIdx.x + e * NT;
+        s[spad(idx / NB) * NB + idx % NB] = v[e];
+    }
+    __syncthreads();
+    ct_fft<R, DIR, true, L, NB, NT>(s, 0, tw, typename CtPlan<L>::T());
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+        const int idx = threadIdx.x + e * NT;
+        const int i = idx / NB;
+        const int b = idx % NB;
+        if (i < n_out && b < ncv) ob[i * out_si + b] = s[spad(i) * NB + b];
+    }
+}
+
+// -------------------------------------------------- z convolution (3-D meshes)
+// CTA (kx tile, ky) with ky in [0, ny]: rows ky and Py - ky (same tensor quadrant
+// row, sign of Nxy and Nyz flipped for the second); ky = 0 and ky = ny are
+// their own mirrors and run alone.
+template <typename R, int L, int NB, int NT>
+__global__ void __launch_bounds__(NT) k_convz_ct(cplx_t<R>* S, const R* __restrict__ Nred, int nz, int ny, int nxh,
+                                                 int pitch, const cplx_t<R>* __restrict__ tw) {
+    using C = cplx_t<R>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C* s = reinterpret_cast<C*>(smem_raw);
+    constexpr int NC = 6 * NB;  // columns: (row, comp, b)
+    constexpr int E = L * NC / NT;
+    static_assert(L * NC % NT == 0, "tile");
+    const int Py = 2 * ny;
+    const int ky = blockIdx.y;
+    const bool two = ky != 0 && ky != ny;
+    const int ky2 = Py - ky;
+    const int c0 = blockIdx.x * NB;
+    const int ncv = min(NB, nxh - c0);
+    const int64_t si = (int64_t)Py * pitch;        // z stride
+    const int64_t cs = (int64_t)nz * Py * pitch;   // component stride
+    C v[E];
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+        const int idx = threadIdx.x + e * NT;
+        const int i = idx / NC;
+        const int col = idx % NC;
+        const int row = col / (3 * NB);
+        const int comp = (col / NB) % 3;
+        const int b = col % NB;
+        C x = mk((R)0, (R)0);
+        if (i < nz && b < ncv && (row == 0 || two))
+            x = S[comp * cs + i * si + (int64_t)(row ? ky2 : ky) * pitch + c0 + b];
+        v[e] = x;
+    }
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+        const int idx = threadIdx.x + e * NT;
+        s[spad(idx / NC) * NC + idx % NC] = v[e];
+    }
+    __syncthreads();
+    ct_fft<R, -1, true, L, NC, NT>(s, 0, tw, typename CtPlan<L>::T());
+    const int Pz = 2 * nz;
+    const int64_t tcs = (int64_t)(nz + 1) * (ny + 1) * nxh;
+    for (int idx = threadIdx.x; idx < L * NB; idx += NT) {
+        const int kz = idx / NB;
+        const int b = idx % NB;
+        if (b >= ncv) continue;
+        const int kzr = kz <= nz ? kz : Pz - kz;
+        const R sz = kz <= nz ? (R)1 : (R)-1;
+        const int64_t o = ((int64_t)kzr * (ny + 1) + ky) * nxh + c0 + b;
+        const R Nxx = Nred[o], Nxy = Nred[tcs + o], Nxz = sz * Nred[2 * tcs + o];
+        const R Nyy = Nred[3 * tcs + o], Nyz = sz * Nred[4 * tcs + o], Nzz = Nred[5 * tcs + o];
+#pragma unroll
+        for (int row = 0; row < 2; ++row) {
+            if (row == 1 && !two) break;
+            const R sy = row ? (R)-1 : (R)1;
+            const int base = spad(kz) * NC + row * 3 * NB + b;
+            const C mx = s[base], my = s[base + NB], mz = s[base + 2 * NB];
+            const R xy = sy * Nxy, yz = sy * Nyz;
+            s[base] = cadd(cadd(cscale(mx, Nxx), cscale(my, xy)), cscale(mz, Nxz));
+            s[base + NB] = cadd(cadd(cscale(mx, xy), cscale(my, Nyy)), cscale(mz, yz));
+            s[base + 2 * NB] = cadd(cadd(cscale(mx, Nxz), cscale(my, yz)), cscale(mz, Nzz));
+        }
+    }
+    __syncthreads();
+    ct_fft<R, 1, true, L, NC, NT>(s, 0, tw, typename CtPlan<L>::T());
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+        const int idx = threadIdx.x + e * NT;
+        const int i = idx / NC;
+        const int col = idx % NC;
+        const int row = col / (3 * NB);
+        const int comp = (col / NB) % 3;
+        const int b = col % NB;
+        if (i < nz && b < ncv && (row == 0 || two))
+            S[comp * cs + i * si + (int64_t)(row ? ky2 : ky) * pitch + c0 + b] = s[spad(i) * NC + col];
+    }
+}
+
+// -------------------------------------------------- y convolution (nz == 1)
+template <typename R, int L, int NB, int NT>
+__global__ void __launch_bounds__(NT) k_convy_ct(cplx_t<R>* S, const R* __restrict__ Nred, int ny, int nxh, int pitch,
+                                                 const cplx_t<R>* __restrict__ tw) {
+    using C = cplx_t<R>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C* s = reinterpret_cast<C*>(smem_raw);
+    constexpr int NC = 3 * NB;
+    constexpr int E = L * NC / NT;
+    static_assert(L * NC % NT == 0, "tile");
+    const int c0 = blockIdx.x * NB;
+    const int ncv = min(NB, nxh - c0);
+    const int64_t cs = (int64_t)ny * pitch;
+    C v[E];
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+        const int idx = threadIdx.x + e * NT;
+        const int i = idx / NC;
+        const int col = idx % NC;
+        const int comp = col / NB;
+        const int b = col % NB;
+        C x = mk((R)0, (R)0);
+        if (i < ny && b < ncv) x = S[comp * cs + (int64_t)i * pitch + c0 + b];
+        v[e] = x;
+    }
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+        const int idx = threadIdx.x + e * NT;
+        s[spad(idx / NC) * NC + idx % NC] = v[e];
+    }
+    __syncthreads();
+    ct_fft<R, -1, true, L, NC, NT>(s, 0, tw, typename CtPlan<L>::T());
+    const int64_t tcs = (int64_t)(ny + 1) * nxh;
+    for (int idx = threadIdx.x; idx < L * NB; idx += NT) {
+        const int ky = idx / NB;
+        const int b = idx % NB;
+        if (b >= ncv) continue;
+        const int kyr = ky <= ny ? ky : L - ky;
+        const R sy = ky <= ny ? (R)1 : (R)-1;
+        const int64_t o = (int64_t)kyr * nxh + c0 + b;
+        const R Nxx = Nred[o], Nxy = sy * Nred[tcs + o], Nyy = Nred[2 * tcs + o], Nzz = Nred[3 * tcs + o];
+        const int base = spad(ky) * NC + b;
+        const C mx = s[base], my = s[base + NB], mz = s[base + 2 * NB];
+        s[base] = cadd(cscale(mx, Nxx), cscale(my, Nxy));
+        s[base + NB] = cadd(cscale(mx, Nxy), cscale(my, Nyy));
+        s[base + 2 * NB] = cscale(mz, Nzz);
+    }
+    __syncthreads();
+    ct_fft<R, 1, true, L, NC, NT>(s, 0, tw, typename CtPlan<L>::T());
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+        const int idx = threadIdx.x + e * NT;
+        const int i = idx / NC;
+        const int col = idx % NC;
+        const int comp = col / NB;
+        const int b = col % NB;
+        if (i < ny && b < ncv) S[comp * cs + (int64_t)i * pitch + c0 + b] = s[spad(i) * NC + col];
+    }
+}
+
+// --------------------------------------------------- x inverse + epilogue
+template <typename R, int EPI, int LC, int NBR, int NT>
+__global__ void __launch_bounds__(NT) k_xinv_ct(const cplx_t<R>* __restrict__ S1, int pitch,
+                                                const cplx_t<R>* __restrict__ tw, const cplx_t<R>* __restrict__ twP,
+                                                Geom g, R scale, const R* __restrict__ m, MsInfo ms, TermList tl,
+                                                EpilogueArgs ep) {
+    using C = cplx_t<R>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C* s = reinterpret_cast<C*>(smem_raw);
+    constexpr int NC = 3 * NBR;
+    constexpr int SB = (LC - 1) + ((LC - 1) >> 4) + 1;
+    constexpr int E = LC * NC / NT;
+    static_assert(LC * NC % NT == 0, "tile");
+    const int64_t rows_pc = (int64_t)g.ny * g.nz;
+    const int64_t ry0 = (int64_t)blockIdx.x * NBR;
+    C v[E];
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+        const int idx = threadIdx.x + e * NT;
+        const int cb = idx / LC;
+        const int k = idx % LC;
+        const int comp = cb / NBR;
+        const int64_t ry = ry0 + cb % NBR;
+        C Z = mk((R)0, (R)0);
+        if (ry < rows_pc) {
+            const C* rp = S1 + (comp * rows_pc + ry) * pitch;
+            const C Xk = rp[k];
+            const C Xm = rp[LC - k];
+            const C E_ = cadd(Xk, cconj(Xm));
+            const C O = cmulc(csub(Xk, cconj(Xm)), twP[k]);
+            Z = cadd(E_, cmul_i<1>(O));
+        }
+        v[e] = Z;
+    }
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+        const int idx = threadIdx.x + e * NT;
+        s[spad(idx % LC) + (idx / LC) * SB] = v[e];
+    }
+    __syncthreads();
+    ct_fft<R, 1, false, LC, NC, NT>(s, SB, tw, typename CtPlan<LC>::T());
+    double eacc = 0;
+    for (int idx = threadIdx.x; idx < NBR * g.nx; idx += NT) {
+        const int b = idx / g.nx;
+        const int x = idx - b * g.nx;
+        const int64_t ry = ry0 + b;
+        if (ry >= rows_pc) continue;
+        const int z = (int)(ry / g.ny);
+        const int y = (int)(ry - (int64_t)z * g.ny);
+        const int64_t cell = ry * g.nx + x;
+        R hd[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const C val = s[spad(x >> 1) + (c * NBR + b) * SB];
+            hd[c] = scale * ((x & 1) ? val.y : val.x);
+        }
+        epilogue_cell<R, EPI>(g, x, y, z, cell, m, ms, tl, ep, hd, eacc);
+    }
+    if constexpr (EPI == EPI_EDENS) block_sum_store(eacc, ep.partials);
+}
+
+// ------------------------------------------------------------------ dispatch
+template <typename K> static void ct_smem(K kernel, size_t bytes) {
+    if (bytes > 48 * 1024) MAF_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+}
+
+// tile widths: about 4096 (FP32) / 2048 (FP64) complex values per CTA for the
+// x passes, 8192 / 4096 for the column passes (a 32-byte row segment at least)
+template <typename R> constexpr int kTileX = sizeof(R) == 4 ? 4096 : 2048;
+template <typename R> constexpr int kTileC = sizeof(R) == 4 ? 8192 : 4096;
+constexpr int cmax(int a, int b) { return a > b ? a : b; }
+constexpr int cmin(int a, int b) { return a < b ? a : b; }
+constexpr int pow2floor(int x) {
+    int p = 1;
+    while (p * 2 <= x) p *= 2;
+    return p;
+}
+
+template <typename R, int LC>
+static void xfwd_L(const R* in, int n_in, int64_t rows, int64_t rows_pc, const R* msf, R ms, cplx_t<R>* out, int pitch,
+                   const void* tw, const void* twP, cudaStream_t st) {
+    constexpr int NB = pow2floor(cmax(1, kTileX<R> / LC));
+    constexpr int NT = LC * NB / kE;
+    static_assert(NT <= kMaxFftThreads, "CTA size");
+    constexpr int SB = (LC - 1) + ((LC - 1) >> 4) + 1;
+    const size_t smem = sizeof(cplx_t<R>) * (size_t)NB * SB;
+    auto k = k_xfwd_ct<R, LC, NB, NT>;
+    ct_smem(k, smem);
+    k<<<(unsigned)ceil_div(rows, NB), NT, smem, st>>>(in, n_in, rows, rows_pc, msf, ms, out, pitch,
+                                                       static_cast<const cplx_t<R>*>(tw),
+                                                       static_cast<const cplx_t<R>*>(twP));
+    MAF_LAUNCH_CHECK();
+}
+
+template <typename R, int DIR, int L>
+static void cols_L(const cplx_t<R>* in, cplx_t<R>* out, int n_in, int n_out, int ncols, int64_t in_si, int64_t out_si,
+                   int64_t in_sbat, int64_t out_sbat, int nbat, const void* tw, cudaStream_t st) {
+    constexpr int NB = pow2floor(cmin(32, cmax(1, kTileC<R> / L)));
+    constexpr int NT = L * NB / kE;
+    static_assert(NT <= kMaxFftThreads, "CTA size");
+    const size_t smem = sizeof(cplx_t<R>) * (size_t)NB * ((L - 1) + ((L - 1) >> 4) + 1);
+    auto k = k_cols_ct<R, DIR, L, NB, NT>;
+    ct_smem(k, smem);
+    dim3 grid((unsigned)ceil_div(ncols, NB), (unsigned)nbat);
+    k<<<grid, NT, smem, st>>>(in, out, n_in, n_out, ncols, in_si, out_si, in_sbat, out_sbat,
+                              static_cast<const cplx_t<R>*>(tw));
+    MAF_LAUNCH_CHECK();
+}
+
+template <typename R, int L>
+static void convz_L(cplx_t<R>* S, const R* Nred, int nz, int ny, int nxh, int pitch, const void* tw, cudaStream_t st) {
+    constexpr int NB = pow2floor(cmin(32, cmax(1, kTileC<R> / (6 * L))));
+    constexpr int NT = L * 6 * NB / kE;
+    static_assert(NT <= kMaxFftThreads, "CTA size");
+    const size_t smem = sizeof(cplx_t<R>) * (size_t)6 * NB * ((L - 1) + ((L - 1) >> 4) + 1);
+    auto k = k_convz_ct<R, L, NB, NT>;
+    ct_smem(k, smem);
+    dim3 grid((unsigned)ceil_div(nxh, NB), (unsigned)(ny + 1));
+    k<<<grid, NT, smem, st>>>(S, Nred, nz, ny, nxh, pitch, static_cast<const cplx_t<R>*>(tw));
+    MAF_LAUNCH_CHECK();
+}
+
+template <typename R, int L>
+static void convy_L(cplx_t<R>* S, const R* Nred, int ny, int nxh, int pitch, const void* tw, cudaStream_t st) {
+    constexpr int NB = pow2floor(cmin(32, cmax(1, kTileC<R> / (3 * L))));
+    constexpr int NT0 = L * 3 * NB / kE;
+    static_assert(NT0 >= 1 && NT0 <= kMaxFftThreads, "CTA size");
+    const size_t smem = sizeof(cplx_t<R>) * (size_t)3 * NB * ((L - 1) + ((L - 1) >> 4) + 1);
+    auto k = k_convy_ct<R, L, NB, NT0>;
+    ct_smem(k, smem);
+    k<<<(unsigned)ceil_div(nxh, NB), NT0, smem, st>>>(S, Nred, ny, nxh, pitch, static_cast<const cplx_t<R>*>(tw));
+    MAF_LAUNCH_CHECK();
+}
+
+template <typename R, int LC>
+static void xinv_L(const cplx_t<R>* S1, int pitch, const void* tw, const void* twP, const Geom& g, R scale, const R* m,
+                   const MsInfo& ms, const TermList& tl, const EpilogueArgs& ep, cudaStream_t st, int* nblocks) {
+    constexpr int NBR = pow2floor(cmax(1, kTileC<R> / (3 * LC)));
+    constexpr int NC = 3 * NBR;
+    constexpr int NT = LC * NC / kE;
+    static_assert(NT <= kMaxFftThreads, "CTA size");
+    constexpr int SB = (LC - 1) + ((LC - 1) >> 4) + 1;
+    const size_t smem = sizeof(cplx_t<R>) * (size_t)NC * SB;
+    const int64_t rows_pc = (int64_t)g.ny * g.nz;
+    const unsigned blocks = (unsigned)ceil_div(rows_pc, NBR);
+    if (nblocks) *nblocks = (int)blocks;
+    const auto* t = static_cast<const cplx_t<R>*>(tw);
+    const auto* tp = static_cast<const cplx_t<R>*>(twP);
+    switch (ep.kind) {
+        case EPI_H: {
+            auto k = k_xinv_ct<R, EPI_H, LC, NBR, NT>;
+            ct_smem(k, smem);
+            k<<<blocks, NT, smem, st>>>(S1, pitch, t, tp, g, scale, m, ms, tl, ep);
+            break;
+        }
+        case EPI_LLG: {
+            auto k = k_xinv_ct<R, EPI_LLG, LC, NBR, NT>;
+            ct_smem(k, smem);
+            k<<<blocks, NT, smem, st>>>(S1, pitch, t, tp, g, scale, m, ms, tl, ep);
+            break;
+        }
+        default: {
+            auto k = k_xinv_ct<R, EPI_EDENS, LC, NBR, NT>;
+            ct_smem(k, smem);
+            k<<<blocks, NT, smem, st>>>(S1, pitch, t, tp, g, scale, m, ms, tl, ep);
+            break;
+        }
+    }
+    MAF_LAUNCH_CHECK();
+}
+
+#define MAF_CT_SWITCH(L, CALL) \
+    switch (L) {               \
+        case 16: CALL(16); return true;     \
+        case 32: CALL(32); return true;     \
+        case 64: CALL(64); return true;     \
+        case 128: CALL(128); return true;   \
+        case 256: CALL(256); return true;   \
+        case 512: CALL(512); return true;   \
+        case 1024: CALL(1024); return true; \
+        case 2048: CALL(2048); return true; \
+        case 4096: CALL(4096); return true; \
+        default: return false;              \
+    }
+
+template <typename R>
+bool ct_xfwd(const R* in, int n_in, int64_t rows, int64_t rows_pc, const R* msf, R ms, cplx_t<R>* out, int pitch,
+             int Px, Twiddles& tw, cudaStream_t st) {
+    const int LC = Px / 2;
+    const bool f64 = sizeof(R) == 8;
+#define X(N) xfwd_L<R, N>(in, n_in, rows, rows_pc, msf, ms, out, pitch, tw.get(N, f64), tw.get(Px, f64), st)
+    MAF_CT_SWITCH(LC, X)
+#undef X
+}
+
+template <typename R, int DIR>
+bool ct_cols(const cplx_t<R>* in, cplx_t<R>* out, int L, int n_in, int n_out, int ncols, int64_t in_si, int64_t out_si,
+             int64_t in_sbat, int64_t out_sbat, int nbat, Twiddles& tw, cudaStream_t st) {
+    const bool f64 = sizeof(R) == 8;
+#define X(N) cols_L<R, DIR, N>(in, out, n_in, n_out, ncols, in_si, out_si, in_sbat, out_sbat, nbat, tw.get(N, f64), st)
+    MAF_CT_SWITCH(L, X)
+#undef X
+}
+
+template <typename R>
+bool ct_convz(cplx_t<R>* S, const R* Nred, int nz, int ny, int nxh, int pitch, Twiddles& tw, cudaStream_t st) {
+    const bool f64 = sizeof(R) == 8;
+    const int L = 2 * nz;
+#define X(N) convz_L<R, N>(S, Nred, nz, ny, nxh, pitch, tw.get(N, f64), st)
+    switch (L) {
+        case 8: X(8); return true;
+        case 16: X(16); return true;
+        case 32: X(32); return true;
+        case 64: X(64); return true;
+        default: return false;
+    }
+#undef X
+}
+
+template <typename R>
+bool ct_convy(cplx_t<R>* S, const R* Nred, int ny, int nxh, int pitch, Twiddles& tw, cudaStream_t st) {
+    const bool f64 = sizeof(R) == 8;
+    const int L = 2 * ny;
+#define X(N) convy_L<R, N>(S, Nred, ny, nxh, pitch, tw.get(N, f64), st)
+    switch (L) {
+        case 16: X(16); return true;
+        case 32: X(32); return true;
+        case 64: X(64); return true;
+        case 128: X(128); return true;
+        case 256: X(256); return true;
+        case 512: X(512); return true;
+        case 1024: X(1024); return true;
+        case 2048: X(2048); return true;
+        default: return false;
+    }
+#undef X
+}
+
+template <typename R>
+bool ct_xinv(const cplx_t<R>* S1, int pitch, int Px, Twiddles& tw, const Geom& g, R scale, const R* m,
+             const MsInfo& ms, const TermList& tl, const EpilogueArgs& ep, cudaStream_t st, int* nblocks) {
+    const int LC = Px / 2;
+    const bool f64 = sizeof(R) == 8;
+#define X(N) xinv_L<R, N>(S1, pitch, tw.get(N, f64), tw.get(Px, f64), g, scale, m, ms, tl, ep, st, nblocks)
+    switch (LC) {
+        case 16: X(16); return true;
+        case 32: X(32); return true;
+        case 64: X(64); return true;
+        case 128: X(128); return true;
+        case 256: X(256); return true;
+        case 512: X(512); return true;
+        case 1024: X(1024); return true;
+        case 2048: X(2048); return true;
+        default: return false;
+    }
+#undef X
+}
+
+#define MAF_INST(R)                                                                                                   \
+    template bool ct_xfwd<R>(const R*, int, int64_t, int64_t, const R*, R, cplx_t<R>*, int, int, Twiddles&,          \
+                             cudaStream_t);                                                                          \
+    template bool ct_cols<R, -1>(const cplx_t<R>*, cplx_t<R>*, int, int, int, int, int64_t, int64_t, int64_t,        \
+                                 int64_t, int, Twiddles&, cudaStream_t);                                             \
+    template bool ct_cols<R, 1>(const cplx_t<R>*, cplx_t<R>*, int, int, int, int, int64_t, int64_t, int64_t, int64_t, \
+                                int, Twiddles&, cudaStream_t);                                                       \
+    template bool ct_convz<R>(cplx_t<R>*, const R*, int, int, int, int, Twiddles&, cudaStream_t);                    \
+    template bool ct_convy<R>(cplx_t<R>*, const R*, int, int, int, Twiddles&, cudaStream_t);                         \
+    template bool ct_xinv<R>(const cplx_t<R>*, int, int, Twiddles&, const Geom&, R, const R*, const MsInfo&,          \
+                             const TermList&, const EpilogueArgs&, cudaStream_t, int*);
+MAF_INST(float)
+MAF_INST(double)
+
+}  // namespace mafb

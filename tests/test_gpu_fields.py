@@ -162,9 +162,13 @@ def test_newell_real_tensor(mesh_args):
 
 @pytest.mark.parametrize("mesh_args", [(12, 10, 6, 2e-9, 2e-9, 3e-9), (30, 20, 1, 3e-9, 3e-9, 3e-9),
                                        (3, 5, 7, 1e-9, 1e-9, 1e-9), (1, 1, 1, 1e-9, 1e-9, 1e-9),
-                                       (1, 7, 3, 1e-9, 2e-9, 3e-9), (25, 1, 1, 1e-9, 1e-9, 1e-9)])
+                                       (1, 7, 3, 1e-9, 2e-9, 3e-9), (25, 1, 1, 1e-9, 1e-9, 1e-9),
+                                       (16, 8, 4, 2e-9, 3e-9, 4e-9), (32, 16, 1, 3e-9, 3e-9, 2e-9),
+                                       (64, 32, 16, 3e-9, 3e-9, 3e-9), (8, 64, 8, 1e-9, 2e-9, 1e-9)])
 def test_demag_fp64_same_tensor(mesh_args):
-    """Convolution parity on identical inputs: the oracle uses the device's tensor."""
+    """Convolution parity on identical inputs: the oracle uses the device's tensor.
+    Power-of-two meshes run the compile-time specialised passes, the others the
+    generic mixed-radix ones."""
     gm, om, gs, os_ = _pair_state(mesh_args, seed=9)
     d = M.DemagField(gm)
     h = d.H_in_Apm(gs)
@@ -213,7 +217,8 @@ def test_demag_energy_cube_with_airbox():
     assert abs(E - analytic) < (E + analytic) / 2 * 5.3e-8
 
 
-@pytest.mark.parametrize("mesh_args", [(32, 24, 4, 3e-9, 3e-9, 3e-9), (40, 30, 1, 2e-9, 2e-9, 1e-9)])
+@pytest.mark.parametrize("mesh_args", [(32, 24, 4, 3e-9, 3e-9, 3e-9), (40, 30, 1, 2e-9, 2e-9, 1e-9),
+                                       (64, 32, 8, 3e-9, 3e-9, 3e-9), (128, 64, 1, 2e-9, 2e-9, 1e-9)])
 def test_demag_fp32_field(mesh_args):
     gm, om, gs64, os_ = _pair_state(mesh_args, seed=11)
     gs32 = M.State(gm, 8e5, random_m((gm.nx, gm.ny, gm.nz), 11), precision="fp32_field")
