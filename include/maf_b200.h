@@ -172,6 +172,41 @@ int maf_llg_integrate_dense(maf_llg l, maf_state s, double time_in_s, double wri
 int maf_llg_rk_attempt(maf_llg l, maf_state s, const char* scheme, double dt, double* m_new_host, double* err);
 /* LLGIntegrator::relax (llg_integrator.cpp:43-66) */
 int maf_llg_relax(maf_llg l, maf_state s, double precision, int eval_E);
+/* ------------------------------------------------------- Stochastic LLG ---
+ * Stochastic_LLG(alpha, T, dt, State, terms, smode) (magnumaf/include/magnumaf/integrators/stochastic_llg.hpp:9-18,
+ * magnumaf/src/integrators/stochastic_integrator.cpp:8-87): fixed-step "Heun", "SemiHeun" or "detRK4" with the
+ * thermal field h_th = sqrt(2D/dt) N(0,1), D = alpha kB T / (gamma mu0 Ms dV).  The reference seeds ArrayFire's
+ * Philox engine from the wall clock; here the thermal field of noise index n is a pure function of
+ * (seed, member, n, cell) (counter-based Philox-4x32-10), so runs are reproducible and every ensemble member has
+ * its own stream.  Heun step s uses index s for the predictor (the previous step's field) and s+1 for the
+ * corrector (stochastic_integrator.cpp:13-15). */
+typedef struct maf_stoch_s* maf_stoch;
+int maf_stochastic_llg_create(maf_stoch* out, double alpha, double T, double dt, const maf_term* terms, int nterms,
+                              const char* smode, unsigned long long seed, unsigned member);
+int maf_stochastic_llg_destroy(maf_stoch h);
+/* Stochastic_Integrator::step (stochastic_integrator.cpp:42-57) */
+int maf_stochastic_llg_step(maf_stoch h, maf_state s);
+int maf_stochastic_llg_steps(maf_stoch h, maf_state s, int n);
+/* Stochastic_LLG::E (stochastic_llg.cpp:6) */
+int maf_stochastic_llg_E(maf_stoch h, maf_state s, double* E);
+/* the thermal field of noise index `index` on this state's mesh, [3][N] (for checking and diagnostics) */
+int maf_stochastic_llg_noise(maf_stoch h, maf_state s, unsigned long long index, double* out_host);
+/* Stochastic_Integrator::get_calls */
+int maf_stochastic_llg_calls(maf_stoch h, unsigned long long* calls);
+
+/* ------------------------------------------------------------- LBFGS ---
+ * LBFGS_Minimizer(terms, tolerance = 1e-6, maxIter = 230)
+ * (magnumaf/include/magnumaf/solvers/lbfgs_minimizer.hpp:9-12, magnumaf/src/solvers/lbfgs_minimizer.cpp:19-505):
+ * m = 5 LBFGS on the normalised magnetisation, gradient m x (m x H), More-Thuente line search. */
+typedef struct maf_lbfgs_s* maf_lbfgs;
+int maf_lbfgs_create(maf_lbfgs* out, const maf_term* terms, int nterms, double tolerance, int maxIter);
+int maf_lbfgs_destroy(maf_lbfgs h);
+int maf_lbfgs_add_term(maf_lbfgs h, maf_term t);
+/* LBFGS_Minimizer::Minimize (lbfgs_minimizer.cpp:55-198): minimises in place, returns the final energy */
+int maf_lbfgs_minimize(maf_lbfgs h, maf_state s, double* E);
+/* iterations of the last minimisation, energy/gradient evaluations so far, max|m x (m x H)| at the end */
+int maf_lbfgs_stats(maf_lbfgs h, unsigned long long* iterations, unsigned long long* fevals, double* grad_max);
+
 /* current step size h and the controller counters {accepted, rejected, hmin, hmax}
  * (controller.hpp:26-31) */
 int maf_llg_get_h(maf_llg l, double* h);

@@ -377,6 +377,433 @@ thread_local DevBuf g_tmp;  // host-copy staging for H outputs
 
 }  // namespace
 
+// ---------------------------------------------------------------------------
+// Stochastic LLG (magnumaf/src/integrators/stochastic_integrator.cpp:8-57,
+// stochastic_llg.cpp:19-22): fixed-step Heun, semi-implicit Heun and the
+// deterministic RK4 reference, with thermal fields from the counter-based
+// generator (rng.cuh): the field of noise index n is sigma * xi(seed, member, n).
+// Heun step s uses xi(s) as the predictor's ("previous") field and xi(s+1) as
+// the corrector's; the semi-implicit scheme draws xi(2s) and xi(2s+1).
+// ---------------------------------------------------------------------------
+struct maf_stoch_s {
+    double alpha = 0, T = 0, dt = 0;
+    int mode = 0;  // 0 Heun, 1 SemiHeun, 2 detRK4
+    unsigned long long seed = 0;
+    unsigned member = 0;
+    unsigned long long calls = 0;  // accepted steps
+    std::vector<std::shared_ptr<Term>> terms;
+    DevBuf k[6];
+    DevBuf mstage64, mstage32, mcand, partials, errbuf;
+};
+
+namespace {
+
+double thermal_sigma(const maf_stoch_s* h, const StateD& s) {
+    // D = alpha kB T / (gamma mu0 Ms dV), h_th = sqrt(2 D / dt) N(0,1)
+    const double dV = s.md.dx * s.md.dy * s.md.dz;
+    const double D = (h->alpha * kKb * h->T) / (kGamma * kMu0 * s.Ms * dV);
+    return std::sqrt((2. * D) / h->dt);
+}
+
+struct StochStage {
+    int n = 0;
+    int j[6] = {};
+    double c[6] = {};
+    bool noise = false;
+    unsigned long long index = 0;
+    double scale = 0;
+};
+
+void stoch_step(maf_stoch_s* h, maf_state_s* st) {
+    StateD& s = st->s;
+    if (s.has_Ms_field) throw Error(MAF_ERR_BADARG, "Stochastic_LLG uses the scalar Ms (stochastic_integrator.cpp:9-10)");
+    const int64_t N = s.md.N(), n3 = 3 * N;
+    const bool f32 = s.precision == PREC_FP32_FIELD;
+    const double dt = h->dt;
+    const double sigma = thermal_sigma(h, s);
+    const unsigned long long q = h->calls;
+    std::vector<StochStage> stages;
+    KList fin;
+    if (h->mode == 0) {  // Heun (stochastic_integrator.cpp:8-17)
+        StochStage a; a.noise = true; a.index = q; a.scale = dt;
+        StochStage b; b.n = 1; b.j[0] = 0; b.c[0] = 1.0; b.noise = true; b.index = q + 1; b.scale = dt;
+        stages = {a, b};
+        fin.n = 2; fin.c[0] = 0.5; fin.c[1] = 0.5;  // (k1 + k2) / 2
+    } else if (h->mode == 1) {  // semi-implicit Heun (:19-32)
+        StochStage a; a.noise = true; a.index = 2 * q; a.scale = dt / 2.;
+        stages.push_back(a);
+        for (int i = 1; i < 6; ++i) {
+            StochStage b; b.n = 1; b.j[0] = i - 1; b.c[0] = 1.0; b.noise = true; b.index = 2 * q + 1;
+            b.scale = i < 5 ? dt / 2. : dt;
+            stages.push_back(b);
+        }
+        fin.n = 1; fin.c[0] = 1.0;
+    } else {  // deterministic RK4 (:34-40)
+        StochStage a; a.scale = dt;
+        StochStage b; b.n = 1; b.j[0] = 0; b.c[0] = 1. / 2.; b.scale = dt;
+        StochStage c; c.n = 1; c.j[0] = 1; c.c[0] = 1. / 2.; c.scale = dt;
+        StochStage d; d.n = 1; d.j[0] = 2; d.c[0] = 1.0; d.scale = dt;
+        stages = {a, b, c, d};
+        fin.n = 4; fin.c[0] = 1. / 6.; fin.c[1] = 2. / 6.; fin.c[2] = 2. / 6.; fin.c[3] = 1. / 6.;
+    }
+    for (size_t i = 0; i < stages.size(); ++i) h->k[i].ensure(sizeof(double) * n3);
+    h->mstage64.ensure(sizeof(double) * n3);
+    if (f32) h->mstage32.ensure(sizeof(float) * n3);
+    h->mcand.ensure(sizeof(double) * n3);
+    h->partials.ensure(sizeof(double) * 148 * 8 + 64);
+    h->errbuf.ensure(sizeof(double) * 4);
+    std::vector<Term*> terms;
+    for (auto& t : h->terms) terms.push_back(t.get());
+    for (size_t i = 0; i < stages.size(); ++i) {
+        const StochStage& sg = stages[i];
+        EpilogueArgs ep;
+        ep.kind = EPI_LLG;
+        ep.out = h->k[i].p;
+        ep.llg.c_prec = -kGamma / (1. + h->alpha * h->alpha);
+        ep.llg.c_damp = -h->alpha * kGamma / (1. + h->alpha * h->alpha);
+        ep.llg.scale = sg.scale;
+        if (sg.noise) {
+            ep.llg.sigma = sigma;
+            ep.llg.seed = h->seed;
+            ep.llg.member = h->member;
+            ep.llg.noise_index = sg.index;
+        }
+        if (sg.n == 0) {
+            ep.llg.m64 = s.m64.as<double>();
+            eval_on_state(st, terms, ep);
+        } else {
+            KList kl;
+            for (int t = 0; t < sg.n; ++t) {
+                kl.k[kl.n] = h->k[sg.j[t]].as<double>();
+                kl.c[kl.n] = sg.c[t];
+                ++kl.n;
+            }
+            rk_combine(s.m64.as<double>(), kl, h->mstage64.as<double>(), f32 ? h->mstage32.as<float>() : nullptr, n3,
+                       s.stream);
+            ep.llg.m64 = h->mstage64.as<double>();
+            if (f32)
+                eval_terms<float>(terms, s.md, h->mstage32.as<float>(), s.msinfo(), ep, s.stream, st->scratch, nullptr);
+            else
+                eval_terms<double>(terms, s.md, h->mstage64.as<double>(), s.msinfo(), ep, s.stream, st->scratch,
+                                   nullptr);
+        }
+    }
+    // m <- normalize(m + sum), normalize = the zero-safe util::normalize (:52)
+    const int base = h->mode == 1 ? 5 : 0;
+    for (int t = 0; t < fin.n; ++t) fin.k[t] = h->k[base + t].as<double>();
+    KList dummy;
+    dummy.n = 1;
+    dummy.k[0] = fin.k[0];
+    dummy.c[0] = 0.0;
+    rk_finalize(s.m64.as<double>(), fin, dummy, 0, 1.0, 0.0, h->mcand.as<double>(), 2, N, h->partials.as<double>(),
+                h->errbuf.as<double>(), s.stream);
+    std::swap(s.m64, h->mcand);
+    st->m32_valid = false;
+    s.t += dt;
+    s.steps++;
+    h->calls++;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// LBFGS minimiser (magnumaf/src/solvers/lbfgs_minimizer.cpp:33-505): m = 5
+// two-loop recursion on the normalised magnetisation with g = m x (m x H),
+// More-Thuente line search; scalars and control flow on the host, every
+// vector operation on the device (one reduction = one synchronisation, as in
+// the reference's scalar<double>() reads).
+// ---------------------------------------------------------------------------
+struct maf_lbfgs_s {
+    std::vector<std::shared_ptr<Term>> terms;
+    double tolerance = 1e-6;
+    size_t maxIter = 230;
+    DevBuf sV[5], yV[5], q, s, y, grad, grad_old, x_old, wa, red;
+    unsigned long long fevals = 0, iterations = 0;
+    double last_gradnorm = 0;
+};
+
+namespace {
+
+struct LbfgsCtx {
+    maf_lbfgs_s* h;
+    maf_state_s* st;
+    int64_t n3, N;
+    cudaStream_t stream;
+    double* red() const { return h->red.as<double>(); }
+    double dot(const DevBuf& a, const DevBuf& b) const {
+        return dot_host(a.as<double>(), b.as<double>(), n3, red(), stream);
+    }
+    double maxabs(const double* a) const { return maxabs_host(a, n3, red(), stream); }
+};
+
+// EnergyAndGradient (lbfgs_minimizer.cpp:38-42) of the state's current m
+double lbfgs_egrad(const LbfgsCtx& c, DevBuf& g) {
+    std::vector<Term*> terms;
+    for (auto& t : c.h->terms) terms.push_back(t.get());
+    EpilogueArgs ep;
+    ep.kind = EPI_EGRAD;
+    ep.out = g.p;
+    ep.llg.m64 = c.st->s.m64.as<double>();
+    double e = 0;
+    eval_on_state(c.st, terms, ep, &e);
+    c.h->fevals++;
+    return e;
+}
+
+// cstep (lbfgs_minimizer.cpp:362-505)
+void cstep(double& stx, double& fx, double& dx, double& sty, double& fy, double& dy, double& stp, double fp, double dp,
+           bool& brackt, double stpmin, double stpmax, int& info) {
+    info = 0;
+    bool bound = false;
+    if ((brackt && ((stp <= std::min(stx, sty)) || (stp >= std::max(stx, sty)))) || (dx * (stp - stx) >= 0.0) ||
+        (stpmax < stpmin))
+        return;
+    const double sgnd = dp * (dx / std::fabs(dx));
+    double stpf = 0, stpc = 0, stpq = 0;
+    if (fp > fx) {
+        info = 1;
+        bound = true;
+        const double theta = 3. * (fx - fp) / (stp - stx) + dx + dp;
+        const double s = std::max(theta, std::max(dx, dp));
+        double gamma = s * std::sqrt((theta / s) * (theta / s) - (dx / s) * (dp / s));
+        if (stp < stx) gamma = -gamma;
+        const double p = (gamma - dx) + theta;
+        const double q = ((gamma - dx) + gamma) + dp;
+        const double r = p / q;
+        stpc = stx + r * (stp - stx);
+        stpq = stx + ((dx / ((fx - fp) / (stp - stx) + dx)) / 2.) * (stp - stx);
+        stpf = std::fabs(stpc - stx) < std::fabs(stpq - stx) ? stpc : stpc + (stpq - stpc) / 2;
+        brackt = true;
+    } else if (sgnd < 0.0) {
+        info = 2;
+        bound = false;
+        const double theta = 3 * (fx - fp) / (stp - stx) + dx + dp;
+        const double s = std::max(theta, std::max(dx, dp));
+        double gamma = s * std::sqrt((theta / s) * (theta / s) - (dx / s) * (dp / s));
+        if (stp > stx) gamma = -gamma;
+        const double p = (gamma - dp) + theta;
+        const double q = ((gamma - dp) + gamma) + dx;
+        const double r = p / q;
+        stpc = stp + r * (stx - stp);
+        stpq = stp + (dp / (dp - dx)) * (stx - stp);
+        stpf = std::fabs(stpc - stp) > std::fabs(stpq - stp) ? stpc : stpq;
+        brackt = true;
+    } else if (std::fabs(dp) < std::fabs(dx)) {
+        info = 3;
+        bound = true;
+        const double theta = 3 * (fx - fp) / (stp - stx) + dx + dp;
+        const double s = std::max(theta, std::max(dx, dp));
+        double gamma = s * std::sqrt(std::max(0., (theta / s) * (theta / s) - (dx / s) * (dp / s)));
+        if (stp > stx) gamma = -gamma;
+        const double p = (gamma - dp) + theta;
+        const double q = (gamma + (dx - dp)) + gamma;
+        const double r = p / q;
+        if ((r < 0.0) && (gamma != 0.0)) stpc = stp + r * (stx - stp);
+        else if (stp > stx) stpc = stpmax;
+        else stpc = stpmin;
+        stpq = stp + (dp / (dp - dx)) * (stx - stp);
+        if (brackt) stpf = std::fabs(stp - stpc) < std::fabs(stp - stpq) ? stpc : stpq;
+        else stpf = std::fabs(stp - stpc) > std::fabs(stp - stpq) ? stpc : stpq;
+    } else {
+        info = 4;
+        bound = false;
+        if (brackt) {
+            const double theta = 3 * (fp - fy) / (sty - stp) + dy + dp;
+            const double s = std::max(theta, std::max(dy, dp));
+            double gamma = s * std::sqrt((theta / s) * (theta / s) - (dy / s) * (dp / s));
+            if (stp > sty) gamma = -gamma;
+            const double p = (gamma - dp) + theta;
+            const double q = ((gamma - dp) + gamma) + dy;
+            const double r = p / q;
+            stpc = stp + r * (sty - stp);
+            stpf = stpc;
+        } else if (stp > stx) {
+            stpf = stpmax;
+        } else {
+            stpf = stpmin;
+        }
+    }
+    if (fp > fx) {
+        sty = stp;
+        fy = fp;
+        dy = dp;
+    } else {
+        if (sgnd < 0.0) {
+            sty = stx;
+            fy = fx;
+            dy = dx;
+        }
+        stx = stp;
+        fx = fp;
+        dx = dp;
+    }
+    stpf = std::min(stpmax, stpf);
+    stpf = std::max(stpmin, stpf);
+    stp = stpf;
+    if (brackt && bound) {
+        if (sty > stx) stp = std::min(stx + 0.66 * (sty - stx), stp);
+        else stp = std::max(stx + 0.66 * (sty - stx), stp);
+    }
+}
+
+// cvsrch (lbfgs_minimizer.cpp:213-360): wa = x_old, s = search direction (device)
+void cvsrch(const LbfgsCtx& c, const DevBuf& wa, double& f, DevBuf& g, double& stp, const DevBuf& s, double tolf) {
+    int infoc = 1;
+    const double xtol = 1e-15, ftol = 1.0e-4, gtol = 0.9, eps = tolf;
+    const double stpmin = 1e-15, stpmax = 1e15, xtrapf = 4;
+    const int maxfev = 20;
+    int nfev = 0;
+    const double dginit = c.dot(g, s);
+    if (dginit >= 0.0) return;  // no descent
+    bool brackt = false, stage1 = true;
+    const double finit = f, dgtest = ftol * dginit;
+    double width = stpmax - stpmin, width1 = 2 * width;
+    double stx = 0.0, fx = finit, dgx = dginit, sty = 0.0, fy = finit, dgy = dginit;
+    double stmin = 0, stmax = 0;
+    StateD& S = c.st->s;
+    while (true) {
+        if (brackt) {
+            stmin = std::min(stx, sty);
+            stmax = std::max(stx, sty);
+        } else {
+            stmin = stx;
+            stmax = stp + xtrapf * (stp - stx);
+        }
+        stp = std::max(stp, stpmin);
+        stp = std::min(stp, stpmax);
+        if ((brackt && ((stp <= stmin) || (stp >= stmax))) || (nfev >= maxfev - 1) || (infoc == 0) ||
+            (brackt && (stmax - stmin <= xtol * stmax)))
+            stp = stx;
+        normalize_combine(S.m64.as<double>(), wa.as<double>(), stp, s.as<double>(), S.md.N(), c.stream);
+        c.st->m32_valid = false;
+        f = lbfgs_egrad(c, g);
+        nfev++;
+        const double dg = c.dot(g, s);
+        const double ftest1 = finit + stp * dgtest;
+        const double ftest2 = finit + eps * std::fabs(finit);
+        const double ft = 2 * ftol - 1;
+        int info = 0;
+        if ((brackt && ((stp <= stmin) || (stp >= stmax))) || (infoc == 0)) info = 6;
+        if ((stp == stpmax) && (f <= ftest2) && (dg <= dgtest)) info = 5;
+        if ((stp == stpmin) && ((f > ftest2) || (dg >= dgtest))) info = 4;
+        if (nfev >= maxfev) info = 3;
+        if (brackt && (stmax - stmin <= xtol * stmax)) info = 2;
+        if ((f <= ftest1) && (std::fabs(dg) <= gtol * (-dginit))) info = 1;
+        if (((f <= ftest2) && (ft * dginit >= dg)) && (std::fabs(dg) <= gtol * (-dginit))) info = 1;
+        if (info != 0) return;
+        if (stage1 && ((f <= ftest2) && (ft * dginit >= dg)) && (dg >= std::min(ftol, gtol) * dginit)) stage1 = false;
+        if (stage1 && (f <= fx) && !((f <= ftest2) && (ft * dginit >= dg))) {
+            const double fm = f - stp * dgtest;
+            double fxm = fx - stx * dgtest, fym = fy - sty * dgtest;
+            const double dgm = dg - dgtest;
+            double dgxm = dgx - dgtest, dgym = dgy - dgtest;
+            cstep(stx, fxm, dgxm, sty, fym, dgym, stp, fm, dgm, brackt, stmin, stmax, infoc);
+            fx = fxm + stx * dgtest;
+            fy = fym + sty * dgtest;
+            dgx = dgxm + dgtest;
+            dgy = dgym + dgtest;
+        } else {
+            cstep(stx, fx, dgx, sty, fy, dgy, stp, f, dg, brackt, stmin, stmax, infoc);
+        }
+        if (brackt) {
+            if (std::fabs(sty - stx) >= 0.66 * width1) stp = stx + 0.5 * (sty - stx);
+            width1 = width;
+            width = std::fabs(sty - stx);
+        }
+    }
+}
+
+// LBFGS_Minimizer::Minimize (lbfgs_minimizer.cpp:55-198)
+double lbfgs_minimize(maf_lbfgs_s* h, maf_state_s* st) {
+    StateD& S = st->s;
+    const int64_t n3 = 3 * S.md.N();
+    for (auto* b : {&h->q, &h->s, &h->y, &h->grad, &h->grad_old, &h->x_old}) b->ensure(sizeof(double) * n3);
+    for (int i = 0; i < 5; ++i) {
+        h->sV[i].ensure(sizeof(double) * n3);
+        h->yV[i].ensure(sizeof(double) * n3);
+    }
+    h->red.ensure(sizeof(double) * (2 * 148 + 8));
+    LbfgsCtx c{h, st, n3, S.md.N(), S.stream};
+    const double eps = 2.22e-16, eps2 = std::sqrt(eps), epsr = std::pow(eps, 0.9);
+    const double tolf2 = std::sqrt(h->tolerance), tolf3 = std::pow(h->tolerance, 0.3333333333333333333333333);
+    double f = lbfgs_egrad(c, h->grad);
+    double gradNorm = c.maxabs(h->grad.as<double>());
+    h->iterations = 0;
+    h->last_gradnorm = gradNorm;
+    if (gradNorm < (epsr * (1 + std::fabs(f)))) return f;
+    const size_t m = 5;
+    double alpha[5] = {0, 0, 0, 0, 0};
+    size_t iter = 0, globIter = 0;
+    double H0k = 1;
+    int order[5] = {0, 1, 2, 3, 4};  // logical slot -> buffer (std::rotate of the reference)
+    do {
+        const double f_old = f;
+        MAF_CUDA(cudaMemcpyAsync(h->x_old.p, S.m64.p, sizeof(double) * n3, cudaMemcpyDeviceToDevice, S.stream));
+        MAF_CUDA(cudaMemcpyAsync(h->grad_old.p, h->grad.p, sizeof(double) * n3, cudaMemcpyDeviceToDevice, S.stream));
+        MAF_CUDA(cudaMemcpyAsync(h->q.p, h->grad.p, sizeof(double) * n3, cudaMemcpyDeviceToDevice, S.stream));
+        const int k = (int)std::min(m, iter);
+        for (int i = k - 1; i >= 0; --i) {
+            const DevBuf& sv = h->sV[order[i]];
+            const DevBuf& yv = h->yV[order[i]];
+            const double rho = 1.0 / c.dot(sv, yv);
+            alpha[i] = rho * c.dot(sv, h->q);
+            axpby(h->q.as<double>(), 1.0, h->q.as<double>(), -alpha[i], yv.as<double>(), n3, S.stream);
+        }
+        axpby(h->q.as<double>(), H0k, h->q.as<double>(), 0.0, nullptr, n3, S.stream);
+        for (int i = 0; i < k; ++i) {
+            const DevBuf& sv = h->sV[order[i]];
+            const DevBuf& yv = h->yV[order[i]];
+            const double rho = 1.0 / c.dot(sv, yv);
+            const double beta = rho * c.dot(yv, h->q);
+            axpby(h->q.as<double>(), 1.0, h->q.as<double>(), alpha[i] - beta, sv.as<double>(), n3, S.stream);
+        }
+        const double phiPrime0 = -c.dot(h->grad, h->q);
+        if (phiPrime0 > 0) {
+            MAF_CUDA(cudaMemcpyAsync(h->q.p, h->grad.p, sizeof(double) * n3, cudaMemcpyDeviceToDevice, S.stream));
+            iter = 0;
+        }
+        // search direction -q (held in s until the step is known)
+        axpby(h->s.as<double>(), -1.0, h->q.as<double>(), 0.0, nullptr, n3, S.stream);
+        double rate = 1.0;
+        cvsrch(c, h->x_old, f, h->grad, rate, h->s, h->tolerance);
+        const double f1 = 1 + std::fabs(f);
+        gradNorm = c.maxabs(h->grad.as<double>());
+        h->last_gradnorm = gradNorm;
+        if (gradNorm < (epsr * f1)) {
+            h->iterations = globIter;
+            return f;
+        }
+        axpby(h->s.as<double>(), 1.0, S.m64.as<double>(), -1.0, h->x_old.as<double>(), n3, S.stream);
+        const double smax = c.maxabs(h->s.as<double>());
+        const double mmax = c.maxabs(S.m64.as<double>());
+        if (((f_old - f) < (h->tolerance * f1)) && (smax < (tolf2 * (1 + mmax))) && (gradNorm <= (tolf3 * f1))) break;
+        axpby(h->y.as<double>(), 1.0, h->grad.as<double>(), -1.0, h->grad_old.as<double>(), n3, S.stream);
+        const double ys = c.dot(h->y, h->s);
+        if (ys <= eps2 * std::sqrt(c.dot(h->y, h->y)) * std::sqrt(c.dot(h->s, h->s))) {
+            // Dennis, Schnabel 9.4.1: skip the update
+        } else {
+            int slot;
+            if (iter < m) {
+                slot = order[iter];
+            } else {
+                const int first = order[0];
+                for (int i = 0; i < 4; ++i) order[i] = order[i + 1];
+                order[4] = first;
+                slot = first;
+            }
+            MAF_CUDA(cudaMemcpyAsync(h->sV[slot].p, h->s.p, sizeof(double) * n3, cudaMemcpyDeviceToDevice, S.stream));
+            MAF_CUDA(cudaMemcpyAsync(h->yV[slot].p, h->y.p, sizeof(double) * n3, cudaMemcpyDeviceToDevice, S.stream));
+            H0k = ys / c.dot(h->y, h->y);
+            iter++;
+        }
+        globIter++;
+    } while (globIter < h->maxIter);
+    h->iterations = globIter;
+    return f;
+}
+
+}  // namespace
+
 // ===========================================================================
 extern "C" {
 
@@ -999,6 +1426,124 @@ int maf_llg_relax(maf_llg l, maf_state s, double precision, int eval_E) {
             for (int i = 0; i < eval_E; ++i) llg_step(l, s);
             E = llg_energy(l, s);
         }
+    });
+}
+
+// ------------------------------------------------------------ Stochastic LLG
+int maf_stochastic_llg_create(maf_stoch* out, double alpha, double T, double dt, const maf_term* terms, int nterms,
+                              const char* smode, unsigned long long seed, unsigned member) {
+    return guarded([&] {
+        check(out, "NULL argument");
+        check(dt > 0, "Stochastic_LLG: dt must be > 0");
+        check(T >= 0, "Stochastic_LLG: T must be >= 0");
+        auto h = std::make_unique<maf_stoch_s>();
+        h->alpha = alpha;
+        h->T = T;
+        h->dt = dt;
+        const std::string m = smode ? smode : "Heun";
+        // get_mode (stochastic_integrator.cpp:59-73); unknown strings are rejected instead of falling back to Heun
+        if (m == "Heun" || m == "0") h->mode = 0;
+        else if (m == "SemiHeun" || m == "1") h->mode = 1;
+        else if (m == "detRK4" || m == "2") h->mode = 2;
+        else throw Error(MAF_ERR_BADARG, "Stochastic_LLG: integrator mode not recognised: " + m);
+        h->seed = seed;
+        h->member = member;
+        for (int i = 0; i < nterms; ++i) {
+            check(terms && terms[i], "Stochastic_LLG: NULL term");
+            h->terms.push_back(terms[i]->t);
+        }
+        check(!h->terms.empty(), "Stochastic_LLG: no field terms");
+        *out = h.release();
+    });
+}
+
+int maf_stochastic_llg_destroy(maf_stoch h) {
+    return guarded([&] { delete h; });
+}
+
+int maf_stochastic_llg_step(maf_stoch h, maf_state s) {
+    return guarded([&] {
+        check(h && s, "NULL argument");
+        stoch_step(h, s);
+    });
+}
+
+int maf_stochastic_llg_steps(maf_stoch h, maf_state s, int n) {
+    return guarded([&] {
+        check(h && s, "NULL argument");
+        for (int i = 0; i < n; ++i) stoch_step(h, s);
+    });
+}
+
+int maf_stochastic_llg_E(maf_stoch h, maf_state s, double* E) {
+    return guarded([&] {
+        check(h && s && E, "NULL argument");
+        std::vector<Term*> terms;
+        for (auto& t : h->terms) terms.push_back(t.get());
+        EpilogueArgs ep;
+        ep.kind = EPI_EDENS;
+        eval_on_state(s, terms, ep, E);
+    });
+}
+
+int maf_stochastic_llg_noise(maf_stoch h, maf_state s, unsigned long long index, double* out) {
+    return guarded([&] {
+        check(h && s && out, "NULL argument");
+        StateD& st = s->s;
+        const int64_t n3 = 3 * st.md.N();
+        h->mstage64.ensure(sizeof(double) * n3);
+        thermal_field(h->mstage64.as<double>(), st.md.N(), thermal_sigma(h, st), h->seed, h->member, index, st.stream);
+        MAF_CUDA(cudaMemcpyAsync(out, h->mstage64.p, sizeof(double) * n3, cudaMemcpyDeviceToHost, st.stream));
+        MAF_CUDA(cudaStreamSynchronize(st.stream));
+    });
+}
+
+int maf_stochastic_llg_calls(maf_stoch h, unsigned long long* calls) {
+    return guarded([&] { check(h && calls, "NULL argument"); *calls = h->calls; });
+}
+
+// ------------------------------------------------------------ LBFGS minimiser
+int maf_lbfgs_create(maf_lbfgs* out, const maf_term* terms, int nterms, double tolerance, int maxIter) {
+    return guarded([&] {
+        check(out, "NULL argument");
+        check(maxIter >= 0, "LBFGS_Minimizer: maxIter must be >= 0");
+        auto h = std::make_unique<maf_lbfgs_s>();
+        for (int i = 0; i < nterms; ++i) {
+            check(terms && terms[i], "LBFGS_Minimizer: NULL term");
+            h->terms.push_back(terms[i]->t);
+        }
+        h->tolerance = tolerance;
+        h->maxIter = (size_t)maxIter;
+        *out = h.release();
+    });
+}
+
+int maf_lbfgs_destroy(maf_lbfgs h) {
+    return guarded([&] { delete h; });
+}
+
+int maf_lbfgs_add_term(maf_lbfgs h, maf_term t) {
+    return guarded([&] {
+        check(h && t, "NULL argument");
+        h->terms.push_back(t->t);
+    });
+}
+
+int maf_lbfgs_minimize(maf_lbfgs h, maf_state s, double* E) {
+    return guarded([&] {
+        check(h && s && E, "NULL argument");
+        // abort_if_size_is_zero (lbfgs_minimizer.cpp:25-30)
+        check(!h->terms.empty(), "LBFGS_Minimizer: Number of terms == 0. Please add at least one term.");
+        *E = lbfgs_minimize(h, s);
+    });
+}
+
+int maf_lbfgs_stats(maf_lbfgs h, unsigned long long* iterations, unsigned long long* fevals, double* grad_max) {
+    return guarded([&] {
+        check(h, "NULL argument");
+        if (iterations) *iterations = h->iterations;
+        if (fevals) *fevals = h->fevals;
+        if (grad_max) *grad_max = h->last_gradnorm;
     });
 }
 

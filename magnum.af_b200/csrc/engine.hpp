@@ -63,6 +63,7 @@ enum Epilogue : int {
     EPI_H = 0,      // write H (precision R) to out[3][N]
     EPI_LLG = 1,    // write k = scale * dm/dt (double) to out[3][N]
     EPI_EDENS = 2,  // accumulate the energy of the term list (double partial sums per CTA)
+    EPI_EGRAD = 3,  // energy partials and the LBFGS gradient m x (m x H) (double) to out[3][N]
 };
 
 struct LLGParams {
@@ -72,6 +73,11 @@ struct LLGParams {
     int dissipation_only = 0;
     double scale = 1.0;            // dt (RKF45/DP45) or 1 (BS23)
     const double* m64 = nullptr;   // state m in FP64 for the cross products
+    // thermal field sigma * xi(seed, member, noise_index, cell) added to H (stochastic LLG)
+    double sigma = 0.0;
+    unsigned long long seed = 0;
+    unsigned member = 0;
+    unsigned long long noise_index = 0;
 };
 
 struct EpilogueArgs {

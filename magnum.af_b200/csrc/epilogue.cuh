@@ -3,6 +3,7 @@
 // or dt * LLG right-hand side in FP64, or accumulate the energy density.
 #pragma once
 #include "engine.hpp"
+#include "rng.cuh"
 
 namespace mafb {
 
@@ -23,7 +24,7 @@ __device__ __forceinline__ void epilogue_cell(const Geom& g, int x, int y, int z
     mvec(m, g, cell, mc);
     const bool msf = ms.field64 != nullptr;
     const R Ms = cell_Ms<R>(ms, cell);
-    if constexpr (EPI == EPI_EDENS) {
+    if constexpr (EPI == EPI_EDENS || EPI == EPI_EGRAD) {
         const double Msd = msf ? ms.field64[cell] : ms.Ms;
         for (int it = 0; it < tl.n; ++it) {
             const TermDesc& t = tl.t[it];
@@ -55,7 +56,8 @@ __device__ __forceinline__ void epilogue_cell(const Geom& g, int x, int y, int z
             const double hm = (double)ht[0] * (double)mc[0] + (double)ht[1] * (double)mc[1] + (double)ht[2] * (double)mc[2];
             eacc += w * Msd * hm;
         }
-    } else {
+    }
+    if constexpr (EPI != EPI_EDENS) {
         R h[3] = {0, 0, 0};
         for (int it = 0; it < tl.n; ++it) {
             const TermDesc& t = tl.t[it];
@@ -70,10 +72,30 @@ __device__ __forceinline__ void epilogue_cell(const Geom& g, int x, int y, int z
             o[cell] = h[0];
             o[g.N + cell] = h[1];
             o[2 * g.N + cell] = h[2];
-        } else {
+        } else if constexpr (EPI == EPI_EGRAD) {
+            // LBFGS gradient m x (m x Heff) (lbfgs_minimizer.cpp:33-36), FP64
             const double* m64 = ep.llg.m64;
             const double M0 = m64[cell], M1 = m64[g.N + cell], M2 = m64[2 * g.N + cell];
             const double H0 = h[0], H1 = h[1], H2 = h[2];
+            const double x0 = M1 * H2 - M2 * H1;
+            const double x1 = M2 * H0 - M0 * H2;
+            const double x2 = M0 * H1 - M1 * H0;
+            double* o = static_cast<double*>(ep.out);
+            o[cell] = M1 * x2 - M2 * x1;
+            o[g.N + cell] = M2 * x0 - M0 * x2;
+            o[2 * g.N + cell] = M0 * x1 - M1 * x0;
+        } else {
+            const double* m64 = ep.llg.m64;
+            const double M0 = m64[cell], M1 = m64[g.N + cell], M2 = m64[2 * g.N + cell];
+            double H0 = h[0], H1 = h[1], H2 = h[2];
+            if (ep.llg.sigma != 0.0) {
+                // Heff + h_th (stochastic_llg.cpp:19-22), h_th = sqrt(2D/dt) N(0,1)
+                double xi[3];
+                normal3(ep.llg.seed, ep.llg.member, ep.llg.noise_index, (uint64_t)cell, xi);
+                H0 += ep.llg.sigma * xi[0];
+                H1 += ep.llg.sigma * xi[1];
+                H2 += ep.llg.sigma * xi[2];
+            }
             const double x0 = M1 * H2 - M2 * H1;
             const double x1 = M2 * H0 - M0 * H2;
             const double x2 = M0 * H1 - M1 * H0;
@@ -97,6 +119,203 @@ __device__ __forceinline__ void epilogue_cell(const Geom& g, int x, int y, int z
             o[cell] = sc * k0;
             o[g.N + cell] = sc * k1;
             o[2 * g.N + cell] = sc * k2;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Fast epilogue for a run of 4 consecutive cells along x (x0 % 4 == 0): all
+// m values the stencils need (the run, its two x neighbours, and the runs at
+// y-1, y+1, z-1, z+1) are fetched first with vector loads, then the terms are
+// evaluated.  Valid when the term list holds only demag, exchange, interface
+// DMI, uniaxial and cubic anisotropy with scalar parameters and a uniform
+// Zeeman field, and the state has no Ms_field (run4_eligible on the host).
+// Same arithmetic per cell as add_local_term / epilogue_cell.
+// ---------------------------------------------------------------------------
+template <typename R> struct Run4 {
+    R c[3][4];            // the run
+    R xl[3], xr[3];       // x neighbours of the first and the last cell
+    R ym[3][4], yp[3][4], zm[3][4], zp[3][4];
+    bool hxl, hxr, hym, hyp, hzm, hzp;
+};
+
+template <typename R> __device__ __forceinline__ void load4(const R* __restrict__ p, R out[4]) {
+    if constexpr (sizeof(R) == 4) {
+        const float4 v = *reinterpret_cast<const float4*>(p);
+        out[0] = v.x; out[1] = v.y; out[2] = v.z; out[3] = v.w;
+    } else {
+        const double2 a = reinterpret_cast<const double2*>(p)[0];
+        const double2 b = reinterpret_cast<const double2*>(p)[1];
+        out[0] = a.x; out[1] = a.y; out[2] = b.x; out[3] = b.y;
+    }
+}
+
+template <typename R>
+__device__ __forceinline__ void run4_load(const R* __restrict__ m, const Geom& g, int x0, int y, int z, int64_t cell0,
+                                          Run4<R>& r) {
+    const int64_t sy = g.nx, sz = (int64_t)g.nx * g.ny;
+    r.hxl = x0 > 0;
+    r.hxr = x0 + 4 < g.nx;
+    r.hym = y > 0;
+    r.hyp = y < g.ny - 1;
+    r.hzm = z > 0;
+    r.hzp = z < g.nz - 1;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        const R* p = m + c * g.N + cell0;
+        load4(p, r.c[c]);
+        r.xl[c] = r.hxl ? p[-1] : (R)0;
+        r.xr[c] = r.hxr ? p[4] : (R)0;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) { r.ym[c][i] = 0; r.yp[c][i] = 0; r.zm[c][i] = 0; r.zp[c][i] = 0; }
+        if (r.hym) load4(p - sy, r.ym[c]);
+        if (r.hyp) load4(p + sy, r.yp[c]);
+        if (r.hzm) load4(p - sz, r.zm[c]);
+        if (r.hzp) load4(p + sz, r.zp[c]);
+    }
+}
+
+// H of cell i of the run (hd = demag contribution)
+template <typename R>
+__device__ __forceinline__ void run4_field(const TermList& tl, const Geom& g, const Run4<R>& r, int i, R Ms,
+                                           const R hd[3], R h[3]) {
+    h[0] = 0;
+    h[1] = 0;
+    h[2] = 0;
+    const bool xm = i > 0 || r.hxl, xp = i < 3 || r.hxr;
+    for (int it = 0; it < tl.n; ++it) {
+        const TermDesc& t = tl.t[it];
+        switch (t.kind) {
+            case TK_DEMAG:
+                h[0] += hd[0]; h[1] += hd[1]; h[2] += hd[2];
+                break;
+            case TK_EXCHANGE: {
+                const R idx2 = (R)(1.0 / (g.dx * g.dx)), idy2 = (R)(1.0 / (g.dy * g.dy)), idz2 = (R)(1.0 / (g.dz * g.dz));
+                const R coef = (R)(2.0 * t.p[0]) / ((R)kMu0 * Ms);
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    const R v = r.c[c][i];
+                    const R left = i > 0 ? r.c[c][i - 1] : r.xl[c];
+                    const R right = i < 3 ? r.c[c][i + 1] : r.xr[c];
+                    const R ax = (xm ? left - v : -v) + (xp ? right - v : -v);
+                    const R ay = (r.hym ? r.ym[c][i] - v : -v) + (r.hyp ? r.yp[c][i] - v : -v);
+                    const R az = (r.hzm ? r.zm[c][i] - v : -v) + (r.hzp ? r.zp[c][i] - v : -v);
+                    h[c] += coef * (ax * idx2 + ay * idy2 + az * idz2);
+                }
+                break;
+            }
+            case TK_DMI: {
+                const R n0 = (R)t.p[1], n1 = (R)t.p[2], n2 = (R)t.p[3];
+                const R hx = (R)(0.5 / g.dx), hy = (R)(0.5 / g.dy), hz = (R)(0.5 / g.dz);
+                R lm[3], rm[3];
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    lm[c] = i > 0 ? r.c[c][i - 1] : r.xl[c];
+                    rm[c] = i < 3 ? r.c[c][i + 1] : r.xr[c];
+                }
+                const R div = (rm[0] - lm[0]) * hx + (r.yp[1][i] - r.ym[1][i]) * hy + (r.zp[2][i] - r.zm[2][i]) * hz;
+                auto nm = [&](const R v0, const R v1, const R v2) { return n0 * v0 + n1 * v1 + n2 * v2; };
+                const R g0 = (nm(rm[0], rm[1], rm[2]) - nm(lm[0], lm[1], lm[2])) * hx;
+                const R g1 = (nm(r.yp[0][i], r.yp[1][i], r.yp[2][i]) - nm(r.ym[0][i], r.ym[1][i], r.ym[2][i])) * hy;
+                const R g2 = (nm(r.zp[0][i], r.zp[1][i], r.zp[2][i]) - nm(r.zm[0][i], r.zm[1][i], r.zm[2][i])) * hz;
+                const R coef = (R)2 * (R)t.p[0] / ((R)kMu0 * Ms);
+                h[0] += coef * (n0 * div - g0);
+                h[1] += coef * (n1 * div - g1);
+                h[2] += coef * (n2 * div - g2);
+                break;
+            }
+            case TK_UNIAXIAL: {
+                const R e0 = (R)t.p[1], e1 = (R)t.p[2], e2 = (R)t.p[3];
+                const R em = e0 * r.c[0][i] + e1 * r.c[1][i] + e2 * r.c[2][i];
+                const R coef = (R)2 * (R)t.p[0] / ((R)kMu0 * Ms);
+                h[0] += coef * (e0 * em);
+                h[1] += coef * (e1 * em);
+                h[2] += coef * (e2 * em);
+                break;
+            }
+            case TK_CUBIC: {
+                const R mc[3] = {r.c[0][i], r.c[1][i], r.c[2][i]};
+                R hc[3];
+                cubic_h123_sum(t, mc, Ms, hc);
+                h[0] += hc[0]; h[1] += hc[1]; h[2] += hc[2];
+                break;
+            }
+            case TK_ZEEMAN:
+                h[0] += (R)t.p[0]; h[1] += (R)t.p[1]; h[2] += (R)t.p[2];
+                break;
+            default: break;
+        }
+    }
+}
+
+// Writes the epilogue output (H, dt*LLG or the LBFGS gradient) of the run.
+template <typename R, int EPI>
+__device__ __forceinline__ void run4_epilogue(const TermList& tl, const Geom& g, const Run4<R>& r, int64_t cell0,
+                                              R Ms, const R hd[4][3], const EpilogueArgs& ep) {
+    R h[4][3];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) run4_field(tl, g, r, i, Ms, hd[i], h[i]);
+    if constexpr (EPI == EPI_H) {
+        R* o = static_cast<R*>(ep.out);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            R* p = o + c * g.N + cell0;
+            if constexpr (sizeof(R) == 4) {
+                *reinterpret_cast<float4*>(p) = make_float4(h[0][c], h[1][c], h[2][c], h[3][c]);
+            } else {
+                reinterpret_cast<double2*>(p)[0] = make_double2(h[0][c], h[1][c]);
+                reinterpret_cast<double2*>(p)[1] = make_double2(h[2][c], h[3][c]);
+            }
+        }
+    } else {
+        const double* m64 = ep.llg.m64;
+        double* o = static_cast<double*>(ep.out);
+        double M[3][4], out[3][4];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) load4(m64 + c * g.N + cell0, M[c]);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            double H0 = h[i][0], H1 = h[i][1], H2 = h[i][2];
+            if constexpr (EPI == EPI_LLG) {
+                if (ep.llg.sigma != 0.0) {
+                    double xi[3];
+                    normal3(ep.llg.seed, ep.llg.member, ep.llg.noise_index, (uint64_t)(cell0 + i), xi);
+                    H0 += ep.llg.sigma * xi[0];
+                    H1 += ep.llg.sigma * xi[1];
+                    H2 += ep.llg.sigma * xi[2];
+                }
+            }
+            const double M0 = M[0][i], M1 = M[1][i], M2 = M[2][i];
+            const double x0 = M1 * H2 - M2 * H1;
+            const double x1 = M2 * H0 - M0 * H2;
+            const double x2 = M0 * H1 - M1 * H0;
+            const double d0 = M1 * x2 - M2 * x1;
+            const double d1 = M2 * x0 - M0 * x2;
+            const double d2 = M0 * x1 - M1 * x0;
+            if constexpr (EPI == EPI_EGRAD) {
+                out[0][i] = d0; out[1][i] = d1; out[2][i] = d2;
+            } else {
+                double cp = ep.llg.c_prec, cd = ep.llg.c_damp;
+                if (ep.llg.alpha) {
+                    const double a = ep.llg.alpha[cell0 + i];
+                    cp = -kGamma / (1. + a * a);
+                    cd = -a * kGamma / (1. + a * a);
+                }
+                const double sc = ep.llg.scale;
+                if (ep.llg.dissipation_only) {
+                    out[0][i] = sc * (cd * d0); out[1][i] = sc * (cd * d1); out[2][i] = sc * (cd * d2);
+                } else {
+                    out[0][i] = sc * (cp * x0 + cd * d0);
+                    out[1][i] = sc * (cp * x1 + cd * d1);
+                    out[2][i] = sc * (cp * x2 + cd * d2);
+                }
+            }
+        }
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            double2* p = reinterpret_cast<double2*>(o + c * g.N + cell0);
+            p[0] = make_double2(out[c][0], out[c][1]);
+            p[1] = make_double2(out[c][2], out[c][3]);
         }
     }
 }

@@ -307,7 +307,7 @@ __global__ void __launch_bounds__(kMaxFftThreads) k_xinv_epi(const cplx_t<R>* __
         }
         epilogue_cell<R, EPI>(g, x, y, z, cell, m, ms, tl, ep, hd, eacc);
     }
-    if constexpr (EPI == EPI_EDENS) block_sum_store(eacc, ep.partials);
+    if constexpr (EPI == EPI_EDENS || EPI == EPI_EGRAD) block_sum_store(eacc, ep.partials);
 }
 
 // Local terms only (no demag in the term list).
@@ -324,7 +324,7 @@ __global__ void __launch_bounds__(256) k_local_epi(Geom g, const R* __restrict__
         const int z = (int)(r / g.ny);
         epilogue_cell<R, EPI>(g, x, y, z, cell, m, ms, tl, ep, hd, eacc);
     }
-    if constexpr (EPI == EPI_EDENS) block_sum_store(eacc, ep.partials);
+    if constexpr (EPI == EPI_EDENS || EPI == EPI_EGRAD) block_sum_store(eacc, ep.partials);
 }
 
 __global__ void k_sum_partials(const double* __restrict__ p, int n, double* out) {
@@ -373,7 +373,8 @@ __global__ void k_d2f(const double* __restrict__ a, float* __restrict__ b, int64
 // launch helpers
 // ---------------------------------------------------------------------------
 template <typename K> static void set_smem(K kernel, size_t bytes) {
-    if (bytes > 48 * 1024) MAF_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    // opt in above 32 KB: the 48 KB default also has to hold the static shared memory
+    if (bytes > 32 * 1024) MAF_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
 }
 
 static int round_threads(int t) {
@@ -570,8 +571,8 @@ template <typename R> void Demag::forward_conv(const R* m, const MsInfo& ms, cud
             k_conv<R><<<grid, threads, smem, st>>>(s2, Nr, fp, ip, nz, (int64_t)Py() * pitch_,
                                                    (int64_t)nz * Py() * pitch_, pitch_, nxh(), nb, 1, ny, nz, nxh());
             MAF_LAUNCH_CHECK();
-            if (marks) marks->mark(st, "z_conv");
         }
+        if (marks) marks->mark(st, "z_conv");
         // pass 4: y inverse, S2 -> S1, keep ky rows [0, ny)
         launch_cols<R, 1>(s2, s1, Py(), Py(), ny, nxh(), pitch_, pitch_, (int64_t)Py() * pitch_,
                           (int64_t)ny * pitch_, 3 * nz, tw_, st);
@@ -643,6 +644,11 @@ void Demag::inverse_x_epilogue(const R* m, const MsInfo& ms, const TermList& tl,
             k_xinv_epi<R, EPI_LLG><<<(unsigned)blocks, threads, smem, st>>>(S1<R>(), pitch_, plan, tP, g, scale, m,
                                                                             ms, tl, ep, nbr);
             break;
+        case EPI_EGRAD:
+            set_smem(k_xinv_epi<R, EPI_EGRAD>, smem);
+            k_xinv_epi<R, EPI_EGRAD><<<(unsigned)blocks, threads, smem, st>>>(S1<R>(), pitch_, plan, tP, g, scale, m,
+                                                                              ms, tl, ep, nbr);
+            break;
         default:
             set_smem(k_xinv_epi<R, EPI_EDENS>, smem);
             k_xinv_epi<R, EPI_EDENS><<<(unsigned)blocks, threads, smem, st>>>(S1<R>(), pitch_, plan, tP, g, scale, m,
@@ -683,7 +689,7 @@ void eval_terms(const std::vector<Term*>& terms, const MeshDims& md, const R* m,
     }
     EpilogueArgs ep = ep_in;
     int nblocks = 0;
-    if (ep.kind == EPI_EDENS) {
+    if (ep.kind == EPI_EDENS || ep.kind == EPI_EGRAD) {
         // upper bound of CTAs for the partial sums
         const int64_t maxb = std::max<int64_t>(md.N(), 148 * 8) + 1;
         scratch.ensure(sizeof(double) * (maxb + 1));
@@ -702,12 +708,13 @@ void eval_terms(const std::vector<Term*>& terms, const MeshDims& md, const R* m,
         switch (ep.kind) {
             case EPI_H: k_local_epi<R, EPI_H><<<(unsigned)blocks, threads, 0, st>>>(g, m, ms, tl, ep); break;
             case EPI_LLG: k_local_epi<R, EPI_LLG><<<(unsigned)blocks, threads, 0, st>>>(g, m, ms, tl, ep); break;
+            case EPI_EGRAD: k_local_epi<R, EPI_EGRAD><<<(unsigned)blocks, threads, 0, st>>>(g, m, ms, tl, ep); break;
             default: k_local_epi<R, EPI_EDENS><<<(unsigned)blocks, threads, 0, st>>>(g, m, ms, tl, ep); break;
         }
         MAF_LAUNCH_CHECK();
         if (marks) marks->mark(st, "local");
     }
-    if (ep.kind == EPI_EDENS) {
+    if (ep.kind == EPI_EDENS || ep.kind == EPI_EGRAD) {
         double* dst = ep.partials + nblocks;
         k_sum_partials<<<1, 256, 0, st>>>(ep.partials, nblocks, dst);
         MAF_LAUNCH_CHECK();

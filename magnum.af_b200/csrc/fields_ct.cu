@@ -255,7 +255,7 @@ template <typename R, int EPI, int LC, int NBR, int NT>
 __global__ void __launch_bounds__(NT) k_xinv_ct(const cplx_t<R>* __restrict__ S1, int pitch,
                                                 const cplx_t<R>* __restrict__ tw, const cplx_t<R>* __restrict__ twP,
                                                 Geom g, R scale, const R* __restrict__ m, MsInfo ms, TermList tl,
-                                                EpilogueArgs ep) {
+                                                EpilogueArgs ep, int run4) {
     using C = cplx_t<R>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C* s = reinterpret_cast<C*>(smem_raw);
@@ -291,6 +291,33 @@ __global__ void __launch_bounds__(NT) k_xinv_ct(const cplx_t<R>* __restrict__ S1
     }
     __syncthreads();
     ct_fft<R, 1, false, LC, NC, NT>(s, SB, tw, typename CtPlan<LC>::T());
+    if constexpr (EPI == EPI_H || EPI == EPI_LLG) {
+        if (run4) {
+            const int runs = g.nx >> 2;
+            for (int idx = threadIdx.x; idx < NBR * runs; idx += NT) {
+                const int b = idx / runs;
+                const int x0 = (idx - b * runs) << 2;
+                const int64_t ry = ry0 + b;
+                if (ry >= rows_pc) continue;
+                const int z = (int)(ry / g.ny);
+                const int y = (int)(ry - (int64_t)z * g.ny);
+                const int64_t cell0 = ry * g.nx + x0;
+                Run4<R> r;
+                run4_load(m, g, x0, y, z, cell0, r);
+                R hd[4][3];
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) {
+                        const C val = s[spad((x0 + i) >> 1) + (c * NBR + b) * SB];
+                        hd[i][c] = scale * (((x0 + i) & 1) ? val.y : val.x);
+                    }
+                }
+                run4_epilogue<R, EPI>(tl, g, r, cell0, (R)ms.Ms, hd, ep);
+            }
+            return;
+        }
+    }
     double eacc = 0;
     for (int idx = threadIdx.x; idx < NBR * g.nx; idx += NT) {
         const int b = idx / g.nx;
@@ -308,12 +335,35 @@ __global__ void __launch_bounds__(NT) k_xinv_ct(const cplx_t<R>* __restrict__ S1
         }
         epilogue_cell<R, EPI>(g, x, y, z, cell, m, ms, tl, ep, hd, eacc);
     }
-    if constexpr (EPI == EPI_EDENS) block_sum_store(eacc, ep.partials);
+    if constexpr (EPI == EPI_EDENS || EPI == EPI_EGRAD) block_sum_store(eacc, ep.partials);
 }
 
 // ------------------------------------------------------------------ dispatch
+// The 4-cell epilogue (epilogue.cuh) needs nx % 4 == 0, 16-byte aligned m and
+// output, a scalar Ms and only terms with scalar parameters.
+template <typename R>
+static bool run4_eligible(const Geom& g, const R* m, const MsInfo& ms, const TermList& tl, const EpilogueArgs& ep) {
+    if (g.nx % 4 != 0 || ms.field64) return false;
+    if (ep.kind != EPI_H && ep.kind != EPI_LLG) return false;
+    if (((uintptr_t)m | (uintptr_t)ep.out) % 16 != 0) return false;
+    if (ep.kind == EPI_LLG && ((uintptr_t)ep.llg.m64 % 16 != 0)) return false;
+    for (int i = 0; i < tl.n; ++i) {
+        const TermDesc& t = tl.t[i];
+        switch (t.kind) {
+            case TK_DEMAG: case TK_EXCHANGE: case TK_CUBIC: break;
+            case TK_DMI: case TK_UNIAXIAL: case TK_ZEEMAN:
+                if (t.f0 || t.f1) return false;
+                break;
+            default: return false;
+        }
+    }
+    return true;
+}
+
+// ------------------------------------------------------------------ launches
 template <typename K> static void ct_smem(K kernel, size_t bytes) {
-    if (bytes > 48 * 1024) MAF_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    // opt in above 32 KB: the 48 KB default also has to hold the static shared memory
+    if (bytes > 32 * 1024) MAF_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
 }
 
 // tile widths: about 4096 (FP32) / 2048 (FP64) complex values per CTA for the
@@ -395,6 +445,7 @@ static void xinv_L(const cplx_t<R>* S1, int pitch, const void* tw, const void* t
     const size_t smem = sizeof(cplx_t<R>) * (size_t)NC * SB;
     const int64_t rows_pc = (int64_t)g.ny * g.nz;
     const unsigned blocks = (unsigned)ceil_div(rows_pc, NBR);
+    const int run4 = run4_eligible(g, m, ms, tl, ep) ? 1 : 0;
     if (nblocks) *nblocks = (int)blocks;
     const auto* t = static_cast<const cplx_t<R>*>(tw);
     const auto* tp = static_cast<const cplx_t<R>*>(twP);
@@ -402,19 +453,25 @@ static void xinv_L(const cplx_t<R>* S1, int pitch, const void* tw, const void* t
         case EPI_H: {
             auto k = k_xinv_ct<R, EPI_H, LC, NBR, NT>;
             ct_smem(k, smem);
-            k<<<blocks, NT, smem, st>>>(S1, pitch, t, tp, g, scale, m, ms, tl, ep);
+            k<<<blocks, NT, smem, st>>>(S1, pitch, t, tp, g, scale, m, ms, tl, ep, run4);
             break;
         }
         case EPI_LLG: {
             auto k = k_xinv_ct<R, EPI_LLG, LC, NBR, NT>;
             ct_smem(k, smem);
-            k<<<blocks, NT, smem, st>>>(S1, pitch, t, tp, g, scale, m, ms, tl, ep);
+            k<<<blocks, NT, smem, st>>>(S1, pitch, t, tp, g, scale, m, ms, tl, ep, run4);
+            break;
+        }
+        case EPI_EGRAD: {
+            auto k = k_xinv_ct<R, EPI_EGRAD, LC, NBR, NT>;
+            ct_smem(k, smem);
+            k<<<blocks, NT, smem, st>>>(S1, pitch, t, tp, g, scale, m, ms, tl, ep, run4);
             break;
         }
         default: {
             auto k = k_xinv_ct<R, EPI_EDENS, LC, NBR, NT>;
             ct_smem(k, smem);
-            k<<<blocks, NT, smem, st>>>(S1, pitch, t, tp, g, scale, m, ms, tl, ep);
+            k<<<blocks, NT, smem, st>>>(S1, pitch, t, tp, g, scale, m, ms, tl, ep, run4);
             break;
         }
     }

@@ -9,6 +9,7 @@
 // magnumaf/src/math.cpp:6-8 (max_4d_abs), magnumaf/src/util/util.cpp:34-42.
 #include "engine.hpp"
 #include "rk.hpp"
+#include "rng.cuh"
 
 namespace mafb {
 
@@ -217,6 +218,120 @@ __global__ void k_f2d(const float* __restrict__ a, double* __restrict__ b, int64
 void f32_to_f64(const float* a, double* b, int64_t n, cudaStream_t st) {
     const int64_t blocks = std::min<int64_t>(ceil_div(n, 256), 148LL * 16);
     k_f2d<<<(unsigned)blocks, 256, 0, st>>>(a, b, n);
+    MAF_LAUNCH_CHECK();
+}
+
+// ---------------------------------------------------------------------------
+// vector operations of the LBFGS minimiser (lbfgs_minimizer.cpp:44-46, 96-177)
+// ---------------------------------------------------------------------------
+constexpr int kRedBlocks = 148 * 2;
+
+// per-block partials: mode 0 sum a*b, mode 1 max |a| (NaN-propagating)
+__global__ void k_red_partials(const double* __restrict__ a, const double* __restrict__ b, int64_t n, int mode,
+                               double* __restrict__ part) {
+    double v = 0.0;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        if (mode == 0) v += a[i] * b[i];
+        else v = nanmax(v, fabs(a[i]));
+    }
+    __shared__ double red[32];
+    for (int o = 16; o > 0; o >>= 1) {
+        const double w = __shfl_down_sync(0xffffffffu, v, o);
+        v = mode == 0 ? v + w : nanmax(v, w);
+    }
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) red[wid] = v;
+    __syncthreads();
+    if (wid == 0) {
+        const int nw = (blockDim.x + 31) >> 5;
+        double s = lane < nw ? red[lane] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) {
+            const double w = __shfl_down_sync(0xffffffffu, s, o);
+            s = mode == 0 ? s + w : nanmax(s, w);
+        }
+        if (lane == 0) part[blockIdx.x] = s;
+    }
+}
+
+__global__ void k_red_final(const double* __restrict__ part, int nb, int mode, double* __restrict__ out) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        double s = 0.0;
+        for (int i = 0; i < nb; ++i) s = mode == 0 ? s + part[i] : nanmax(s, part[i]);
+        *out = s;
+    }
+}
+
+double reduce_host(const double* a, const double* b, int64_t n, int mode, double* scratch, cudaStream_t st) {
+    const int blocks = (int)std::min<int64_t>(ceil_div(n, 256), kRedBlocks);
+    k_red_partials<<<blocks, 256, 0, st>>>(a, b, n, mode, scratch);
+    MAF_LAUNCH_CHECK();
+    k_red_final<<<1, 32, 0, st>>>(scratch, blocks, mode, scratch + kRedBlocks);
+    MAF_LAUNCH_CHECK();
+    double v = 0;
+    MAF_CUDA(cudaMemcpyAsync(&v, scratch + kRedBlocks, sizeof(double), cudaMemcpyDeviceToHost, st));
+    MAF_CUDA(cudaStreamSynchronize(st));
+    return v;
+}
+
+double dot_host(const double* a, const double* b, int64_t n, double* scratch, cudaStream_t st) {
+    return reduce_host(a, b, n, 0, scratch, st);
+}
+
+double maxabs_host(const double* a, int64_t n, double* scratch, cudaStream_t st) {
+    return reduce_host(a, nullptr, n, 1, scratch, st);
+}
+
+__global__ void k_axpby(double* out, double a, const double* x, double b, const double* y, int64_t n) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double v = a * x[i];
+        out[i] = y ? v + b * y[i] : v;
+    }
+}
+
+void axpby(double* out, double a, const double* x, double b, const double* y, int64_t n, cudaStream_t st) {
+    const int64_t blocks = std::min<int64_t>(ceil_div(n, 256), 148LL * 16);
+    k_axpby<<<(unsigned)blocks, 256, 0, st>>>(out, a, x, b, y, n);
+    MAF_LAUNCH_CHECK();
+}
+
+// m = normalize(wa + stp * s) with the zero-safe normalize (lbfgs_minimizer.cpp:274-275)
+__global__ void k_normalize_combine(double* __restrict__ m, const double* __restrict__ wa, double stp,
+                                    const double* __restrict__ s, int64_t N) {
+    for (int64_t cell = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; cell < N;
+         cell += (int64_t)gridDim.x * blockDim.x) {
+        double v[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) v[c] = wa[c * N + cell] + stp * s[c * N + cell];
+        const double nrm = sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) m[c * N + cell] = nrm != 0 ? v[c] / nrm : 0.0;
+    }
+}
+
+void normalize_combine(double* m, const double* wa, double stp, const double* s, int64_t N, cudaStream_t st) {
+    const int64_t blocks = std::min<int64_t>(ceil_div(N, 256), 148LL * 8);
+    k_normalize_combine<<<(unsigned)blocks, 256, 0, st>>>(m, wa, stp, s, N);
+    MAF_LAUNCH_CHECK();
+}
+
+// thermal field sigma * xi(seed, member, index, cell) [3][N] (the h_th of
+// stochastic_integrator.cpp:11 as this library draws it)
+__global__ void k_noise(double* __restrict__ out, int64_t N, double sigma, unsigned long long seed, unsigned member,
+                        unsigned long long index) {
+    for (int64_t cell = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; cell < N;
+         cell += (int64_t)gridDim.x * blockDim.x) {
+        double xi[3];
+        normal3(seed, member, index, (uint64_t)cell, xi);
+        out[cell] = sigma * xi[0];
+        out[N + cell] = sigma * xi[1];
+        out[2 * N + cell] = sigma * xi[2];
+    }
+}
+
+void thermal_field(double* out, int64_t N, double sigma, unsigned long long seed, unsigned member,
+                   unsigned long long index, cudaStream_t st) {
+    const int64_t blocks = std::min<int64_t>(ceil_div(N, 256), 148LL * 8);
+    k_noise<<<(unsigned)blocks, 256, 0, st>>>(out, N, sigma, seed, member, index);
     MAF_LAUNCH_CHECK();
 }
 

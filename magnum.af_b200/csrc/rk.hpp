@@ -18,5 +18,12 @@ void normalize_m(double* m, int64_t N, int mode, unsigned long long* zero_count_
 void ms_field_from_m(const double* m, double Ms, double* msf, float* msf32, int64_t N, cudaStream_t st);
 void mean_m(const double* m, int64_t N, double* scratch, double* out_dev, cudaStream_t st);
 void f32_to_f64(const float* a, double* b, int64_t n, cudaStream_t st);
+void thermal_field(double* out, int64_t N, double sigma, unsigned long long seed, unsigned member,
+                   unsigned long long index, cudaStream_t st);
+// LBFGS vector operations; scratch needs 2*148+1 doubles; the reductions synchronise
+double dot_host(const double* a, const double* b, int64_t n, double* scratch, cudaStream_t st);
+double maxabs_host(const double* a, int64_t n, double* scratch, cudaStream_t st);
+void axpby(double* out, double a, const double* x, double b, const double* y, int64_t n, cudaStream_t st);
+void normalize_combine(double* m, const double* wa, double stp, const double* s, int64_t N, cudaStream_t st);
 
 }  // namespace mafb

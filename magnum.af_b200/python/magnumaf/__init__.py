@@ -89,6 +89,19 @@ _SIGS = {
     "maf_llg_integrate_dense": (_I, [_P, _P, _D, _D, _DP, _I, C.POINTER(_I)]),
     "maf_llg_rk_attempt": (_I, [_P, _P, C.c_char_p, _D, _DP, _DP]),
     "maf_llg_relax": (_I, [_P, _P, _D, _I]),
+    "maf_stochastic_llg_create": (_I, [C.POINTER(_P), _D, _D, _D, C.POINTER(_P), _I, C.c_char_p, C.c_ulonglong,
+                                       C.c_uint]),
+    "maf_stochastic_llg_destroy": (_I, [_P]),
+    "maf_stochastic_llg_step": (_I, [_P, _P]),
+    "maf_stochastic_llg_steps": (_I, [_P, _P, _I]),
+    "maf_stochastic_llg_E": (_I, [_P, _P, _DP]),
+    "maf_stochastic_llg_noise": (_I, [_P, _P, C.c_ulonglong, _DP]),
+    "maf_stochastic_llg_calls": (_I, [_P, C.POINTER(C.c_ulonglong)]),
+    "maf_lbfgs_create": (_I, [C.POINTER(_P), C.POINTER(_P), _I, _D, _I]),
+    "maf_lbfgs_destroy": (_I, [_P]),
+    "maf_lbfgs_add_term": (_I, [_P, _P]),
+    "maf_lbfgs_minimize": (_I, [_P, _P, _DP]),
+    "maf_lbfgs_stats": (_I, [_P, C.POINTER(C.c_ulonglong), C.POINTER(C.c_ulonglong), _DP]),
     "maf_llg_get_h": (_I, [_P, _DP]),
     "maf_llg_counters": (_I, [_P, C.POINTER(C.c_ulonglong)]),
 }
@@ -526,3 +539,78 @@ class LLGIntegrator:
             _ck(lib.maf_llg_pass_name(self._h, state._h, i, buf, 64))
             out.append((buf.value.decode(), float(ms[i])))
         return out
+
+
+class LBFGS_Minimizer:
+    """LBFGS_Minimizer(terms=[], tol=1e-6, maxiter=230, verbose=0) (python/magnumaf.pyx:1786-1835)."""
+
+    def __init__(self, terms: Sequence[FieldTerm] = (), tol=1e-6, maxiter=230, verbose=0):
+        self._h = _P()
+        self._terms = list(terms)
+        arr = (_P * max(1, len(self._terms)))(*[t._h for t in self._terms])
+        _ck(lib.maf_lbfgs_create(C.byref(self._h), arr, len(self._terms), float(tol), int(maxiter)))
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib.maf_lbfgs_destroy(self._h)
+            self._h = None
+
+    def add_terms(self, *args):
+        for t in args:
+            _ck(lib.maf_lbfgs_add_term(self._h, t._h))
+            self._terms.append(t)
+
+    def minimize(self, state: State) -> float:
+        v = C.c_double()
+        _ck(lib.maf_lbfgs_minimize(self._h, state._h, C.byref(v)))
+        return v.value
+
+    def stats(self):
+        it, fe = C.c_ulonglong(), C.c_ulonglong()
+        g = C.c_double()
+        _ck(lib.maf_lbfgs_stats(self._h, C.byref(it), C.byref(fe), C.byref(g)))
+        return {"iterations": it.value, "fevals": fe.value, "grad_max": g.value}
+
+
+class Stochastic_LLG:
+    """Stochastic_LLG(alpha, T, dt, state, terms=[], smode="Heun") (python/magnumaf.pyx:881-910):
+    fixed-step Heun / SemiHeun / detRK4 at temperature T [K] with time step dt [s].
+    ``seed`` and ``member`` select the counter-based random stream (the reference
+    seeds from the wall clock)."""
+
+    def __init__(self, alpha, T, dt, state: State, terms: Sequence[FieldTerm] = (), smode="Heun", seed=0,
+                 member=0):
+        self._h = _P()
+        self._terms = list(terms)
+        arr = (_P * max(1, len(self._terms)))(*[t._h for t in self._terms])
+        self.alpha, self.T, self.dt = float(alpha), float(T), float(dt)
+        _ck(lib.maf_stochastic_llg_create(C.byref(self._h), self.alpha, self.T, self.dt, arr, len(self._terms),
+                                          str(smode).encode(), int(seed), int(member)))
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib.maf_stochastic_llg_destroy(self._h)
+            self._h = None
+
+    def step(self, state: State):
+        _ck(lib.maf_stochastic_llg_step(self._h, state._h))
+
+    def steps(self, state: State, n: int):
+        _ck(lib.maf_stochastic_llg_steps(self._h, state._h, int(n)))
+
+    def Eeff_in_J(self, state: State) -> float:
+        v = C.c_double()
+        _ck(lib.maf_stochastic_llg_E(self._h, state._h, C.byref(v)))
+        return v.value
+
+    def thermal_field(self, state: State, index: int) -> np.ndarray:
+        """The thermal field h_th of noise index `index`, (nx, ny, nz, 3)."""
+        out = np.empty((state.mesh.nx, state.mesh.ny, state.mesh.nz, 3), order="F")
+        _ck(lib.maf_stochastic_llg_noise(self._h, state._h, int(index), _dptr(out)))
+        return out
+
+    @property
+    def calls(self) -> int:
+        v = C.c_ulonglong()
+        _ck(lib.maf_stochastic_llg_calls(self._h, C.byref(v)))
+        return v.value

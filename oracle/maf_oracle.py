@@ -919,6 +919,36 @@ def heun_step(state, terms, alpha, dt, h_th_prev, h_th):
     state.t += dt
 
 
+def semi_implicit_heun_step(state, terms, alpha, dt, h_th_init, h_th):
+    """stochastic_integrator.cpp:19-32 with given thermal fields."""
+    def f(m, h):
+        s = state.copy()
+        s.m = m
+        return LLG(alpha, m, Heff_in_Apm(terms, s) + h)
+    m1 = dt / 2. * f(state.m, h_th_init)
+    m2 = dt / 2. * f(state.m + m1, h_th)
+    m3 = dt / 2. * f(state.m + m2, h_th)
+    m4 = dt / 2. * f(state.m + m3, h_th)
+    m5 = dt / 2. * f(state.m + m4, h_th)
+    res = dt * f(state.m + m5, h_th)
+    state.m = normalize(state.m + res)
+    state.t += dt
+
+
+def det_rk4_step(state, terms, alpha, dt):
+    """stochastic_integrator.cpp:34-40 (deterministic RK4 reference)."""
+    def f(m):
+        s = state.copy()
+        s.m = m
+        return LLG(alpha, m, Heff_in_Apm(terms, s))
+    k1 = dt * f(state.m)
+    k2 = dt * f(state.m + 1. / 2. * k1)
+    k3 = dt * f(state.m + 1. / 2. * k2)
+    k4 = dt * f(state.m + k3)
+    state.m = normalize(state.m + (k1 + 2. * k2 + 2. * k3 + k4) / 6.)
+    state.t += dt
+
+
 # ---------------------------------------------------------------------------
 # util reductions (util.cpp:30-55)
 # ---------------------------------------------------------------------------
