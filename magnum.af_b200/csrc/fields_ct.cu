@@ -6,6 +6,8 @@
 // batch into registers before they are written to shared memory, and the
 // z convolution handles the rows ky and Py - ky in one CTA so that the stored
 // tensor quadrant is read from HBM once.
+#include <algorithm>
+
 #include "ct_dispatch.hpp"
 #include "epilogue.cuh"
 #include "fft_ct.cuh"
@@ -108,6 +110,76 @@ __global__ void __launch_bounds__(NT) k_cols_ct(const cplx_t<R>* in, cplx_t<R>* 
         const int b = idx % NB;
         if (i < n_out && b < ncv) ob[i * out_si + b] = s[spad(i) * NB + b];
     }
+}
+
+// ---------------------------------------------- pipelined strided columns
+// Persistent CTAs loop over the column tiles; the next tile is fetched into the
+// second shared-memory buffer with cp.async (zero-filled where the transform is
+// padded) while the current one is transformed, so HBM reads overlap the FFT.
+template <int BYTES> __device__ __forceinline__ void cp_async_zfill(void* smem, const void* gmem, bool valid) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    const int n = valid ? BYTES : 0;
+    if constexpr (BYTES == 16)
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(n));
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;\n" ::"r"(s), "l"(gmem), "n"(BYTES), "r"(n));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N> __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
+template <typename R, int DIR, int L, int NB, int NT>
+__global__ void __launch_bounds__(NT) k_cols_pipe(const cplx_t<R>* in, cplx_t<R>* out, int n_in, int n_out, int ncols,
+                                                  int64_t in_si, int64_t out_si, int64_t in_sbat, int64_t out_sbat,
+                                                  int nbat, const cplx_t<R>* __restrict__ tw) {
+    using C = cplx_t<R>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    constexpr int LP = (L - 1) + ((L - 1) >> 4) + 1;
+    constexpr int E = L * NB / NT;
+    static_assert(L * NB % NT == 0, "tile");
+    C* const buf0 = reinterpret_cast<C*>(smem_raw);
+    const int ntx = (ncols + NB - 1) / NB;
+    const int tiles = ntx * nbat;
+    auto issue = [&](int t, C* dst) {
+        const int bat = t / ntx;
+        const int c0 = (t - bat * ntx) * NB;
+        const int ncv = min(NB, ncols - c0);
+        const C* ib = in + (int64_t)bat * in_sbat + c0;
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            const int idx = threadIdx.x + e * NT;
+            const int i = idx / NB;
+            const int b = idx % NB;
+            const bool valid = i < n_in && b < ncv;
+            cp_async_zfill<sizeof(C)>(dst + spad(i) * NB + b, valid ? ib + i * in_si + b : ib, valid);
+        }
+    };
+    int cur = 0;
+    int t = blockIdx.x;
+    if (t < tiles) issue(t, buf0);
+    cp_async_commit();
+    for (; t < tiles; t += gridDim.x) {
+        const int tn = t + gridDim.x;
+        if (tn < tiles) issue(tn, buf0 + (cur ^ 1) * (LP * NB));
+        cp_async_commit();
+        cp_async_wait<1>();
+        __syncthreads();
+        C* s = buf0 + cur * (LP * NB);
+        ct_fft<R, DIR, true, L, NB, NT>(s, 0, tw, typename CtPlan<L>::T());
+        const int bat = t / ntx;
+        const int c0 = (t - bat * ntx) * NB;
+        const int ncv = min(NB, ncols - c0);
+        C* ob = out + (int64_t)bat * out_sbat + c0;
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            const int idx = threadIdx.x + e * NT;
+            const int i = idx / NB;
+            const int b = idx % NB;
+            if (i < n_out && b < ncv) ob[i * out_si + b] = s[spad(i) * NB + b];
+        }
+        __syncthreads();
+        cur ^= 1;
+    }
+    cp_async_wait<0>();
 }
 
 // -------------------------------------------------- z convolution (3-D meshes)
@@ -401,11 +473,20 @@ static void cols_L(const cplx_t<R>* in, cplx_t<R>* out, int n_in, int n_out, int
     constexpr int NT = L * NB / kE;
     static_assert(NT <= kMaxFftThreads, "CTA size");
     const size_t smem = sizeof(cplx_t<R>) * (size_t)NB * ((L - 1) + ((L - 1) >> 4) + 1);
-    auto k = k_cols_ct<R, DIR, L, NB, NT>;
-    ct_smem(k, smem);
-    dim3 grid((unsigned)ceil_div(ncols, NB), (unsigned)nbat);
-    k<<<grid, NT, smem, st>>>(in, out, n_in, n_out, ncols, in_si, out_si, in_sbat, out_sbat,
-                              static_cast<const cplx_t<R>*>(tw));
+    // persistent, double-buffered: as many CTAs as fit, each looping over tiles
+    auto k = k_cols_pipe<R, DIR, L, NB, NT>;
+    ct_smem(k, 2 * smem);
+    static int per_sm = 0;
+    if (!per_sm) {
+        MAF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, NT, 2 * smem));
+        per_sm = std::max(per_sm, 1);
+    }
+    int sms = 0;
+    MAF_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0));
+    const int64_t tiles = ceil_div(ncols, NB) * (int64_t)nbat;
+    const unsigned grid = (unsigned)std::min<int64_t>(tiles, (int64_t)sms * per_sm);
+    k<<<grid, NT, 2 * smem, st>>>(in, out, n_in, n_out, ncols, in_si, out_si, in_sbat, out_sbat, nbat,
+                                  static_cast<const cplx_t<R>*>(tw));
     MAF_LAUNCH_CHECK();
 }
 
