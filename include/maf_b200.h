@@ -212,6 +212,22 @@ int maf_lbfgs_stats(maf_lbfgs h, unsigned long long* iterations, unsigned long l
 int maf_llg_get_h(maf_llg l, double* h);
 int maf_llg_counters(maf_llg l, unsigned long long out[4]);
 
+/* ------------------------------------------------- no-allocation mean ---
+ * No counterpart in the reference.  <m> of a device-resident FP64 field
+ * m_dev[3][ncells] (e.g. from maf_state_device_m), with the definition of
+ * maf_state_mean_m: sum over cells / number of cells with |m| != 0.  It
+ * allocates no device memory, for callers that must not: code sampling <m>
+ * between steps while other streams run (cudaMalloc can synchronise the
+ * device), or an application that has reserved all free device memory.
+ * Its scratch is a fixed 128 KiB static device array per device, which limits
+ * ncells to 33554432 (2^25); larger ncells return MAF_ERR_BADARG.  The first
+ * call on a device looks up that array's address.  Work is queued on
+ * cuda_stream (NULL: the legacy default stream) and the call returns after that
+ * stream has finished it.  Calls that overlap on one device (other streams or
+ * host threads, unordered) share the scratch and race: both results are then
+ * undefined. */
+int maf_mean_m_noalloc(const double* m_dev, long long ncells, double out[3], void* cuda_stream);
+
 #ifdef __cplusplus
 }
 #endif

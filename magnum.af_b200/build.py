@@ -31,6 +31,7 @@ SOURCES = {
     "llg.cu": [],
     "newell.cu": ["-fmad=false"],
     "capi.cu": [],
+    "noalloc.cu": [],
 }
 
 

@@ -7,6 +7,7 @@
 #include <vector>
 
 #include "../../include/maf_b200.h"
+#include "capi_internal.hpp"
 #include "engine.hpp"
 #include "rk.hpp"
 
@@ -162,6 +163,16 @@ Scheme make_scheme(const std::string& name) {
 }
 
 }  // namespace
+
+// Error handling shared with entry points defined in other translation units:
+// runs f after the device check and maps exceptions to status codes and
+// maf_last_error() exactly like the entry points in this file.
+int mafb::capi_run(const std::function<void()>& f) {
+    return guarded([&] {
+        require_device();
+        f();
+    });
+}
 
 // ---------------------------------------------------------------------------
 // handle structs

@@ -104,6 +104,7 @@ _SIGS = {
     "maf_lbfgs_stats": (_I, [_P, C.POINTER(C.c_ulonglong), C.POINTER(C.c_ulonglong), _DP]),
     "maf_llg_get_h": (_I, [_P, _DP]),
     "maf_llg_counters": (_I, [_P, C.POINTER(C.c_ulonglong)]),
+    "maf_mean_m_noalloc": (_I, [_P, C.c_longlong, _DP, _P]),
 }
 for _name, (_res, _args) in _SIGS.items():
     _f = getattr(lib, _name)
