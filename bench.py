@@ -122,6 +122,11 @@ class ClockSampler:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.Q,
                                           "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.f,
                                          stderr=subprocess.DEVNULL)
+            # nvidia-smi needs a moment before its first sample: wait for it so
+            # that the samples cover the timed region that follows
+            t0 = time.time()
+            while time.time() - t0 < 3.0 and os.path.getsize(self.path) == 0:
+                time.sleep(0.02)
         except Exception:
             self.proc = None
 
@@ -286,8 +291,8 @@ def run_ours(args):
     clk = ClockSampler(local)
     clk.start()
     ms32 = timed(f32, args.steps, args.warmup)
-    clocks = clk.stop()
     ms64 = timed(f64, args.steps, args.warmup)
+    clocks = clk.stop()
 
     # accuracy of the FP32-field form against the FP64 form on the full mesh
     f32()
@@ -340,7 +345,8 @@ def run_ours(args):
         "vs_baseline": None,
         "dtype": "f32",
         "data": "synthetic (seeded random m on the unit sphere, random 50 mT-ball Zeeman field)",
-        "config": {"workload": "H_eff demag+exchange+cubic+Zeeman, 1024x1024x16 cells of 3 nm (FP32-field form)",
+        "config": {"workload": "H_eff demag+exchange+cubic+Zeeman, %dx%dx%d cells of 3 nm (FP32-field form)"
+                               % (NX, NY, NZ),
                    "cells": NX * NY * NZ, "parallelism": "replicas x%d" % world,
                    "l2": "inputs larger than L2 (m 201 MB, spectra 403-806 MB per pass)"},
         "fp64_form": {"value": world * args.steps / (ms64 * 1e-3), "ms_per_step": ms64 / args.steps,

@@ -121,6 +121,141 @@ __device__ __forceinline__ void ct_fft(cplx_t<R>* s, int sb, const cplx_t<R>* __
     ct_run<R, DIR, BFAST, L, 1, NB, NT, RS...>(s, sb, tw);
 }
 
+// ----------------------------------------------------------------------------
+// Stages with global I/O fused in.  The first stage (Ns = 1, no twiddles) takes
+// its RAD inputs j + r L/RAD of column b from ld(b, i) -- straight from global
+// memory into registers, so the zero-padded half of a transform costs no
+// shared-memory traffic -- and writes its outputs j RAD + r to shared memory.
+// The last stage (Ns = L/RAD) reads shared memory and hands its outputs
+// j + r Ns to st(b, i, value), so rows that are truncated are never stored.
+// Each saves one shared-memory round trip and one barrier per element.
+// ----------------------------------------------------------------------------
+template <bool BFAST, int NB, int NBF> __device__ __forceinline__ void ct_bj(int q, int& b, int& j) {
+    b = BFAST ? q % NB : q / NBF;
+    j = BFAST ? q / NB : q % NBF;
+}
+
+// The caller synchronises before s is overwritten; ends with a barrier.
+template <typename R, int RAD, int DIR, bool BFAST, int L, int NB, int NT, typename LD>
+__device__ __forceinline__ void ct_stage_in(cplx_t<R>* s, int sb, LD&& ld) {
+    using C = cplx_t<R>;
+    constexpr int NBF = L / RAD;
+    constexpr int TOTAL = NBF * NB;
+    constexpr int BPT = (TOTAL + NT - 1) / NT;
+    C v[BPT][RAD];
+#pragma unroll
+    for (int k = 0; k < BPT; ++k) {
+        const int q = threadIdx.x + k * NT;
+        if (TOTAL % NT == 0 || q < TOTAL) {
+            int b, j;
+            ct_bj<BFAST, NB, NBF>(q, b, j);
+#pragma unroll
+            for (int r = 0; r < RAD; ++r) v[k][r] = ld(b, j + r * NBF);
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < BPT; ++k) {
+        const int q = threadIdx.x + k * NT;
+        if (TOTAL % NT == 0 || q < TOTAL) {
+            int b, j;
+            ct_bj<BFAST, NB, NBF>(q, b, j);
+            bfly_ct<RAD, DIR, R>(v[k]);
+#pragma unroll
+            for (int r = 0; r < RAD; ++r) {
+                const int i = j * RAD + r;
+                s[BFAST ? spad(i) * NB + b : spad(i) + b * sb] = v[k][r];
+            }
+        }
+    }
+    __syncthreads();
+}
+
+// Reads s written by the previous stage (which ended with a barrier); no
+// barrier at the end: the caller synchronises before s is reused.
+template <typename R, int RAD, int DIR, bool BFAST, int L, int NB, int NT, typename ST>
+__device__ __forceinline__ void ct_stage_out(const cplx_t<R>* s, int sb, const cplx_t<R>* __restrict__ tw, ST&& st) {
+    using C = cplx_t<R>;
+    constexpr int NBF = L / RAD;
+    constexpr int NS = NBF;
+    constexpr int TOTAL = NBF * NB;
+    constexpr int BPT = (TOTAL + NT - 1) / NT;
+#pragma unroll
+    for (int k = 0; k < BPT; ++k) {
+        const int q = threadIdx.x + k * NT;
+        if (TOTAL % NT == 0 || q < TOTAL) {
+            int b, j;
+            ct_bj<BFAST, NB, NBF>(q, b, j);
+            C v[RAD];
+#pragma unroll
+            for (int r = 0; r < RAD; ++r) {
+                const int i = j + r * NBF;
+                C x = s[BFAST ? spad(i) * NB + b : spad(i) + b * sb];
+                if (NS > 1 && r > 0) {
+                    const C w = tw[r * j];
+                    x = DIR < 0 ? cmul(x, w) : cmulc(x, w);
+                }
+                v[r] = x;
+            }
+            bfly_ct<RAD, DIR, R>(v);
+#pragma unroll
+            for (int r = 0; r < RAD; ++r) st(b, j + r * NS, v[r]);
+        }
+    }
+}
+
+template <typename R, int DIR, bool BFAST, int L, int NS, int NB, int NT, typename ST, int RAD, int... REST>
+__device__ __forceinline__ void ct_run_out(cplx_t<R>* s, int sb, const cplx_t<R>* __restrict__ tw, ST&& st) {
+    if constexpr (sizeof...(REST) == 0) {
+        static_assert(NS * RAD == L, "radix sequence");
+        ct_stage_out<R, RAD, DIR, BFAST, L, NB, NT>(s, sb, tw, st);
+    } else {
+        ct_stage<R, RAD, DIR, BFAST, L, NS, NB, NT>(s, sb, tw);
+        ct_run_out<R, DIR, BFAST, L, NS * RAD, NB, NT, ST, REST...>(s, sb, tw, st);
+    }
+}
+
+// global -> first stage -> ... -> last stage, result in shared memory
+template <typename R, int DIR, bool BFAST, int L, int NB, int NT, typename LD, int R0, int... RS>
+__device__ __forceinline__ void ct_fft_in(cplx_t<R>* s, int sb, const cplx_t<R>* __restrict__ tw, LD&& ld,
+                                          Radices<R0, RS...>) {
+    ct_stage_in<R, R0, DIR, BFAST, L, NB, NT>(s, sb, ld);
+    if constexpr (sizeof...(RS) > 0) ct_run<R, DIR, BFAST, L, R0, NB, NT, RS...>(s, sb, tw);
+}
+
+// shared memory -> ... -> last stage -> global
+template <typename R, int DIR, bool BFAST, int L, int NB, int NT, typename ST, int... RS>
+__device__ __forceinline__ void ct_fft_out(cplx_t<R>* s, int sb, const cplx_t<R>* __restrict__ tw, ST&& st,
+                                           Radices<RS...>) {
+    ct_run_out<R, DIR, BFAST, L, 1, NB, NT, ST, RS...>(s, sb, tw, st);
+}
+
+// global -> ... -> global; the caller synchronises before s is reused
+template <typename R, int DIR, bool BFAST, int L, int NB, int NT, typename LD, typename ST, int R0, int... RS>
+__device__ __forceinline__ void ct_fft_io(cplx_t<R>* s, int sb, const cplx_t<R>* __restrict__ tw, LD&& ld, ST&& st,
+                                          Radices<R0, RS...>) {
+    if constexpr (sizeof...(RS) == 0) {
+        // one stage: load, butterfly, store; shared memory is not used
+        static_assert(R0 == L, "radix sequence");
+        using C = cplx_t<R>;
+        constexpr int BPT = (NB + NT - 1) / NT;
+#pragma unroll
+        for (int k = 0; k < BPT; ++k) {
+            const int q = threadIdx.x + k * NT;
+            if (NB % NT == 0 || q < NB) {
+                C v[R0];
+#pragma unroll
+                for (int r = 0; r < R0; ++r) v[r] = ld(q, r);
+                bfly_ct<R0, DIR, R>(v);
+#pragma unroll
+                for (int r = 0; r < R0; ++r) st(q, r, v[r]);
+            }
+        }
+    } else {
+        ct_stage_in<R, R0, DIR, BFAST, L, NB, NT>(s, sb, ld);
+        ct_run_out<R, DIR, BFAST, L, R0, NB, NT, ST, RS...>(s, sb, tw, st);
+    }
+}
+
 // radix sequence per power-of-two length (16 first, smaller radices last)
 template <int L> struct CtPlan;
 template <> struct CtPlan<2> { using T = Radices<2>; };

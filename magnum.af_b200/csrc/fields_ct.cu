@@ -14,6 +14,11 @@
 
 namespace mafb {
 
+// Resident CTAs per SM that a kernel is compiled for (a register cap): at
+// least T32 threads per SM in FP32, T64 in FP64.
+template <typename R, int NT, int T32, int T64>
+constexpr int kMinBlocks = (sizeof(R) == 4 ? T32 : T64) / NT > 1 ? (sizeof(R) == 4 ? T32 : T64) / NT : 1;
+
 // ------------------------------------------------------------------ x forward
 template <typename R, int LC, int NB, int NT>
 __global__ void __launch_bounds__(NT) k_xfwd_ct(const R* __restrict__ in, int n_in, int64_t rows, int64_t rows_pc,
@@ -73,113 +78,26 @@ __global__ void __launch_bounds__(NT) k_xfwd_ct(const R* __restrict__ in, int n_
 }
 
 // ------------------------------------------------------------ strided columns
+// Batched column transforms (the y passes): the first radix stage loads its
+// inputs straight from global memory (rows >= n_in are the zero padding and
+// are not read), the last stage stores straight to global memory (rows >=
+// n_out are truncated and not written).
 template <typename R, int DIR, int L, int NB, int NT>
-__global__ void __launch_bounds__(NT) k_cols_ct(const cplx_t<R>* in, cplx_t<R>* out, int n_in, int n_out, int ncols,
+__global__ void __launch_bounds__(NT, (kMinBlocks<R, NT, 1024, 512>)) k_cols_ct(const cplx_t<R>* in, cplx_t<R>* out, int n_in, int n_out, int ncols,
                                                 int64_t in_si, int64_t out_si, int64_t in_sbat, int64_t out_sbat,
                                                 const cplx_t<R>* __restrict__ tw) {
     using C = cplx_t<R>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C* s = reinterpret_cast<C*>(smem_raw);
-    constexpr int E = L * NB / NT;
-    static_assert(L * NB % NT == 0, "tile");
     const int c0 = blockIdx.x * NB;
     const C* ib = in + (int64_t)blockIdx.y * in_sbat + c0;
     C* ob = out + (int64_t)blockIdx.y * out_sbat + c0;
     const int ncv = min(NB, ncols - c0);
-    C v[E];
-#pragma unroll
-    for (int e = 0; e < E; ++e) {
-        const int idx = threadIdx.x + e * NT;
-        const int i = idx / NB;
-        const int b = idx % NB;
-        C x = mk((R)0, (R)0);
-        if (i < n_in && b < ncv) x = ib[i * in_si + b];
-        v[e] = x;
-    }
-#pragma unroll
-    for (int e = 0; e < E; ++e) {
-        const int idx = threadIdx.x + e * NT;
-        s[spad(idx / NB) * NB + idx % NB] = v[e];
-    }
-    __syncthreads();
-    ct_fft<R, DIR, true, L, NB, NT>(s, 0, tw, typename CtPlan<L>::T());
-#pragma unroll
-    for (int e = 0; e < E; ++e) {
-        const int idx = threadIdx.x + e * NT;
-        const int i = idx / NB;
-        const int b = idx % NB;
-        if (i < n_out && b < ncv) ob[i * out_si + b] = s[spad(i) * NB + b];
-    }
-}
-
-// ---------------------------------------------- pipelined strided columns
-// Persistent CTAs loop over the column tiles; the next tile is fetched into the
-// second shared-memory buffer with cp.async (zero-filled where the transform is
-// padded) while the current one is transformed, so HBM reads overlap the FFT.
-template <int BYTES> __device__ __forceinline__ void cp_async_zfill(void* smem, const void* gmem, bool valid) {
-    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-    const int n = valid ? BYTES : 0;
-    if constexpr (BYTES == 16)
-        asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(n));
-    else
-        asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;\n" ::"r"(s), "l"(gmem), "n"(BYTES), "r"(n));
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
-template <int N> __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
-
-template <typename R, int DIR, int L, int NB, int NT>
-__global__ void __launch_bounds__(NT) k_cols_pipe(const cplx_t<R>* in, cplx_t<R>* out, int n_in, int n_out, int ncols,
-                                                  int64_t in_si, int64_t out_si, int64_t in_sbat, int64_t out_sbat,
-                                                  int nbat, const cplx_t<R>* __restrict__ tw) {
-    using C = cplx_t<R>;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    constexpr int LP = (L - 1) + ((L - 1) >> 4) + 1;
-    constexpr int E = L * NB / NT;
-    static_assert(L * NB % NT == 0, "tile");
-    C* const buf0 = reinterpret_cast<C*>(smem_raw);
-    const int ntx = (ncols + NB - 1) / NB;
-    const int tiles = ntx * nbat;
-    auto issue = [&](int t, C* dst) {
-        const int bat = t / ntx;
-        const int c0 = (t - bat * ntx) * NB;
-        const int ncv = min(NB, ncols - c0);
-        const C* ib = in + (int64_t)bat * in_sbat + c0;
-#pragma unroll
-        for (int e = 0; e < E; ++e) {
-            const int idx = threadIdx.x + e * NT;
-            const int i = idx / NB;
-            const int b = idx % NB;
-            const bool valid = i < n_in && b < ncv;
-            cp_async_zfill<sizeof(C)>(dst + spad(i) * NB + b, valid ? ib + i * in_si + b : ib, valid);
-        }
+    auto ld = [&](int b, int i) -> C { return (i < n_in && b < ncv) ? ib[i * in_si + b] : mk((R)0, (R)0); };
+    auto st = [&](int b, int i, C v) {
+        if (i < n_out && b < ncv) ob[i * out_si + b] = v;
     };
-    int cur = 0;
-    int t = blockIdx.x;
-    if (t < tiles) issue(t, buf0);
-    cp_async_commit();
-    for (; t < tiles; t += gridDim.x) {
-        const int tn = t + gridDim.x;
-        if (tn < tiles) issue(tn, buf0 + (cur ^ 1) * (LP * NB));
-        cp_async_commit();
-        cp_async_wait<1>();
-        __syncthreads();
-        C* s = buf0 + cur * (LP * NB);
-        ct_fft<R, DIR, true, L, NB, NT>(s, 0, tw, typename CtPlan<L>::T());
-        const int bat = t / ntx;
-        const int c0 = (t - bat * ntx) * NB;
-        const int ncv = min(NB, ncols - c0);
-        C* ob = out + (int64_t)bat * out_sbat + c0;
-#pragma unroll
-        for (int e = 0; e < E; ++e) {
-            const int idx = threadIdx.x + e * NT;
-            const int i = idx / NB;
-            const int b = idx % NB;
-            if (i < n_out && b < ncv) ob[i * out_si + b] = s[spad(i) * NB + b];
-        }
-        __syncthreads();
-        cur ^= 1;
-    }
-    cp_async_wait<0>();
+    ct_fft_io<R, DIR, true, L, NB, NT>(s, 0, tw, ld, st, typename CtPlan<L>::T());
 }
 
 // -------------------------------------------------- z convolution (3-D meshes)
@@ -187,13 +105,12 @@ __global__ void __launch_bounds__(NT) k_cols_pipe(const cplx_t<R>* in, cplx_t<R>
 // row, sign of Nxy and Nyz flipped for the second); ky = 0 and ky = ny are
 // their own mirrors and run alone.
 template <typename R, int L, int NB, int NT>
-__global__ void __launch_bounds__(NT) k_convz_ct(cplx_t<R>* S, const R* __restrict__ Nred, int nz, int ny, int nxh,
+__global__ void __launch_bounds__(NT, (kMinBlocks<R, NT, 768, 512>)) k_convz_ct(cplx_t<R>* S, const R* __restrict__ Nred, int nz, int ny, int nxh,
                                                  int pitch, const cplx_t<R>* __restrict__ tw) {
     using C = cplx_t<R>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C* s = reinterpret_cast<C*>(smem_raw);
     constexpr int NC = 6 * NB;  // columns: (row, comp, b)
-    constexpr int E = L * NC / NT;
     static_assert(L * NC % NT == 0, "tile");
     const int Py = 2 * ny;
     const int ky = blockIdx.y;
@@ -203,27 +120,20 @@ __global__ void __launch_bounds__(NT) k_convz_ct(cplx_t<R>* S, const R* __restri
     const int ncv = min(NB, nxh - c0);
     const int64_t si = (int64_t)Py * pitch;        // z stride
     const int64_t cs = (int64_t)nz * Py * pitch;   // component stride
-    C v[E];
-#pragma unroll
-    for (int e = 0; e < E; ++e) {
-        const int idx = threadIdx.x + e * NT;
-        const int i = idx / NC;
-        const int col = idx % NC;
+    // column col = (row, comp, b) of the tile at z = i; rows i >= nz are padding
+    auto at = [&](int col, int i, bool& ok) -> int64_t {
         const int row = col / (3 * NB);
         const int comp = (col / NB) % 3;
         const int b = col % NB;
-        C x = mk((R)0, (R)0);
-        if (i < nz && b < ncv && (row == 0 || two))
-            x = S[comp * cs + i * si + (int64_t)(row ? ky2 : ky) * pitch + c0 + b];
-        v[e] = x;
-    }
-#pragma unroll
-    for (int e = 0; e < E; ++e) {
-        const int idx = threadIdx.x + e * NT;
-        s[spad(idx / NC) * NC + idx % NC] = v[e];
-    }
-    __syncthreads();
-    ct_fft<R, -1, true, L, NC, NT>(s, 0, tw, typename CtPlan<L>::T());
+        ok = i < nz && b < ncv && (row == 0 || two);
+        return comp * cs + i * si + (int64_t)(row ? ky2 : ky) * pitch + c0 + b;
+    };
+    auto ld = [&](int col, int i) -> C {
+        bool ok;
+        const int64_t o = at(col, i, ok);
+        return ok ? S[o] : mk((R)0, (R)0);
+    };
+    ct_fft_in<R, -1, true, L, NC, NT>(s, 0, tw, ld, typename CtPlan<L>::T());
     const int Pz = 2 * nz;
     const int64_t tcs = (int64_t)(nz + 1) * (ny + 1) * nxh;
     for (int idx = threadIdx.x; idx < L * NB; idx += NT) {
@@ -248,18 +158,12 @@ __global__ void __launch_bounds__(NT) k_convz_ct(cplx_t<R>* S, const R* __restri
         }
     }
     __syncthreads();
-    ct_fft<R, 1, true, L, NC, NT>(s, 0, tw, typename CtPlan<L>::T());
-#pragma unroll
-    for (int e = 0; e < E; ++e) {
-        const int idx = threadIdx.x + e * NT;
-        const int i = idx / NC;
-        const int col = idx % NC;
-        const int row = col / (3 * NB);
-        const int comp = (col / NB) % 3;
-        const int b = col % NB;
-        if (i < nz && b < ncv && (row == 0 || two))
-            S[comp * cs + i * si + (int64_t)(row ? ky2 : ky) * pitch + c0 + b] = s[spad(i) * NC + col];
-    }
+    auto st = [&](int col, int i, C v) {
+        bool ok;
+        const int64_t o = at(col, i, ok);
+        if (ok) S[o] = v;
+    };
+    ct_fft_out<R, 1, true, L, NC, NT>(s, 0, tw, st, typename CtPlan<L>::T());
 }
 
 // -------------------------------------------------- y convolution (nz == 1)
@@ -270,30 +174,16 @@ __global__ void __launch_bounds__(NT) k_convy_ct(cplx_t<R>* S, const R* __restri
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C* s = reinterpret_cast<C*>(smem_raw);
     constexpr int NC = 3 * NB;
-    constexpr int E = L * NC / NT;
     static_assert(L * NC % NT == 0, "tile");
     const int c0 = blockIdx.x * NB;
     const int ncv = min(NB, nxh - c0);
     const int64_t cs = (int64_t)ny * pitch;
-    C v[E];
-#pragma unroll
-    for (int e = 0; e < E; ++e) {
-        const int idx = threadIdx.x + e * NT;
-        const int i = idx / NC;
-        const int col = idx % NC;
-        const int comp = col / NB;
-        const int b = col % NB;
-        C x = mk((R)0, (R)0);
-        if (i < ny && b < ncv) x = S[comp * cs + (int64_t)i * pitch + c0 + b];
-        v[e] = x;
-    }
-#pragma unroll
-    for (int e = 0; e < E; ++e) {
-        const int idx = threadIdx.x + e * NT;
-        s[spad(idx / NC) * NC + idx % NC] = v[e];
-    }
-    __syncthreads();
-    ct_fft<R, -1, true, L, NC, NT>(s, 0, tw, typename CtPlan<L>::T());
+    // column col = (comp, b) at y = i; rows i >= ny are padding
+    auto ld = [&](int col, int i) -> C {
+        const int comp = col / NB, b = col % NB;
+        return (i < ny && b < ncv) ? S[comp * cs + (int64_t)i * pitch + c0 + b] : mk((R)0, (R)0);
+    };
+    ct_fft_in<R, -1, true, L, NC, NT>(s, 0, tw, ld, typename CtPlan<L>::T());
     const int64_t tcs = (int64_t)(ny + 1) * nxh;
     for (int idx = threadIdx.x; idx < L * NB; idx += NT) {
         const int ky = idx / NB;
@@ -310,16 +200,11 @@ __global__ void __launch_bounds__(NT) k_convy_ct(cplx_t<R>* S, const R* __restri
         s[base + 2 * NB] = cscale(mz, Nzz);
     }
     __syncthreads();
-    ct_fft<R, 1, true, L, NC, NT>(s, 0, tw, typename CtPlan<L>::T());
-#pragma unroll
-    for (int e = 0; e < E; ++e) {
-        const int idx = threadIdx.x + e * NT;
-        const int i = idx / NC;
-        const int col = idx % NC;
-        const int comp = col / NB;
-        const int b = col % NB;
-        if (i < ny && b < ncv) S[comp * cs + (int64_t)i * pitch + c0 + b] = s[spad(i) * NC + col];
-    }
+    auto st = [&](int col, int i, C v) {
+        const int comp = col / NB, b = col % NB;
+        if (i < ny && b < ncv) S[comp * cs + (int64_t)i * pitch + c0 + b] = v;
+    };
+    ct_fft_out<R, 1, true, L, NC, NT>(s, 0, tw, st, typename CtPlan<L>::T());
 }
 
 // --------------------------------------------------- x inverse + epilogue
@@ -473,20 +358,11 @@ static void cols_L(const cplx_t<R>* in, cplx_t<R>* out, int n_in, int n_out, int
     constexpr int NT = L * NB / kE;
     static_assert(NT <= kMaxFftThreads, "CTA size");
     const size_t smem = sizeof(cplx_t<R>) * (size_t)NB * ((L - 1) + ((L - 1) >> 4) + 1);
-    // persistent, double-buffered: as many CTAs as fit, each looping over tiles
-    auto k = k_cols_pipe<R, DIR, L, NB, NT>;
-    ct_smem(k, 2 * smem);
-    static int per_sm = 0;
-    if (!per_sm) {
-        MAF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, NT, 2 * smem));
-        per_sm = std::max(per_sm, 1);
-    }
-    int sms = 0;
-    MAF_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0));
-    const int64_t tiles = ceil_div(ncols, NB) * (int64_t)nbat;
-    const unsigned grid = (unsigned)std::min<int64_t>(tiles, (int64_t)sms * per_sm);
-    k<<<grid, NT, 2 * smem, st>>>(in, out, n_in, n_out, ncols, in_si, out_si, in_sbat, out_sbat, nbat,
-                                  static_cast<const cplx_t<R>*>(tw));
+    auto k = k_cols_ct<R, DIR, L, NB, NT>;
+    ct_smem(k, smem);
+    dim3 grid((unsigned)ceil_div(ncols, NB), (unsigned)nbat);
+    k<<<grid, NT, smem, st>>>(in, out, n_in, n_out, ncols, in_si, out_si, in_sbat, out_sbat,
+                              static_cast<const cplx_t<R>*>(tw));
     MAF_LAUNCH_CHECK();
 }
 
@@ -518,7 +394,9 @@ static void convy_L(cplx_t<R>* S, const R* Nred, int ny, int nxh, int pitch, con
 template <typename R, int LC>
 static void xinv_L(const cplx_t<R>* S1, int pitch, const void* tw, const void* twP, const Geom& g, R scale, const R* m,
                    const MsInfo& ms, const TermList& tl, const EpilogueArgs& ep, cudaStream_t st, int* nblocks) {
-    constexpr int NBR = pow2floor(cmax(1, kTileC<R> / (3 * LC)));
+    // half the column-pass tile: the epilogue's register demand allows one
+    // 384-thread CTA per SM, two CTAs of half the rows overlap their phases
+    constexpr int NBR = pow2floor(cmax(1, kTileC<R> / (6 * LC)));
     constexpr int NC = 3 * NBR;
     constexpr int NT = LC * NC / kE;
     static_assert(NT <= kMaxFftThreads, "CTA size");
