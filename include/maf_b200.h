@@ -212,6 +212,33 @@ int maf_lbfgs_stats(maf_lbfgs h, unsigned long long* iterations, unsigned long l
 int maf_llg_get_h(maf_llg l, double* h);
 int maf_llg_counters(maf_llg l, unsigned long long out[4]);
 
+/* ------------------------------------------------------- String method ---
+ * StringMethod(state, inputimages, n_interp, dt, llg)
+ * (magnumaf/include/magnumaf/solvers/string_method.hpp:9-39, magnumaf/src/solvers/string_method.cpp:12-46):
+ * n_interp images on the device, linearly interpolated along the arc length of
+ * the input images (at least two, on the state's mesh) and normalised.  The
+ * llg handle is borrowed and must outlive the string; all images are stepped
+ * with it, sharing its step-size controller as in the reference. */
+typedef struct maf_string_s* maf_string;
+int maf_string_create(maf_string* out, maf_state state, const maf_state* inputimages, int n_inputimages, int n_interp,
+                      double dt, maf_llg llg);
+int maf_string_destroy(maf_string h);
+/* StringMethod::step (string_method.cpp:128-132): every image integrated for dt,
+ * arc lengths x (FrobeniusNorm of image differences), linear re-interpolation */
+int maf_string_step(maf_string h);
+/* StringMethod::calc_E (string_method.cpp:48-55): E[i] of every image, E_out[n_interp] */
+int maf_string_calc_E(maf_string h, double* E_out);
+/* StringMethod::run (string_method.cpp:174-314): returns the lowest barrier max(E) - E[0] in dE and writes
+ * the reference's .dat files and gnuplot script under filepath (no VTK files, gnuplot is not run);
+ * iterations (optional) receives the number of string steps taken */
+int maf_string_run(maf_string h, const char* filepath, double string_abort_rel_diff, double string_abort_abs_diff,
+                   int string_steps, int every_string_to_vti, int verbose, double* dE, int* iterations);
+int maf_string_n_images(maf_string h, int* n);
+/* current arc-length coordinates x[n_interp] and the regular grid x_interp[n_interp] */
+int maf_string_get_x(maf_string h, double* x, double* x_interp);
+/* image i as a state handle owned by the string (do not destroy it) */
+int maf_string_image(maf_string h, int i, maf_state* image);
+
 /* ------------------------------------------------- no-allocation mean ---
  * No counterpart in the reference.  <m> of a device-resident FP64 field
  * m_dev[3][ncells] (e.g. from maf_state_device_m), with the definition of

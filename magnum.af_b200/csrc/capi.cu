@@ -1,6 +1,10 @@
 // C ABI of the magnum.af B200 library (declared in include/maf_b200.h).
+#include <algorithm>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
+#include <fstream>
+#include <iomanip>
 #include <limits>
 #include <memory>
 #include <string>
@@ -1569,6 +1573,354 @@ int maf_llg_counters(maf_llg l, unsigned long long out[4]) {
         out[1] = l->ctrl.n_reject;
         out[2] = l->ctrl.n_hmin;
         out[3] = l->ctrl.n_hmax;
+    });
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// String method (magnumaf/include/magnumaf/solvers/string_method.hpp:9-39,
+//                magnumaf/src/solvers/string_method.cpp:12-314)
+//
+// The images live on the device as states of the template's mesh and Ms; one
+// LLG integrator (borrowed, as the reference's StringMethod holds one
+// LLGIntegrator) steps every image in turn, so its controller state carries
+// over from image to image exactly as in the reference.  Arc lengths are
+// device reductions of sum (m_i - m_{i-1})^2; the re-interpolation and the
+// zero-safe normalisation are device kernels.
+// ---------------------------------------------------------------------------
+struct maf_string_s {
+    maf_llg_s* llg = nullptr;
+    int n_interp = 0;
+    double dt = 0;
+    cudaStream_t stream = nullptr;
+    std::vector<std::unique_ptr<maf_state_s>> images;
+    std::vector<double> x, x_interp, E;
+    DevBuf tmp;      // [n_interp][3N] copy of the images for the re-interpolation
+    DevBuf scratch;  // reduction partials
+    ~maf_string_s() {
+        if (stream) cudaStreamSynchronize(stream);
+        images.clear();
+        tmp.release();
+        scratch.release();
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+namespace {
+
+// a state with the template's mesh, precision and Ms (or Ms_field), on stream st
+std::unique_ptr<maf_state_s> make_image(const maf_state_s& tmpl, cudaStream_t st) {
+    auto h = std::make_unique<maf_state_s>();
+    StateD& s = h->s;
+    const StateD& t = tmpl.s;
+    s.md = t.md;
+    s.precision = t.precision;
+    s.Ms = t.Ms;
+    s.has_Ms_field = t.has_Ms_field;
+    s.stream = st;
+    s.own_stream = false;
+    const int64_t N = s.md.N();
+    s.m64.alloc(sizeof(double) * 3 * N);
+    if (t.has_Ms_field) {
+        s.Msf64.alloc(sizeof(double) * N);
+        MAF_CUDA(cudaMemcpyAsync(s.Msf64.p, t.Msf64.p, sizeof(double) * N, cudaMemcpyDeviceToDevice, st));
+        if (s.precision == PREC_FP32_FIELD) {
+            s.Msf32.alloc(sizeof(float) * N);
+            MAF_CUDA(cudaMemcpyAsync(s.Msf32.p, t.Msf32.p, sizeof(float) * N, cudaMemcpyDeviceToDevice, st));
+        }
+    }
+    return h;
+}
+
+// FrobeniusNorm(a - b) = sqrt(mean((a - b)^2)) over all 3N values (util.cpp:53-55)
+double frob_diff(maf_string_s* h, const double* a, const double* b, int64_t n3) {
+    h->scratch.ensure(sizeof(double) * (2 * 148 + 2));
+    return std::sqrt(sqdiff_host(a, b, n3, h->scratch.as<double>(), h->stream) / (double)n3);
+}
+
+// StringMethod::calc_x (string_method.cpp:57-81)
+void string_calc_x(maf_string_s* h, const std::vector<const double*>& ms, int64_t n3) {
+    h->x.assign(1, 0.0);
+    for (size_t i = 1; i < ms.size(); ++i) h->x.push_back(h->x[i - 1] + frob_diff(h, ms[i], ms[i - 1], n3));
+    h->x_interp.clear();
+    for (int i = 0; i < h->n_interp; ++i)
+        h->x_interp.push_back(static_cast<double>(i) / static_cast<double>(h->n_interp - 1) * h->x.back());
+}
+
+// the bracket search of string_method.cpp:22-28 / :86-92 (x[j] is only read for
+// j < x.size(), which the reference's loop never exceeds either)
+int string_bracket(const maf_string_s* h, int i) {
+    int j = 0;
+    const int jmax = std::min<int>(h->n_interp, (int)h->x.size());
+    while (j < jmax && h->x[j] < h->x_interp[i]) ++j;
+    if (j > 0) --j;
+    return j;
+}
+
+void string_normalize(maf_string_s* h) {
+    for (auto& img : h->images) {
+        normalize_m(img->s.m64.as<double>(), img->s.md.N(), 0, nullptr, h->stream);
+        img->m32_valid = false;
+    }
+}
+
+// StringMethod::integrate (string_method.cpp:108-121)
+void string_integrate(maf_string_s* h) {
+    for (auto& img : h->images) {
+        const double t0 = img->s.t;
+        while (img->s.t < t0 + h->dt) llg_step(h->llg, img.get());
+    }
+}
+
+// StringMethod::lin_interpolate (string_method.cpp:83-106)
+void string_lin_interpolate(maf_string_s* h) {
+    const int n = h->n_interp;
+    const int64_t n3 = 3 * h->images[0]->s.md.N();
+    h->tmp.ensure(sizeof(double) * n3 * n);
+    double* tmp = h->tmp.as<double>();
+    std::vector<double> t_tmp(n);
+    std::vector<unsigned long long> steps_tmp(n);
+    for (int i = 0; i < n; ++i) {
+        MAF_CUDA(cudaMemcpyAsync(tmp + i * n3, h->images[i]->s.m64.p, sizeof(double) * n3, cudaMemcpyDeviceToDevice,
+                                 h->stream));
+        t_tmp[i] = h->images[i]->s.t;
+        steps_tmp[i] = h->images[i]->s.steps;
+    }
+    for (int i = 0; i < n; ++i) {
+        const int j = string_bracket(h, i);
+        double* out = h->images[i]->s.m64.as<double>();
+        if (j < n - 1) {
+            lerp(out, tmp + j * n3, tmp + (j + 1) * n3, h->x_interp[i] - h->x[j], h->x[j + 1] - h->x[j], n3,
+                 h->stream);
+        } else {
+            std::printf("Warning: x_interp[j=%d] exceedes x range, y_interp[j] value set to y[j]\n", j);
+            MAF_CUDA(cudaMemcpyAsync(out, tmp + j * n3, sizeof(double) * n3, cudaMemcpyDeviceToDevice, h->stream));
+            h->images[i]->s.t = t_tmp[j];
+            h->images[i]->s.steps = steps_tmp[j];
+        }
+    }
+    string_normalize(h);
+}
+
+std::vector<const double*> image_ms(const maf_string_s* h) {
+    std::vector<const double*> v;
+    for (auto& img : h->images) v.push_back(img->s.m64.as<double>());
+    return v;
+}
+
+// StringMethod::step (string_method.cpp:128-132)
+void string_step(maf_string_s* h) {
+    string_integrate(h);
+    string_calc_x(h, image_ms(h), 3 * h->images[0]->s.md.N());
+    string_lin_interpolate(h);
+}
+
+// StringMethod::calc_E (string_method.cpp:48-55)
+void string_calc_E(maf_string_s* h) {
+    h->E.clear();
+    for (auto& img : h->images) h->E.push_back(llg_energy(h->llg, img.get()));
+}
+
+}  // namespace
+
+namespace {
+
+// gnuplot script of string_method.cpp:145-172 (written, not executed)
+void string_write_plotfile(const std::string& filepath) {
+    std::ofstream f(filepath + "plot_string_method.gpi");
+    f << "set terminal pdf\nset key left top Left\n\n"
+      << "set title 'Energy over image ID for each iteration'\nset xlabel 'Image ID'\nset ylabel 'E [J]'\n"
+      << "set cblabel 'Iteration'\nset format y '%.1e'\nset output 'E_curves.pdf'\n"
+      << "p 'E_curves.dat' u 2:3:1 w l palette t 'E'\n\n"
+      << "set title 'Energy barrier over iteration'\nset xlabel 'Iteration'\nset ylabel 'dE [J]'\n"
+      << "set output 'dE_over_iteration.pdf'\np 'dE_over_iteration.dat' u 1:2 w l notitle\n\n"
+      << "set title 'Energy over image ID'\nset xlabel 'Image ID'\nset ylabel 'E [J]'\nset output 'E.pdf'\n"
+      << "p 'E_last_step.dat' u 1:3 w l t 'Last iteration', 'E_max_lowest.dat' u 1:3 w l t 'Lowest barrier'\n";
+}
+
+// StringMethod::run (string_method.cpp:174-314): the iteration, the abort
+// criteria and the .dat files; the reference's VTK image files and its
+// gnuplot call are not produced.  Where the reference indexes E[-1] it means
+// the last image; E.back() is written.
+double string_run(maf_string_s* h, const std::string& filepath, double rel_abort, double abs_abort, int steps,
+                  bool verbose, int* iterations) {
+    string_write_plotfile(filepath);
+    std::ofstream f_steps(filepath + "dE_over_iteration.dat");
+    f_steps << "# i \t dE [J] \t dE rel_diff to step i-1 \t dE abs_diff to step i-1\n";
+    f_steps.precision(12);
+    std::ofstream f_curves(filepath + "E_curves.dat");
+    f_curves << "# step \t image \t dE=E[j]-E[0] \t E[j]-E[-1] \t E[j]\n";
+    f_curves.precision(12);
+    double max_lowest = 1e100, max_prev = 1e100;
+    int i_max_lowest = -1;
+    std::vector<double> E_max_lowest;
+    int it = 0;
+    for (int i = 0; i < steps; ++i) {
+        it = i + 1;
+        string_step(h);
+        string_calc_E(h);
+        const double emax = *std::max_element(h->E.begin(), h->E.end());
+        const double barrier = emax - h->E[0];
+        if (barrier < max_lowest) {
+            max_lowest = barrier;
+            i_max_lowest = i;
+            E_max_lowest = h->E;
+        }
+        const double abs_diff = std::fabs(barrier - max_prev);
+        const double rel_diff = std::fabs((2. * abs_diff) / (barrier + max_prev));
+        if (i > 25 && rel_diff < rel_abort) {
+            if (verbose)
+                std::printf("StringMethod run: relative difference of two consecutive E_barriers is: rel_diff=%e. "
+                            "This is smaller than %e\n", rel_diff, rel_abort);
+            f_steps << "#StringMethod run: relative difference of two consecutive E_barriers is: rel_diff= "
+                    << rel_diff << " This is smaller than " << rel_abort << "\n";
+            break;
+        }
+        if (i > 25 && abs_diff < abs_abort) {
+            if (verbose)
+                std::printf("StringMethod run: absolute difference of two consecutive E_barriers is: abs_diff=%e "
+                            "is smaller than %e\n", abs_diff, abs_abort);
+            f_steps << "#StringMethod run: absolute difference of two consecutive E_barriers is: abs_diff= "
+                    << abs_diff << " is smaller than " << abs_abort << "\n";
+            break;
+        }
+        {
+            std::ofstream fb(filepath + "E_barrier.dat");
+            fb.precision(12);
+            fb << "# max_lowest \t this->images[0].mesh.nx \t this->images[0].mesh.dx\n"
+               << max_lowest << "\t" << h->images[0]->s.md.nx << "\t" << h->images[0]->s.md.dx << "\n";
+        }
+        for (size_t j = 0; j < h->E.size(); ++j)
+            f_curves << i << " " << j << " " << h->E[j] - h->E[0] << " " << h->E[j] - h->E.back() << " " << h->E[j]
+                     << "\n";
+        f_curves << i << "\n\n\n";
+        max_prev = barrier;
+        if (verbose)
+            std::printf("step=%d, dE[J]=%e, rel_diff[J]= %e, abs_diff[J]=%e\n", i, barrier, rel_diff, abs_diff);
+        f_steps << i << "\t" << std::setw(18) << barrier << "\t" << rel_diff << "\t" << abs_diff << "\n";
+    }
+    if (verbose) std::printf("i=%d, minimal dE=%e\n", i_max_lowest, max_lowest);
+    if (!E_max_lowest.empty())
+        f_steps << "#i , lowest overall:   max-[0], max-[-1] max [J]: " << i_max_lowest << "\t" << max_lowest << "\t"
+                << max_lowest + E_max_lowest[0] - E_max_lowest.back() << "\t" << max_lowest + E_max_lowest[0]
+                << "\n";
+    std::ofstream fE(filepath + "E_last_step.dat");
+    fE << " i \t << E[i] \t << dE = E[i] - E[0] \t << E[i] - E[-1] \n";
+    fE.precision(12);
+    std::ofstream fL(filepath + "E_max_lowest.dat");
+    fL << " i \t << E_max_lowest[i] \t << E_max_lowest[i] - E_max_lowest[0] \t << E_max_lowest[i] - E_max_lowest[-1]\n";
+    fL.precision(12);
+    for (size_t i = 0; i < h->E.size(); ++i) {
+        fE << i << "\t" << h->E[i] << "\t" << h->E[i] - h->E[0] << "\t" << h->E[i] - h->E.back() << "\n";
+        if (i < E_max_lowest.size())
+            fL << i << "\t" << E_max_lowest[i] << "\t" << E_max_lowest[i] - E_max_lowest[0] << "\t"
+               << E_max_lowest[i] - E_max_lowest.back() << "\n";
+    }
+    if (iterations) *iterations = it;
+    return max_lowest;
+}
+
+}  // namespace
+
+extern "C" {
+
+int maf_string_create(maf_string* out, maf_state state, const maf_state* inputimages, int n_inputimages, int n_interp,
+                      double dt, maf_llg llg) {
+    return guarded([&] {
+        check(out && state && inputimages && llg, "maf_string_create: NULL argument");
+        check(n_inputimages >= 2,
+              "StringMethod: invalid inputimages provided, please add at least two states/magnetizations for "
+              "interpolation of initial path.");
+        check(n_interp >= 2, "StringMethod: n_interp must be at least 2");
+        check(!llg->terms.empty(), "LLGIntegrator: no field terms");
+        const MeshDims md = state->s.md;
+        for (int i = 0; i < n_inputimages; ++i) {
+            check(inputimages[i] != nullptr, "maf_string_create: NULL input image");
+            check(inputimages[i]->s.md == md, "StringMethod: input image mesh differs from the state's mesh");
+        }
+        auto h = std::make_unique<maf_string_s>();
+        h->llg = llg;
+        h->n_interp = n_interp;
+        h->dt = dt;
+        MAF_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+        MAF_CUDA(cudaStreamSynchronize(state->s.stream));
+        std::vector<const double*> in_m;
+        for (int i = 0; i < n_inputimages; ++i) {
+            MAF_CUDA(cudaStreamSynchronize(inputimages[i]->s.stream));
+            in_m.push_back(inputimages[i]->s.m64.as<double>());
+        }
+        const int64_t n3 = 3 * md.N();
+        string_calc_x(h.get(), in_m, n3);
+        for (int i = 0; i < n_interp; ++i) {
+            auto img = make_image(*state, h->stream);
+            const int j = string_bracket(h.get(), i);
+            if (j < n_interp - 1) {
+                lerp(img->s.m64.as<double>(), in_m[j], in_m[j + 1], h->x_interp[i] - h->x[j], h->x[j + 1] - h->x[j],
+                     n3, h->stream);
+            } else {
+                std::printf("Warning: x_interp[j=%d] exceedes x range, y_interp[j] value set to y[j]\n", j);
+                MAF_CUDA(cudaMemcpyAsync(img->s.m64.p, in_m[j], sizeof(double) * n3, cudaMemcpyDeviceToDevice,
+                                         h->stream));
+                img->s.t = inputimages[j]->s.t;
+                img->s.steps = inputimages[j]->s.steps;
+            }
+            h->images.push_back(std::move(img));
+        }
+        for (auto& img : h->images) check_llg_state(llg, img.get());
+        string_normalize(h.get());
+        MAF_CUDA(cudaStreamSynchronize(h->stream));
+        *out = h.release();
+    });
+}
+
+int maf_string_destroy(maf_string h) {
+    return guarded([&] { delete h; });
+}
+
+int maf_string_step(maf_string h) {
+    return guarded([&] {
+        check(h, "NULL argument");
+        string_step(h);
+        MAF_CUDA(cudaStreamSynchronize(h->stream));
+    });
+}
+
+int maf_string_calc_E(maf_string h, double* E_out) {
+    return guarded([&] {
+        check(h, "NULL argument");
+        string_calc_E(h);
+        if (E_out) std::copy(h->E.begin(), h->E.end(), E_out);
+    });
+}
+
+int maf_string_run(maf_string h, const char* filepath, double string_abort_rel_diff, double string_abort_abs_diff,
+                   int string_steps, int every_string_to_vti, int verbose, double* dE, int* iterations) {
+    (void)every_string_to_vti;
+    return guarded([&] {
+        check(h && filepath && dE, "NULL argument");
+        *dE = string_run(h, filepath, string_abort_rel_diff, string_abort_abs_diff, string_steps, verbose != 0,
+                         iterations);
+    });
+}
+
+int maf_string_n_images(maf_string h, int* n) {
+    return guarded([&] { check(h && n, "NULL argument"); *n = h->n_interp; });
+}
+
+int maf_string_get_x(maf_string h, double* x, double* x_interp) {
+    return guarded([&] {
+        check(h, "NULL argument");
+        if (x) std::copy(h->x.begin(), h->x.end(), x);
+        if (x_interp) std::copy(h->x_interp.begin(), h->x_interp.end(), x_interp);
+    });
+}
+
+int maf_string_image(maf_string h, int i, maf_state* image) {
+    return guarded([&] {
+        check(h && image, "NULL argument");
+        check(i >= 0 && i < h->n_interp, "maf_string_image: image index out of range");
+        *image = h->images[i].get();
     });
 }
 

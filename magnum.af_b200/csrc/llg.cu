@@ -226,18 +226,25 @@ void f32_to_f64(const float* a, double* b, int64_t n, cudaStream_t st) {
 // ---------------------------------------------------------------------------
 constexpr int kRedBlocks = 148 * 2;
 
-// per-block partials: mode 0 sum a*b, mode 1 max |a| (NaN-propagating)
+// per-block partials: mode 0 sum a*b, mode 1 max |a| (NaN-propagating),
+// mode 2 sum (a-b)^2 (the string method's Frobenius norm of image differences)
 __global__ void k_red_partials(const double* __restrict__ a, const double* __restrict__ b, int64_t n, int mode,
                                double* __restrict__ part) {
     double v = 0.0;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        if (mode == 0) v += a[i] * b[i];
-        else v = nanmax(v, fabs(a[i]));
+        if (mode == 0) {
+            v += a[i] * b[i];
+        } else if (mode == 2) {
+            const double d = a[i] - b[i];
+            v += d * d;
+        } else {
+            v = nanmax(v, fabs(a[i]));
+        }
     }
     __shared__ double red[32];
     for (int o = 16; o > 0; o >>= 1) {
         const double w = __shfl_down_sync(0xffffffffu, v, o);
-        v = mode == 0 ? v + w : nanmax(v, w);
+        v = mode != 1 ? v + w : nanmax(v, w);
     }
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     if (lane == 0) red[wid] = v;
@@ -247,7 +254,7 @@ __global__ void k_red_partials(const double* __restrict__ a, const double* __res
         double s = lane < nw ? red[lane] : 0.0;
         for (int o = 16; o > 0; o >>= 1) {
             const double w = __shfl_down_sync(0xffffffffu, s, o);
-            s = mode == 0 ? s + w : nanmax(s, w);
+            s = mode != 1 ? s + w : nanmax(s, w);
         }
         if (lane == 0) part[blockIdx.x] = s;
     }
@@ -256,7 +263,7 @@ __global__ void k_red_partials(const double* __restrict__ a, const double* __res
 __global__ void k_red_final(const double* __restrict__ part, int nb, int mode, double* __restrict__ out) {
     if (threadIdx.x == 0 && blockIdx.x == 0) {
         double s = 0.0;
-        for (int i = 0; i < nb; ++i) s = mode == 0 ? s + part[i] : nanmax(s, part[i]);
+        for (int i = 0; i < nb; ++i) s = mode != 1 ? s + part[i] : nanmax(s, part[i]);
         *out = s;
     }
 }
@@ -279,6 +286,24 @@ double dot_host(const double* a, const double* b, int64_t n, double* scratch, cu
 
 double maxabs_host(const double* a, int64_t n, double* scratch, cudaStream_t st) {
     return reduce_host(a, nullptr, n, 1, scratch, st);
+}
+
+double sqdiff_host(const double* a, const double* b, int64_t n, double* scratch, cudaStream_t st) {
+    return reduce_host(a, b, n, 2, scratch, st);
+}
+
+// out = a + (c1 * (b - a)) / c2, the string method's linear re-interpolation
+// in the reference's order of operations (string_method.cpp:94-95)
+__global__ void k_lerp(double* __restrict__ out, const double* __restrict__ a, const double* __restrict__ b, double c1,
+                       double c2, int64_t n) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = a[i] + (c1 * (b[i] - a[i])) / c2;
+}
+
+void lerp(double* out, const double* a, const double* b, double c1, double c2, int64_t n, cudaStream_t st) {
+    const int64_t blocks = std::min<int64_t>(ceil_div(n, 256), 148LL * 16);
+    k_lerp<<<(unsigned)blocks, 256, 0, st>>>(out, a, b, c1, c2, n);
+    MAF_LAUNCH_CHECK();
 }
 
 __global__ void k_axpby(double* out, double a, const double* x, double b, const double* y, int64_t n) {

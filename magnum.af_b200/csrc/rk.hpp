@@ -25,5 +25,8 @@ double dot_host(const double* a, const double* b, int64_t n, double* scratch, cu
 double maxabs_host(const double* a, int64_t n, double* scratch, cudaStream_t st);
 void axpby(double* out, double a, const double* x, double b, const double* y, int64_t n, cudaStream_t st);
 void normalize_combine(double* m, const double* wa, double stp, const double* s, int64_t N, cudaStream_t st);
+// string method: sum (a-b)^2 over n values (synchronises), out = a + (c1 (b - a)) / c2
+double sqdiff_host(const double* a, const double* b, int64_t n, double* scratch, cudaStream_t st);
+void lerp(double* out, const double* a, const double* b, double c1, double c2, int64_t n, cudaStream_t st);
 
 }  // namespace mafb

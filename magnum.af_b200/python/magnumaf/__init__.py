@@ -105,6 +105,14 @@ _SIGS = {
     "maf_llg_get_h": (_I, [_P, _DP]),
     "maf_llg_counters": (_I, [_P, C.POINTER(C.c_ulonglong)]),
     "maf_mean_m_noalloc": (_I, [_P, C.c_longlong, _DP, _P]),
+    "maf_string_create": (_I, [C.POINTER(_P), _P, C.POINTER(_P), _I, _I, _D, _P]),
+    "maf_string_destroy": (_I, [_P]),
+    "maf_string_step": (_I, [_P]),
+    "maf_string_calc_E": (_I, [_P, _DP]),
+    "maf_string_run": (_I, [_P, C.c_char_p, _D, _D, _I, _I, _I, _DP, C.POINTER(_I)]),
+    "maf_string_n_images": (_I, [_P, C.POINTER(_I)]),
+    "maf_string_get_x": (_I, [_P, _DP, _DP]),
+    "maf_string_image": (_I, [_P, _I, C.POINTER(_P)]),
 }
 for _name, (_res, _args) in _SIGS.items():
     _f = getattr(lib, _name)
@@ -196,9 +204,25 @@ class State:
                                      float("nan"), _dptr(msf), _dptr(mf), prec))
 
     def __del__(self):
-        if getattr(self, "_h", None):
+        if getattr(self, "_h", None) and getattr(self, "_owned", True):
             lib.maf_state_destroy(self._h)
-            self._h = None
+        self._h = None
+
+    @classmethod
+    def _borrowed(cls, handle, mesh, owner):
+        """A view of a state handle that another object owns (e.g. a string image)."""
+        obj = cls.__new__(cls)
+        obj.mesh = mesh
+        obj._h = handle
+        obj._owned = False
+        obj._owner = owner  # keeps the owner alive while the view exists
+        return obj
+
+    @property
+    def precision(self) -> str:
+        v = C.c_int()
+        _ck(lib.maf_state_precision(self._h, C.byref(v)))
+        return "fp32_field" if v.value == MAF_FP32_FIELD else "fp64"
 
     def __str__(self):
         mx, my, mz = self.mean_m()
@@ -571,6 +595,69 @@ class LBFGS_Minimizer:
         g = C.c_double()
         _ck(lib.maf_lbfgs_stats(self._h, C.byref(it), C.byref(fe), C.byref(g)))
         return {"iterations": it.value, "fevals": fe.value, "grad_max": g.value}
+
+
+class StringMethod:
+    """StringMethod(state, inputimages, n_interp, dt, llg) (python/magnumaf.pyx:1034-1068).
+
+    ``inputimages`` are States or m arrays (nx, ny, nz, 3); arrays become states
+    with the template state's Ms (or Ms_field).  ``run`` returns the lowest
+    energy barrier max(E) - E[0] in J and writes the reference's .dat files
+    under ``filepath``.  The images stay on the device; ``images`` gives views."""
+
+    def __init__(self, state: State, inputimages, n_interp, dt, llg: LLGIntegrator):
+        if not inputimages or len(inputimages) == 1:
+            raise RuntimeError("StringMethod: invalid inputimages provided, please add at least two "
+                               "states/magnetizations for interpolation of initial path.")
+        self._h = _P()
+        self._llg = llg
+        self.mesh = state.mesh
+        ms_field = state.Ms_field
+        ms = ms_field if ms_field is not None else state.Ms
+        self._inputs = [a if isinstance(a, State) else State(state.mesh, ms, a, precision=state.precision)
+                        for a in inputimages]
+        arr = (_P * len(self._inputs))(*[a._h for a in self._inputs])
+        _ck(lib.maf_string_create(C.byref(self._h), state._h, arr, len(self._inputs), int(n_interp), float(dt),
+                                  llg._h))
+        self.n_interp = int(n_interp)
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib.maf_string_destroy(self._h)
+            self._h = None
+
+    def run(self, filepath, string_abort_rel_diff=1e-12, string_abort_abs_diff=1e-27, string_steps=10000,
+            every_string_to_vti=50, verbose=True):
+        dE = C.c_double()
+        it = C.c_int()
+        _ck(lib.maf_string_run(self._h, str(filepath).encode(), float(string_abort_rel_diff),
+                               float(string_abort_abs_diff), int(string_steps), int(every_string_to_vti),
+                               int(bool(verbose)), C.byref(dE), C.byref(it)))
+        self.iterations = it.value
+        return dE.value
+
+    def step(self):
+        _ck(lib.maf_string_step(self._h))
+
+    def calc_E(self) -> np.ndarray:
+        out = np.empty(self.n_interp)
+        _ck(lib.maf_string_calc_E(self._h, _dptr(out)))
+        return out
+
+    def x(self):
+        x = np.empty(self.n_interp)
+        xi = np.empty(self.n_interp)
+        _ck(lib.maf_string_get_x(self._h, _dptr(x), _dptr(xi)))
+        return x, xi
+
+    @property
+    def images(self):
+        out = []
+        for i in range(self.n_interp):
+            h = _P()
+            _ck(lib.maf_string_image(self._h, i, C.byref(h)))
+            out.append(State._borrowed(h, self.mesh, self))
+        return out
 
 
 class Stochastic_LLG:
