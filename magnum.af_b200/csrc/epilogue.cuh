@@ -175,74 +175,101 @@ __device__ __forceinline__ void run4_load(const R* __restrict__ m, const Geom& g
     }
 }
 
-// H of cell i of the run (hd = demag contribution)
+// H of the four cells of the run (hd = demag contribution).  Terms outer,
+// cells inner; the per-term constants come from TermDesc::q, prepared once per
+// launch on the host (prepare_run4), so no division is left in the cell loop:
+//   exchange  q = 2A/(mu0 Ms) / (dx^2, dy^2, dz^2)
+//   DMI       q = 2D/(mu0 Ms), 1/(2dx), 1/(2dy), 1/(2dz)
+//   uniaxial  q = 2Ku/(mu0 Ms)
+//   cubic     q = -2Kc1/(mu0 Ms), -2Kc2/(mu0 Ms), -4Kc3/(mu0 Ms)
 template <typename R>
-__device__ __forceinline__ void run4_field(const TermList& tl, const Geom& g, const Run4<R>& r, int i, R Ms,
-                                           const R hd[3], R h[3]) {
-    h[0] = 0;
-    h[1] = 0;
-    h[2] = 0;
-    const bool xm = i > 0 || r.hxl, xp = i < 3 || r.hxr;
+__device__ __forceinline__ void run4_fields(const TermList& tl, const Run4<R>& r, const R hd[4][3], R h[4][3]) {
+#pragma unroll
+    for (int i = 0; i < 4; ++i) h[i][0] = h[i][1] = h[i][2] = 0;
     for (int it = 0; it < tl.n; ++it) {
         const TermDesc& t = tl.t[it];
         switch (t.kind) {
             case TK_DEMAG:
-                h[0] += hd[0]; h[1] += hd[1]; h[2] += hd[2];
+#pragma unroll
+                for (int i = 0; i < 4; ++i) { h[i][0] += hd[i][0]; h[i][1] += hd[i][1]; h[i][2] += hd[i][2]; }
                 break;
             case TK_EXCHANGE: {
-                const R idx2 = (R)(1.0 / (g.dx * g.dx)), idy2 = (R)(1.0 / (g.dy * g.dy)), idz2 = (R)(1.0 / (g.dz * g.dz));
-                const R coef = (R)(2.0 * t.p[0]) / ((R)kMu0 * Ms);
+                const R qx = (R)t.q[0], qy = (R)t.q[1], qz = (R)t.q[2];
 #pragma unroll
                 for (int c = 0; c < 3; ++c) {
-                    const R v = r.c[c][i];
-                    const R left = i > 0 ? r.c[c][i - 1] : r.xl[c];
-                    const R right = i < 3 ? r.c[c][i + 1] : r.xr[c];
-                    const R ax = (xm ? left - v : -v) + (xp ? right - v : -v);
-                    const R ay = (r.hym ? r.ym[c][i] - v : -v) + (r.hyp ? r.yp[c][i] - v : -v);
-                    const R az = (r.hzm ? r.zm[c][i] - v : -v) + (r.hzp ? r.zp[c][i] - v : -v);
-                    h[c] += coef * (ax * idx2 + ay * idy2 + az * idz2);
+#pragma unroll
+                    for (int i = 0; i < 4; ++i) {
+                        const R v = r.c[c][i];
+                        const R left = i > 0 ? r.c[c][i - 1] - v : (r.hxl ? r.xl[c] - v : -v);
+                        const R right = i < 3 ? r.c[c][i + 1] - v : (r.hxr ? r.xr[c] - v : -v);
+                        const R ay = (r.hym ? r.ym[c][i] - v : -v) + (r.hyp ? r.yp[c][i] - v : -v);
+                        const R az = (r.hzm ? r.zm[c][i] - v : -v) + (r.hzp ? r.zp[c][i] - v : -v);
+                        h[i][c] += (left + right) * qx + ay * qy + az * qz;
+                    }
                 }
                 break;
             }
             case TK_DMI: {
+                const R coef = (R)t.q[0], hx = (R)t.q[1], hy = (R)t.q[2], hz = (R)t.q[3];
                 const R n0 = (R)t.p[1], n1 = (R)t.p[2], n2 = (R)t.p[3];
-                const R hx = (R)(0.5 / g.dx), hy = (R)(0.5 / g.dy), hz = (R)(0.5 / g.dz);
-                R lm[3], rm[3];
-#pragma unroll
-                for (int c = 0; c < 3; ++c) {
-                    lm[c] = i > 0 ? r.c[c][i - 1] : r.xl[c];
-                    rm[c] = i < 3 ? r.c[c][i + 1] : r.xr[c];
-                }
-                const R div = (rm[0] - lm[0]) * hx + (r.yp[1][i] - r.ym[1][i]) * hy + (r.zp[2][i] - r.zm[2][i]) * hz;
                 auto nm = [&](const R v0, const R v1, const R v2) { return n0 * v0 + n1 * v1 + n2 * v2; };
-                const R g0 = (nm(rm[0], rm[1], rm[2]) - nm(lm[0], lm[1], lm[2])) * hx;
-                const R g1 = (nm(r.yp[0][i], r.yp[1][i], r.yp[2][i]) - nm(r.ym[0][i], r.ym[1][i], r.ym[2][i])) * hy;
-                const R g2 = (nm(r.zp[0][i], r.zp[1][i], r.zp[2][i]) - nm(r.zm[0][i], r.zm[1][i], r.zm[2][i])) * hz;
-                const R coef = (R)2 * (R)t.p[0] / ((R)kMu0 * Ms);
-                h[0] += coef * (n0 * div - g0);
-                h[1] += coef * (n1 * div - g1);
-                h[2] += coef * (n2 * div - g2);
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    R lm[3], rm[3];
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) {
+                        lm[c] = i > 0 ? r.c[c][i - 1] : r.xl[c];
+                        rm[c] = i < 3 ? r.c[c][i + 1] : r.xr[c];
+                    }
+                    const R div = (rm[0] - lm[0]) * hx + (r.yp[1][i] - r.ym[1][i]) * hy + (r.zp[2][i] - r.zm[2][i]) * hz;
+                    const R g0 = (nm(rm[0], rm[1], rm[2]) - nm(lm[0], lm[1], lm[2])) * hx;
+                    const R g1 = (nm(r.yp[0][i], r.yp[1][i], r.yp[2][i]) - nm(r.ym[0][i], r.ym[1][i], r.ym[2][i])) * hy;
+                    const R g2 = (nm(r.zp[0][i], r.zp[1][i], r.zp[2][i]) - nm(r.zm[0][i], r.zm[1][i], r.zm[2][i])) * hz;
+                    h[i][0] += coef * (n0 * div - g0);
+                    h[i][1] += coef * (n1 * div - g1);
+                    h[i][2] += coef * (n2 * div - g2);
+                }
                 break;
             }
             case TK_UNIAXIAL: {
                 const R e0 = (R)t.p[1], e1 = (R)t.p[2], e2 = (R)t.p[3];
-                const R em = e0 * r.c[0][i] + e1 * r.c[1][i] + e2 * r.c[2][i];
-                const R coef = (R)2 * (R)t.p[0] / ((R)kMu0 * Ms);
-                h[0] += coef * (e0 * em);
-                h[1] += coef * (e1 * em);
-                h[2] += coef * (e2 * em);
+                const R coef = (R)t.q[0];
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    const R em = coef * (e0 * r.c[0][i] + e1 * r.c[1][i] + e2 * r.c[2][i]);
+                    h[i][0] += e0 * em;
+                    h[i][1] += e1 * em;
+                    h[i][2] += e2 * em;
+                }
                 break;
             }
             case TK_CUBIC: {
-                const R mc[3] = {r.c[0][i], r.c[1][i], r.c[2][i]};
-                R hc[3];
-                cubic_h123_sum(t, mc, Ms, hc);
-                h[0] += hc[0]; h[1] += hc[1]; h[2] += hc[2];
+                const R c1[3] = {(R)t.p[3], (R)t.p[4], (R)t.p[5]};
+                const R c2[3] = {(R)t.p[6], (R)t.p[7], (R)t.p[8]};
+                const R c3[3] = {(R)t.p[9], (R)t.p[10], (R)t.p[11]};
+                const R k1 = (R)t.q[0], k2 = (R)t.q[1], k3 = (R)t.q[2];
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    const R m0 = r.c[0][i], m1 = r.c[1][i], m2 = r.c[2][i];
+                    const R c1m = c1[0] * m0 + c1[1] * m1 + c1[2] * m2;
+                    const R c2m = c2[0] * m0 + c2[1] * m1 + c2[2] * m2;
+                    const R c3m = c3[0] * m0 + c3[1] * m1 + c3[2] * m2;
+                    const R s1 = c1m * c1m, s2 = c2m * c2m, s3 = c3m * c3m;
+                    // h1 + h2 + h3 of cubic_h123 with the prefactors folded in
+                    const R w1 = k1 * (s2 + s3) * c1m + k2 * (s2 * s3) * c1m + k3 * (s2 * s2 + s3 * s3) * (s1 * c1m);
+                    const R w2 = k1 * (s1 + s3) * c2m + k2 * (s1 * s3) * c2m + k3 * (s1 * s1 + s3 * s3) * (s2 * c2m);
+                    const R w3 = k1 * (s1 + s2) * c3m + k2 * (s1 * s2) * c3m + k3 * (s1 * s1 + s2 * s2) * (s3 * c3m);
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) h[i][c] += w1 * c1[c] + w2 * c2[c] + w3 * c3[c];
+                }
                 break;
             }
-            case TK_ZEEMAN:
-                h[0] += (R)t.p[0]; h[1] += (R)t.p[1]; h[2] += (R)t.p[2];
+            case TK_ZEEMAN: {
+                const R z0 = (R)t.p[0], z1 = (R)t.p[1], z2 = (R)t.p[2];
+#pragma unroll
+                for (int i = 0; i < 4; ++i) { h[i][0] += z0; h[i][1] += z1; h[i][2] += z2; }
                 break;
+            }
             default: break;
         }
     }
@@ -253,8 +280,7 @@ template <typename R, int EPI>
 __device__ __forceinline__ void run4_epilogue(const TermList& tl, const Geom& g, const Run4<R>& r, int64_t cell0,
                                               R Ms, const R hd[4][3], const EpilogueArgs& ep) {
     R h[4][3];
-#pragma unroll
-    for (int i = 0; i < 4; ++i) run4_field(tl, g, r, i, Ms, hd[i], h[i]);
+    run4_fields(tl, r, hd, h);
     if constexpr (EPI == EPI_H) {
         R* o = static_cast<R*>(ep.out);
 #pragma unroll

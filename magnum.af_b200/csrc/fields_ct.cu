@@ -166,6 +166,95 @@ __global__ void __launch_bounds__(NT, (kMinBlocks<R, NT, 768, 512>)) k_convz_ct(
     ct_fft_out<R, 1, true, L, NC, NT>(s, 0, tw, st, typename CtPlan<L>::T());
 }
 
+// ------------------------------ z convolution, transforms in registers (nz <= 16)
+// Same tile as k_convz_ct, one thread per column (row, comp, b).  The zero-padded
+// length-L (= 2 nz) transform is two length-nz DFTs held in registers:
+//   X[2k] = DFT(x)[k],  X[2k+1] = DFT(x_n W_L^n)[k]            (forward)
+//   y[n]  = IDFT(Y_even)[n] + W_L^-n IDFT(Y_odd)[n],  n < nz   (inverse, truncated)
+// so only the padded half's zeros are skipped for free, no shared-memory stage
+// is needed inside the transforms, and shared memory carries only the spectra
+// between the transforms and the 3-component tensor product.
+template <typename R, int NZ, int NB>
+__global__ void __launch_bounds__(6 * NB, (kMinBlocks<R, 6 * NB, 576, 288>))
+    k_convz_reg(cplx_t<R>* S, const R* __restrict__ Nred, int ny, int nxh, int pitch,
+                const cplx_t<R>* __restrict__ tw) {
+    using C = cplx_t<R>;
+    constexpr int L = 2 * NZ;
+    constexpr int NC = 6 * NB;  // columns (row, comp, b) = threads
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C* s = reinterpret_cast<C*>(smem_raw);  // [L][NC]
+    const int Py = 2 * ny;
+    const int ky = blockIdx.y;
+    const bool two = ky != 0 && ky != ny;
+    const int c0 = blockIdx.x * NB;
+    const int ncv = min(NB, nxh - c0);
+    const int64_t si = (int64_t)Py * pitch;       // z stride
+    const int64_t cs = (int64_t)NZ * Py * pitch;  // component stride
+    const int col = threadIdx.x;
+    {
+        const int row = col / (3 * NB);
+        const int comp = (col / NB) % 3;
+        const int b = col % NB;
+        const bool ok = b < ncv && (row == 0 || two);
+        const C* src = S + comp * cs + (int64_t)(row ? Py - ky : ky) * pitch + c0 + b;
+        C e[NZ], o[NZ];
+#pragma unroll
+        for (int n = 0; n < NZ; ++n) e[n] = ok ? src[n * si] : mk((R)0, (R)0);
+#pragma unroll
+        for (int n = 0; n < NZ; ++n) o[n] = cmul(e[n], tw[n]);
+        bfly_ct<NZ, -1, R>(e);
+        bfly_ct<NZ, -1, R>(o);
+#pragma unroll
+        for (int k = 0; k < NZ; ++k) {
+            s[(2 * k) * NC + col] = e[k];
+            s[(2 * k + 1) * NC + col] = o[k];
+        }
+    }
+    __syncthreads();
+    const int64_t tcs = (int64_t)(NZ + 1) * (ny + 1) * nxh;
+    for (int idx = threadIdx.x; idx < L * NB; idx += NC) {
+        const int kz = idx / NB;
+        const int b = idx % NB;
+        if (b >= ncv) continue;
+        const int kzr = kz <= NZ ? kz : L - kz;
+        const R sz = kz <= NZ ? (R)1 : (R)-1;
+        const int64_t o = ((int64_t)kzr * (ny + 1) + ky) * nxh + c0 + b;
+        const R Nxx = Nred[o], Nxy = Nred[tcs + o], Nxz = sz * Nred[2 * tcs + o];
+        const R Nyy = Nred[3 * tcs + o], Nyz = sz * Nred[4 * tcs + o], Nzz = Nred[5 * tcs + o];
+#pragma unroll
+        for (int row = 0; row < 2; ++row) {
+            if (row == 1 && !two) break;
+            const R sy = row ? (R)-1 : (R)1;
+            const int base = kz * NC + row * 3 * NB + b;
+            const C mx = s[base], my = s[base + NB], mz = s[base + 2 * NB];
+            const R xy = sy * Nxy, yz = sy * Nyz;
+            s[base] = cadd(cadd(cscale(mx, Nxx), cscale(my, xy)), cscale(mz, Nxz));
+            s[base + NB] = cadd(cadd(cscale(mx, xy), cscale(my, Nyy)), cscale(mz, yz));
+            s[base + 2 * NB] = cadd(cadd(cscale(mx, Nxz), cscale(my, yz)), cscale(mz, Nzz));
+        }
+    }
+    __syncthreads();
+    {
+        const int row = col / (3 * NB);
+        const int comp = (col / NB) % 3;
+        const int b = col % NB;
+        const bool ok = b < ncv && (row == 0 || two);
+        C e[NZ], o[NZ];
+#pragma unroll
+        for (int k = 0; k < NZ; ++k) {
+            e[k] = s[(2 * k) * NC + col];
+            o[k] = s[(2 * k + 1) * NC + col];
+        }
+        bfly_ct<NZ, 1, R>(e);
+        bfly_ct<NZ, 1, R>(o);
+        if (ok) {
+            C* dst = S + comp * cs + (int64_t)(row ? Py - ky : ky) * pitch + c0 + b;
+#pragma unroll
+            for (int n = 0; n < NZ; ++n) dst[n * si] = cadd(e[n], cmulc(o[n], tw[n]));
+        }
+    }
+}
+
 // -------------------------------------------------- y convolution (nz == 1)
 template <typename R, int L, int NB, int NT>
 __global__ void __launch_bounds__(NT) k_convy_ct(cplx_t<R>* S, const R* __restrict__ Nred, int ny, int nxh, int pitch,
@@ -317,6 +406,37 @@ static bool run4_eligible(const Geom& g, const R* m, const MsInfo& ms, const Ter
     return true;
 }
 
+// Per-launch constants of the 4-cell epilogue (TermDesc::q); the scalar Ms is
+// known because run4 excludes an Ms_field.
+static void prepare_run4(TermList& tl, const Geom& g, double Ms) {
+    const double mu0Ms = kMu0 * Ms;
+    for (int i = 0; i < tl.n; ++i) {
+        TermDesc& t = tl.t[i];
+        switch (t.kind) {
+            case TK_EXCHANGE: {
+                const double c = 2.0 * t.p[0] / mu0Ms;
+                t.q[0] = c / (g.dx * g.dx);
+                t.q[1] = c / (g.dy * g.dy);
+                t.q[2] = c / (g.dz * g.dz);
+                break;
+            }
+            case TK_DMI:
+                t.q[0] = 2.0 * t.p[0] / mu0Ms;
+                t.q[1] = 0.5 / g.dx;
+                t.q[2] = 0.5 / g.dy;
+                t.q[3] = 0.5 / g.dz;
+                break;
+            case TK_UNIAXIAL: t.q[0] = 2.0 * t.p[0] / mu0Ms; break;
+            case TK_CUBIC:
+                t.q[0] = -2.0 * t.p[0] / mu0Ms;
+                t.q[1] = -2.0 * t.p[1] / mu0Ms;
+                t.q[2] = -4.0 * t.p[2] / mu0Ms;
+                break;
+            default: break;
+        }
+    }
+}
+
 // ------------------------------------------------------------------ launches
 template <typename K> static void ct_smem(K kernel, size_t bytes) {
     // opt in above 32 KB: the 48 KB default also has to hold the static shared memory
@@ -372,10 +492,20 @@ static void convz_L(cplx_t<R>* S, const R* Nred, int nz, int ny, int nxh, int pi
     constexpr int NT = L * 6 * NB / kE;
     static_assert(NT <= kMaxFftThreads, "CTA size");
     const size_t smem = sizeof(cplx_t<R>) * (size_t)6 * NB * ((L - 1) + ((L - 1) >> 4) + 1);
-    auto k = k_convz_ct<R, L, NB, NT>;
-    ct_smem(k, smem);
-    dim3 grid((unsigned)ceil_div(nxh, NB), (unsigned)(ny + 1));
-    k<<<grid, NT, smem, st>>>(S, Nred, nz, ny, nxh, pitch, static_cast<const cplx_t<R>*>(tw));
+    if constexpr (L <= 32) {
+        // transforms in registers: one thread per column, NB columns of kx
+        constexpr int NBR = sizeof(R) == 4 ? 32 : 16;
+        constexpr size_t smem_r = sizeof(cplx_t<R>) * (size_t)L * 6 * NBR;
+        auto kr = k_convz_reg<R, L / 2, NBR>;
+        ct_smem(kr, smem_r);
+        dim3 grid((unsigned)ceil_div(nxh, NBR), (unsigned)(ny + 1));
+        kr<<<grid, 6 * NBR, smem_r, st>>>(S, Nred, ny, nxh, pitch, static_cast<const cplx_t<R>*>(tw));
+    } else {
+        auto k = k_convz_ct<R, L, NB, NT>;
+        ct_smem(k, smem);
+        dim3 grid((unsigned)ceil_div(nxh, NB), (unsigned)(ny + 1));
+        k<<<grid, NT, smem, st>>>(S, Nred, nz, ny, nxh, pitch, static_cast<const cplx_t<R>*>(tw));
+    }
     MAF_LAUNCH_CHECK();
 }
 
@@ -393,7 +523,7 @@ static void convy_L(cplx_t<R>* S, const R* Nred, int ny, int nxh, int pitch, con
 
 template <typename R, int LC>
 static void xinv_L(const cplx_t<R>* S1, int pitch, const void* tw, const void* twP, const Geom& g, R scale, const R* m,
-                   const MsInfo& ms, const TermList& tl, const EpilogueArgs& ep, cudaStream_t st, int* nblocks) {
+                   const MsInfo& ms, const TermList& tl_in, const EpilogueArgs& ep, cudaStream_t st, int* nblocks) {
     // half the column-pass tile: the epilogue's register demand allows one
     // 384-thread CTA per SM, two CTAs of half the rows overlap their phases
     constexpr int NBR = pow2floor(cmax(1, kTileC<R> / (6 * LC)));
@@ -404,7 +534,9 @@ static void xinv_L(const cplx_t<R>* S1, int pitch, const void* tw, const void* t
     const size_t smem = sizeof(cplx_t<R>) * (size_t)NC * SB;
     const int64_t rows_pc = (int64_t)g.ny * g.nz;
     const unsigned blocks = (unsigned)ceil_div(rows_pc, NBR);
-    const int run4 = run4_eligible(g, m, ms, tl, ep) ? 1 : 0;
+    const int run4 = run4_eligible(g, m, ms, tl_in, ep) ? 1 : 0;
+    TermList tl = tl_in;
+    if (run4) prepare_run4(tl, g, ms.Ms);
     if (nblocks) *nblocks = (int)blocks;
     const auto* t = static_cast<const cplx_t<R>*>(tw);
     const auto* tp = static_cast<const cplx_t<R>*>(twP);
