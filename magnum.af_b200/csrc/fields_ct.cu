@@ -29,22 +29,26 @@ __global__ void __launch_bounds__(NT) k_xfwd_ct(const R* __restrict__ in, int n_
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C* s = reinterpret_cast<C*>(smem_raw);
     constexpr int SB = (LC - 1) + ((LC - 1) >> 4) + 1;
-    constexpr int E = LC * NB / NT;
     static_assert(LC * NB % NT == 0, "tile");
     const int64_t r0 = (int64_t)blockIdx.x * NB;
-    C v[E];
-#pragma unroll
-    for (int e = 0; e < E; ++e) {
-        const int idx = threadIdx.x + e * NT;
-        const int b = idx / LC;
-        const int k = idx % LC;
+    const bool even = (n_in & 1) == 0;
+    // packed pair (in[2k], in[2k+1]) * Ms of row b, loaded straight into the first stage
+    auto ld = [&](int b, int k) -> C {
         const int64_t row = r0 + b;
         R a = 0, c = 0;
         if (row < rows) {
             const R* rp = in + row * n_in;
             const int x0 = 2 * k, x1 = 2 * k + 1;
-            if (x0 < n_in) a = rp[x0];
-            if (x1 < n_in) c = rp[x1];
+            if (even) {
+                if (x0 < n_in) {
+                    const auto v2 = *reinterpret_cast<const cplx_t<R>*>(rp + x0);
+                    a = v2.x;
+                    c = v2.y;
+                }
+            } else {
+                if (x0 < n_in) a = rp[x0];
+                if (x1 < n_in) c = rp[x1];
+            }
             if (msf) {
                 const R* mp = msf + (row % rows_pc) * n_in;
                 if (x0 < n_in) a *= mp[x0];
@@ -54,15 +58,9 @@ __global__ void __launch_bounds__(NT) k_xfwd_ct(const R* __restrict__ in, int n_
                 c *= ms;
             }
         }
-        v[e] = mk(a, c);
-    }
-#pragma unroll
-    for (int e = 0; e < E; ++e) {
-        const int idx = threadIdx.x + e * NT;
-        s[spad(idx % LC) + (idx / LC) * SB] = v[e];
-    }
-    __syncthreads();
-    ct_fft<R, -1, false, LC, NB, NT>(s, SB, tw, typename CtPlan<LC>::T());
+        return mk(a, c);
+    };
+    ct_fft_in<R, -1, false, LC, NB, NT>(s, SB, tw, ld, typename CtPlan<LC>::T());
     const R half = (R)0.5;
     for (int idx = threadIdx.x; idx < NB * (LC + 1); idx += NT) {
         const int b = idx / (LC + 1);
@@ -307,47 +305,34 @@ __global__ void __launch_bounds__(NT) k_xinv_ct(const cplx_t<R>* __restrict__ S1
     C* s = reinterpret_cast<C*>(smem_raw);
     constexpr int NC = 3 * NBR;
     constexpr int SB = (LC - 1) + ((LC - 1) >> 4) + 1;
-    constexpr int E = LC * NC / NT;
     static_assert(LC * NC % NT == 0, "tile");
-    const int64_t rows_pc = (int64_t)g.ny * g.nz;
-    const int64_t ry0 = (int64_t)blockIdx.x * NBR;
-    C v[E];
-#pragma unroll
-    for (int e = 0; e < E; ++e) {
-        const int idx = threadIdx.x + e * NT;
-        const int cb = idx / LC;
-        const int k = idx % LC;
-        const int comp = cb / NBR;
-        const int64_t ry = ry0 + cb % NBR;
-        C Z = mk((R)0, (R)0);
-        if (ry < rows_pc) {
-            const C* rp = S1 + (comp * rows_pc + ry) * pitch;
-            const C Xk = rp[k];
-            const C Xm = rp[LC - k];
-            const C E_ = cadd(Xk, cconj(Xm));
-            const C O = cmulc(csub(Xk, cconj(Xm)), twP[k]);
-            Z = cadd(E_, cmul_i<1>(O));
-        }
-        v[e] = Z;
-    }
-#pragma unroll
-    for (int e = 0; e < E; ++e) {
-        const int idx = threadIdx.x + e * NT;
-        s[spad(idx % LC) + (idx / LC) * SB] = v[e];
-    }
-    __syncthreads();
-    ct_fft<R, 1, false, LC, NC, NT>(s, SB, tw, typename CtPlan<LC>::T());
+    const int rows_pc = g.ny * g.nz;
+    const int ry0 = blockIdx.x * NBR;
+    // Z[k] = (X[k] + X*[LC-k]) + i (X[k] - X*[LC-k]) W^-k of column (comp, row),
+    // formed from global memory straight into the first stage
+    auto ld = [&](int col, int k) -> C {
+        const int comp = col / NBR;
+        const int ry = ry0 + col % NBR;
+        if (ry >= rows_pc) return mk((R)0, (R)0);
+        const C* rp = S1 + ((int64_t)comp * rows_pc + ry) * pitch;
+        const C Xk = rp[k];
+        const C Xm = rp[LC - k];
+        const C E_ = cadd(Xk, cconj(Xm));
+        const C O = cmulc(csub(Xk, cconj(Xm)), twP[k]);
+        return cadd(E_, cmul_i<1>(O));
+    };
+    ct_fft_in<R, 1, false, LC, NC, NT>(s, SB, tw, ld, typename CtPlan<LC>::T());
     if constexpr (EPI == EPI_H || EPI == EPI_LLG) {
         if (run4) {
             const int runs = g.nx >> 2;
             for (int idx = threadIdx.x; idx < NBR * runs; idx += NT) {
                 const int b = idx / runs;
                 const int x0 = (idx - b * runs) << 2;
-                const int64_t ry = ry0 + b;
+                const int ry = ry0 + b;
                 if (ry >= rows_pc) continue;
-                const int z = (int)(ry / g.ny);
-                const int y = (int)(ry - (int64_t)z * g.ny);
-                const int64_t cell0 = ry * g.nx + x0;
+                const int z = ry / g.ny;
+                const int y = ry - z * g.ny;
+                const int64_t cell0 = (int64_t)ry * g.nx + x0;
                 Run4<R> r;
                 run4_load(m, g, x0, y, z, cell0, r);
                 R hd[4][3];
@@ -368,11 +353,11 @@ __global__ void __launch_bounds__(NT) k_xinv_ct(const cplx_t<R>* __restrict__ S1
     for (int idx = threadIdx.x; idx < NBR * g.nx; idx += NT) {
         const int b = idx / g.nx;
         const int x = idx - b * g.nx;
-        const int64_t ry = ry0 + b;
+        const int ry = ry0 + b;
         if (ry >= rows_pc) continue;
-        const int z = (int)(ry / g.ny);
-        const int y = (int)(ry - (int64_t)z * g.ny);
-        const int64_t cell = ry * g.nx + x;
+        const int z = ry / g.ny;
+        const int y = ry - z * g.ny;
+        const int64_t cell = (int64_t)ry * g.nx + x;
         R hd[3];
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
