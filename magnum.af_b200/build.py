@@ -60,7 +60,9 @@ def build(force: bool = False, verbose: bool = False) -> str:
     def compile_one(item):
         src, extra = item
         obj = os.path.join(OBJDIR, src.replace(".cu", ".o"))
-        cmd = [nv, *COMMON, *ARCH, *extra, "-c", os.path.join(CSRC, src), "-o", obj]
+        # MAF_NVCC_EXTRA: additional nvcc options, e.g. -DMAF_COLS_TILE_F32=16384 (tile sizes)
+        user = os.environ.get("MAF_NVCC_EXTRA", "").split()
+        cmd = [nv, *COMMON, *ARCH, *extra, *user, "-c", os.path.join(CSRC, src), "-o", obj]
         if verbose:
             print(" ".join(cmd), flush=True)
         r = subprocess.run(cmd, capture_output=True, text=True)

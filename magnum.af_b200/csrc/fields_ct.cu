@@ -61,17 +61,24 @@ __global__ void __launch_bounds__(NT) k_xfwd_ct(const R* __restrict__ in, int n_
         return mk(a, c);
     };
     ct_fft_in<R, -1, false, LC, NB, NT>(s, SB, tw, ld, typename CtPlan<LC>::T());
+    // R2C post-processing by pairs: with E = (Z_k + Z*_{L-k})/2, O = -i (Z_k - Z*_{L-k})/2
+    // and t = W_{2L}^k O, X[k] = E + t and X[L-k] = (E - t)*  (W_{2L}^{L-k} = -(W_{2L}^k)*),
+    // so one pair of shared-memory reads and one twiddle give two outputs.
     const R half = (R)0.5;
-    for (int idx = threadIdx.x; idx < NB * (LC + 1); idx += NT) {
-        const int b = idx / (LC + 1);
-        const int k = idx - b * (LC + 1);
+    constexpr int KH = LC / 2 + 1;
+    for (int idx = threadIdx.x; idx < NB * KH; idx += NT) {
+        const int b = idx / KH;
+        const int k = idx - b * KH;
         const int64_t row = r0 + b;
         if (row >= rows) continue;
-        const C Zk = s[spad(k == LC ? 0 : k) + b * SB];
+        const C Zk = s[spad(k) + b * SB];
         const C Zm = s[spad(k == 0 ? 0 : LC - k) + b * SB];
         const C E_ = cscale(cadd(Zk, cconj(Zm)), half);
         const C O = cscale(cmul_i<-1>(csub(Zk, cconj(Zm))), half);
-        out[row * pitch + k] = cadd(E_, cmul(twP[k], O));
+        const C t = cmul(twP[k], O);
+        C* o = out + row * pitch;
+        o[k] = cadd(E_, t);
+        if (k < LC / 2) o[LC - k] = cconj(csub(E_, t));
     }
 }
 
@@ -432,6 +439,11 @@ template <typename K> static void ct_smem(K kernel, size_t bytes) {
 // x passes, 8192 / 4096 for the column passes (a 32-byte row segment at least)
 template <typename R> constexpr int kTileX = sizeof(R) == 4 ? 4096 : 2048;
 template <typename R> constexpr int kTileC = sizeof(R) == 4 ? 8192 : 4096;
+// complex values per CTA tile of the y passes (columns x length); a build option
+#ifndef MAF_COLS_TILE_F32
+#define MAF_COLS_TILE_F32 8192
+#endif
+template <typename R> constexpr int kTileCols = sizeof(R) == 4 ? MAF_COLS_TILE_F32 : 4096;
 constexpr int cmax(int a, int b) { return a > b ? a : b; }
 constexpr int cmin(int a, int b) { return a < b ? a : b; }
 constexpr int pow2floor(int x) {
@@ -459,9 +471,9 @@ static void xfwd_L(const R* in, int n_in, int64_t rows, int64_t rows_pc, const R
 template <typename R, int DIR, int L>
 static void cols_L(const cplx_t<R>* in, cplx_t<R>* out, int n_in, int n_out, int ncols, int64_t in_si, int64_t out_si,
                    int64_t in_sbat, int64_t out_sbat, int nbat, const void* tw, cudaStream_t st) {
-    constexpr int NB = pow2floor(cmin(32, cmax(1, kTileC<R> / L)));
+    constexpr int NB = pow2floor(cmin(32, cmax(1, kTileCols<R> / L)));
     constexpr int NT = L * NB / kE;
-    static_assert(NT <= kMaxFftThreads, "CTA size");
+    static_assert(NT <= 1024, "CTA size");
     const size_t smem = sizeof(cplx_t<R>) * (size_t)NB * ((L - 1) + ((L - 1) >> 4) + 1);
     auto k = k_cols_ct<R, DIR, L, NB, NT>;
     ct_smem(k, smem);
