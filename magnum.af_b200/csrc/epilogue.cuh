@@ -124,38 +124,54 @@ __device__ __forceinline__ void epilogue_cell(const Geom& g, int x, int y, int z
 }
 
 // ---------------------------------------------------------------------------
-// Fast epilogue for a run of 4 consecutive cells along x (x0 % 4 == 0): all
+// Fast epilogue for a run of N = 2 or 4 consecutive cells along x (x0 % N == 0): all
 // m values the stencils need (the run, its two x neighbours, and the runs at
 // y-1, y+1, z-1, z+1) are fetched first with vector loads, then the terms are
 // evaluated.  Valid when the term list holds only demag, exchange, interface
 // DMI, uniaxial and cubic anisotropy with scalar parameters and a uniform
-// Zeeman field, and the state has no Ms_field (run4_eligible on the host).
+// Zeeman field, the state has no Ms_field and nx % 4 == 0 (run4_eligible on the host).
 // Same arithmetic per cell as add_local_term / epilogue_cell.
 // ---------------------------------------------------------------------------
-template <typename R> struct Run4 {
-    R c[3][4];            // the run
+template <typename R, int N> struct RunN {
+    R c[3][N];            // the run
     R xl[3], xr[3];       // x neighbours of the first and the last cell
-    R ym[3][4], yp[3][4], zm[3][4], zp[3][4];
+    R ym[3][N], yp[3][N], zm[3][N], zp[3][N];
     bool hxl, hxr, hym, hyp, hzm, hzp;
 };
 
-template <typename R> __device__ __forceinline__ void load4(const R* __restrict__ p, R out[4]) {
-    if constexpr (sizeof(R) == 4) {
+template <typename R, int N> __device__ __forceinline__ void loadN(const R* __restrict__ p, R out[N]) {
+    if constexpr (sizeof(R) == 4 && N == 4) {
         const float4 v = *reinterpret_cast<const float4*>(p);
         out[0] = v.x; out[1] = v.y; out[2] = v.z; out[3] = v.w;
+    } else if constexpr (sizeof(R) == 4) {
+        const float2 v = *reinterpret_cast<const float2*>(p);
+        out[0] = v.x; out[1] = v.y;
     } else {
-        const double2 a = reinterpret_cast<const double2*>(p)[0];
-        const double2 b = reinterpret_cast<const double2*>(p)[1];
-        out[0] = a.x; out[1] = a.y; out[2] = b.x; out[3] = b.y;
+#pragma unroll
+        for (int h = 0; h < N / 2; ++h) {
+            const double2 a = reinterpret_cast<const double2*>(p)[h];
+            out[2 * h] = a.x; out[2 * h + 1] = a.y;
+        }
     }
 }
 
-template <typename R>
-__device__ __forceinline__ void run4_load(const R* __restrict__ m, const Geom& g, int x0, int y, int z, int64_t cell0,
-                                          Run4<R>& r) {
+template <typename R, int N> __device__ __forceinline__ void storeN(R* p, const R v[N]) {
+    if constexpr (sizeof(R) == 4 && N == 4) {
+        *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
+    } else if constexpr (sizeof(R) == 4) {
+        *reinterpret_cast<float2*>(p) = make_float2(v[0], v[1]);
+    } else {
+#pragma unroll
+        for (int h = 0; h < N / 2; ++h) reinterpret_cast<double2*>(p)[h] = make_double2(v[2 * h], v[2 * h + 1]);
+    }
+}
+
+template <typename R, int N>
+__device__ __forceinline__ void runN_load(const R* __restrict__ m, const Geom& g, int x0, int y, int z, int64_t cell0,
+                                          RunN<R, N>& r) {
     const int64_t sy = g.nx, sz = (int64_t)g.nx * g.ny;
     r.hxl = x0 > 0;
-    r.hxr = x0 + 4 < g.nx;
+    r.hxr = x0 + N < g.nx;
     r.hym = y > 0;
     r.hyp = y < g.ny - 1;
     r.hzm = z > 0;
@@ -163,45 +179,45 @@ __device__ __forceinline__ void run4_load(const R* __restrict__ m, const Geom& g
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
         const R* p = m + c * g.N + cell0;
-        load4(p, r.c[c]);
+        loadN<R, N>(p, r.c[c]);
         r.xl[c] = r.hxl ? p[-1] : (R)0;
-        r.xr[c] = r.hxr ? p[4] : (R)0;
+        r.xr[c] = r.hxr ? p[N] : (R)0;
 #pragma unroll
-        for (int i = 0; i < 4; ++i) { r.ym[c][i] = 0; r.yp[c][i] = 0; r.zm[c][i] = 0; r.zp[c][i] = 0; }
-        if (r.hym) load4(p - sy, r.ym[c]);
-        if (r.hyp) load4(p + sy, r.yp[c]);
-        if (r.hzm) load4(p - sz, r.zm[c]);
-        if (r.hzp) load4(p + sz, r.zp[c]);
+        for (int i = 0; i < N; ++i) { r.ym[c][i] = 0; r.yp[c][i] = 0; r.zm[c][i] = 0; r.zp[c][i] = 0; }
+        if (r.hym) loadN<R, N>(p - sy, r.ym[c]);
+        if (r.hyp) loadN<R, N>(p + sy, r.yp[c]);
+        if (r.hzm) loadN<R, N>(p - sz, r.zm[c]);
+        if (r.hzp) loadN<R, N>(p + sz, r.zp[c]);
     }
 }
 
-// H of the four cells of the run (hd = demag contribution).  Terms outer,
+// H of the N cells of the run (hd = demag contribution).  Terms outer,
 // cells inner; the per-term constants come from TermDesc::q, prepared once per
 // launch on the host (prepare_run4), so no division is left in the cell loop:
 //   exchange  q = 2A/(mu0 Ms) / (dx^2, dy^2, dz^2)
 //   DMI       q = 2D/(mu0 Ms), 1/(2dx), 1/(2dy), 1/(2dz)
 //   uniaxial  q = 2Ku/(mu0 Ms)
 //   cubic     q = -2Kc1/(mu0 Ms), -2Kc2/(mu0 Ms), -4Kc3/(mu0 Ms)
-template <typename R>
-__device__ __forceinline__ void run4_fields(const TermList& tl, const Run4<R>& r, const R hd[4][3], R h[4][3]) {
+template <typename R, int N>
+__device__ __forceinline__ void runN_fields(const TermList& tl, const RunN<R, N>& r, const R hd[N][3], R h[N][3]) {
 #pragma unroll
-    for (int i = 0; i < 4; ++i) h[i][0] = h[i][1] = h[i][2] = 0;
+    for (int i = 0; i < N; ++i) h[i][0] = h[i][1] = h[i][2] = 0;
     for (int it = 0; it < tl.n; ++it) {
         const TermDesc& t = tl.t[it];
         switch (t.kind) {
             case TK_DEMAG:
 #pragma unroll
-                for (int i = 0; i < 4; ++i) { h[i][0] += hd[i][0]; h[i][1] += hd[i][1]; h[i][2] += hd[i][2]; }
+                for (int i = 0; i < N; ++i) { h[i][0] += hd[i][0]; h[i][1] += hd[i][1]; h[i][2] += hd[i][2]; }
                 break;
             case TK_EXCHANGE: {
                 const R qx = (R)t.q[0], qy = (R)t.q[1], qz = (R)t.q[2];
 #pragma unroll
                 for (int c = 0; c < 3; ++c) {
 #pragma unroll
-                    for (int i = 0; i < 4; ++i) {
+                    for (int i = 0; i < N; ++i) {
                         const R v = r.c[c][i];
                         const R left = i > 0 ? r.c[c][i - 1] - v : (r.hxl ? r.xl[c] - v : -v);
-                        const R right = i < 3 ? r.c[c][i + 1] - v : (r.hxr ? r.xr[c] - v : -v);
+                        const R right = i < N - 1 ? r.c[c][i + 1] - v : (r.hxr ? r.xr[c] - v : -v);
                         const R ay = (r.hym ? r.ym[c][i] - v : -v) + (r.hyp ? r.yp[c][i] - v : -v);
                         const R az = (r.hzm ? r.zm[c][i] - v : -v) + (r.hzp ? r.zp[c][i] - v : -v);
                         h[i][c] += (left + right) * qx + ay * qy + az * qz;
@@ -214,12 +230,12 @@ __device__ __forceinline__ void run4_fields(const TermList& tl, const Run4<R>& r
                 const R n0 = (R)t.p[1], n1 = (R)t.p[2], n2 = (R)t.p[3];
                 auto nm = [&](const R v0, const R v1, const R v2) { return n0 * v0 + n1 * v1 + n2 * v2; };
 #pragma unroll
-                for (int i = 0; i < 4; ++i) {
+                for (int i = 0; i < N; ++i) {
                     R lm[3], rm[3];
 #pragma unroll
                     for (int c = 0; c < 3; ++c) {
                         lm[c] = i > 0 ? r.c[c][i - 1] : r.xl[c];
-                        rm[c] = i < 3 ? r.c[c][i + 1] : r.xr[c];
+                        rm[c] = i < N - 1 ? r.c[c][i + 1] : r.xr[c];
                     }
                     const R div = (rm[0] - lm[0]) * hx + (r.yp[1][i] - r.ym[1][i]) * hy + (r.zp[2][i] - r.zm[2][i]) * hz;
                     const R g0 = (nm(rm[0], rm[1], rm[2]) - nm(lm[0], lm[1], lm[2])) * hx;
@@ -235,7 +251,7 @@ __device__ __forceinline__ void run4_fields(const TermList& tl, const Run4<R>& r
                 const R e0 = (R)t.p[1], e1 = (R)t.p[2], e2 = (R)t.p[3];
                 const R coef = (R)t.q[0];
 #pragma unroll
-                for (int i = 0; i < 4; ++i) {
+                for (int i = 0; i < N; ++i) {
                     const R em = coef * (e0 * r.c[0][i] + e1 * r.c[1][i] + e2 * r.c[2][i]);
                     h[i][0] += e0 * em;
                     h[i][1] += e1 * em;
@@ -249,7 +265,7 @@ __device__ __forceinline__ void run4_fields(const TermList& tl, const Run4<R>& r
                 const R c3[3] = {(R)t.p[9], (R)t.p[10], (R)t.p[11]};
                 const R k1 = (R)t.q[0], k2 = (R)t.q[1], k3 = (R)t.q[2];
 #pragma unroll
-                for (int i = 0; i < 4; ++i) {
+                for (int i = 0; i < N; ++i) {
                     const R m0 = r.c[0][i], m1 = r.c[1][i], m2 = r.c[2][i];
                     const R c1m = c1[0] * m0 + c1[1] * m1 + c1[2] * m2;
                     const R c2m = c2[0] * m0 + c2[1] * m1 + c2[2] * m2;
@@ -267,7 +283,7 @@ __device__ __forceinline__ void run4_fields(const TermList& tl, const Run4<R>& r
             case TK_ZEEMAN: {
                 const R z0 = (R)t.p[0], z1 = (R)t.p[1], z2 = (R)t.p[2];
 #pragma unroll
-                for (int i = 0; i < 4; ++i) { h[i][0] += z0; h[i][1] += z1; h[i][2] += z2; }
+                for (int i = 0; i < N; ++i) { h[i][0] += z0; h[i][1] += z1; h[i][2] += z2; }
                 break;
             }
             default: break;
@@ -276,31 +292,28 @@ __device__ __forceinline__ void run4_fields(const TermList& tl, const Run4<R>& r
 }
 
 // Writes the epilogue output (H, dt*LLG or the LBFGS gradient) of the run.
-template <typename R, int EPI>
-__device__ __forceinline__ void run4_epilogue(const TermList& tl, const Geom& g, const Run4<R>& r, int64_t cell0,
-                                              R Ms, const R hd[4][3], const EpilogueArgs& ep) {
-    R h[4][3];
-    run4_fields(tl, r, hd, h);
+template <typename R, int EPI, int N>
+__device__ __forceinline__ void runN_epilogue(const TermList& tl, const Geom& g, const RunN<R, N>& r, int64_t cell0,
+                                              const R hd[N][3], const EpilogueArgs& ep) {
+    R h[N][3];
+    runN_fields<R, N>(tl, r, hd, h);
     if constexpr (EPI == EPI_H) {
         R* o = static_cast<R*>(ep.out);
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-            R* p = o + c * g.N + cell0;
-            if constexpr (sizeof(R) == 4) {
-                *reinterpret_cast<float4*>(p) = make_float4(h[0][c], h[1][c], h[2][c], h[3][c]);
-            } else {
-                reinterpret_cast<double2*>(p)[0] = make_double2(h[0][c], h[1][c]);
-                reinterpret_cast<double2*>(p)[1] = make_double2(h[2][c], h[3][c]);
-            }
+            R v[N];
+#pragma unroll
+            for (int i = 0; i < N; ++i) v[i] = h[i][c];
+            storeN<R, N>(o + c * g.N + cell0, v);
         }
     } else {
         const double* m64 = ep.llg.m64;
         double* o = static_cast<double*>(ep.out);
-        double M[3][4], out[3][4];
+        double M[3][N], out[3][N];
 #pragma unroll
-        for (int c = 0; c < 3; ++c) load4(m64 + c * g.N + cell0, M[c]);
+        for (int c = 0; c < 3; ++c) loadN<double, N>(m64 + c * g.N + cell0, M[c]);
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
+        for (int i = 0; i < N; ++i) {
             double H0 = h[i][0], H1 = h[i][1], H2 = h[i][2];
             if constexpr (EPI == EPI_LLG) {
                 if (ep.llg.sigma != 0.0) {
@@ -338,11 +351,7 @@ __device__ __forceinline__ void run4_epilogue(const TermList& tl, const Geom& g,
             }
         }
 #pragma unroll
-        for (int c = 0; c < 3; ++c) {
-            double2* p = reinterpret_cast<double2*>(o + c * g.N + cell0);
-            p[0] = make_double2(out[c][0], out[c][1]);
-            p[1] = make_double2(out[c][2], out[c][3]);
-        }
+        for (int c = 0; c < 3; ++c) storeN<double, N>(o + c * g.N + cell0, out[c]);
     }
 }
 

@@ -19,6 +19,17 @@ namespace mafb {
 template <typename R, int NT, int T32, int T64>
 constexpr int kMinBlocks = (sizeof(R) == 4 ? T32 : T64) / NT > 1 ? (sizeof(R) == 4 ? T32 : T64) / NT : 1;
 
+// cells per run of the x-inverse fast epilogue (2 or 4; nx % 4 == 0 either way); a build option
+#ifndef MAF_RUN_CELLS
+#define MAF_RUN_CELLS 2
+#endif
+constexpr int kRunCells = MAF_RUN_CELLS;
+static_assert(kRunCells == 2 || kRunCells == 4, "run length");
+// resident threads per SM the FP32 x-inverse kernel is compiled for (register cap); a build option
+#ifndef MAF_XINV_THREADS
+#define MAF_XINV_THREADS 576
+#endif
+
 // ------------------------------------------------------------------ x forward
 template <typename R, int LC, int NB, int NT>
 __global__ void __launch_bounds__(NT) k_xfwd_ct(const R* __restrict__ in, int n_in, int64_t rows, int64_t rows_pc,
@@ -303,7 +314,7 @@ __global__ void __launch_bounds__(NT) k_convy_ct(cplx_t<R>* S, const R* __restri
 
 // --------------------------------------------------- x inverse + epilogue
 template <typename R, int EPI, int LC, int NBR, int NT>
-__global__ void __launch_bounds__(NT) k_xinv_ct(const cplx_t<R>* __restrict__ S1, int pitch,
+__global__ void __launch_bounds__(NT, (kMinBlocks<R, NT, MAF_XINV_THREADS, 192>)) k_xinv_ct(const cplx_t<R>* __restrict__ S1, int pitch,
                                                 const cplx_t<R>* __restrict__ tw, const cplx_t<R>* __restrict__ twP,
                                                 Geom g, R scale, const R* __restrict__ m, MsInfo ms, TermList tl,
                                                 EpilogueArgs ep, int run4) {
@@ -331,27 +342,30 @@ __global__ void __launch_bounds__(NT) k_xinv_ct(const cplx_t<R>* __restrict__ S1
     ct_fft_in<R, 1, false, LC, NC, NT>(s, SB, tw, ld, typename CtPlan<LC>::T());
     if constexpr (EPI == EPI_H || EPI == EPI_LLG) {
         if (run4) {
-            const int runs = g.nx >> 2;
+            constexpr int RN = kRunCells;  // cells per run (2 or 4)
+            const int runs = g.nx / RN;
             for (int idx = threadIdx.x; idx < NBR * runs; idx += NT) {
                 const int b = idx / runs;
-                const int x0 = (idx - b * runs) << 2;
+                const int x0 = (idx - b * runs) * RN;
                 const int ry = ry0 + b;
                 if (ry >= rows_pc) continue;
                 const int z = ry / g.ny;
                 const int y = ry - z * g.ny;
                 const int64_t cell0 = (int64_t)ry * g.nx + x0;
-                Run4<R> r;
-                run4_load(m, g, x0, y, z, cell0, r);
-                R hd[4][3];
+                RunN<R, RN> r;
+                runN_load<R, RN>(m, g, x0, y, z, cell0, r);
+                R hd[RN][3];
 #pragma unroll
-                for (int i = 0; i < 4; ++i) {
+                for (int i = 0; i < RN; i += 2) {
 #pragma unroll
                     for (int c = 0; c < 3; ++c) {
+                        // cells x0 + i and x0 + i + 1 are the two halves of one packed value
                         const C val = s[spad((x0 + i) >> 1) + (c * NBR + b) * SB];
-                        hd[i][c] = scale * (((x0 + i) & 1) ? val.y : val.x);
+                        hd[i][c] = scale * val.x;
+                        hd[i + 1][c] = scale * val.y;
                     }
                 }
-                run4_epilogue<R, EPI>(tl, g, r, cell0, (R)ms.Ms, hd, ep);
+                runN_epilogue<R, EPI, RN>(tl, g, r, cell0, hd, ep);
             }
             return;
         }
