@@ -194,6 +194,19 @@ int maf_stochastic_llg_noise(maf_stoch h, maf_state s, unsigned long long index,
 /* Stochastic_Integrator::get_calls */
 int maf_stochastic_llg_calls(maf_stoch h, unsigned long long* calls);
 
+/* Batched ensemble (no counterpart in the reference, which steps one integrator
+ * at a time): member i is integrator i stepping state i (distinct states on
+ * distinct streams; any meshes).  maf_stoch_batch_steps advances every member by
+ * nsteps steps; after a first eager step, pairs of steps of all members replay
+ * one captured CUDA graph in which each member runs on its own stream, so small
+ * members run concurrently.  Results are bit-identical to calling
+ * maf_stochastic_llg_steps on each member.  Do not change a member's stream
+ * while it belongs to a batch. */
+typedef struct maf_stoch_batch_s* maf_stoch_batch;
+int maf_stoch_batch_create(maf_stoch_batch* out, const maf_stoch* integrators, const maf_state* states, int n);
+int maf_stoch_batch_destroy(maf_stoch_batch b);
+int maf_stoch_batch_steps(maf_stoch_batch b, int nsteps);
+
 /* ------------------------------------------------------------- LBFGS ---
  * LBFGS_Minimizer(terms, tolerance = 1e-6, maxIter = 230)
  * (magnumaf/include/magnumaf/solvers/lbfgs_minimizer.hpp:9-12, magnumaf/src/solvers/lbfgs_minimizer.cpp:19-505):

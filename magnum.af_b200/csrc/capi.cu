@@ -429,7 +429,10 @@ struct StochStage {
     double scale = 0;
 };
 
-void stoch_step(maf_stoch_s* h, maf_state_s* st) {
+// One step.  With q_dev (a device copy of h->calls) the noise stream indices are
+// read from q_dev on the device and q_dev is advanced by a device kernel, so the
+// step can be captured in a CUDA graph and replayed.
+void stoch_step(maf_stoch_s* h, maf_state_s* st, unsigned long long* q_dev = nullptr) {
     StateD& s = st->s;
     if (s.has_Ms_field) throw Error(MAF_ERR_BADARG, "Stochastic_LLG uses the scalar Ms (stochastic_integrator.cpp:9-10)");
     const int64_t N = s.md.N(), n3 = 3 * N;
@@ -482,6 +485,12 @@ void stoch_step(maf_stoch_s* h, maf_state_s* st) {
             ep.llg.seed = h->seed;
             ep.llg.member = h->member;
             ep.llg.noise_index = sg.index;
+            if (q_dev) {  // index = mul * q + offset, q read on the device
+                const unsigned mul = h->mode == 1 ? 2u : 1u;
+                ep.llg.noise_base = q_dev;
+                ep.llg.noise_mul = mul;
+                ep.llg.noise_index = sg.index - mul * q;
+            }
         }
         if (sg.n == 0) {
             ep.llg.m64 = s.m64.as<double>();
@@ -513,6 +522,7 @@ void stoch_step(maf_stoch_s* h, maf_state_s* st) {
     rk_finalize(s.m64.as<double>(), fin, dummy, 0, 1.0, 0.0, h->mcand.as<double>(), 2, N, h->partials.as<double>(),
                 h->errbuf.as<double>(), s.stream);
     std::swap(s.m64, h->mcand);
+    if (q_dev) inc_counter(q_dev, s.stream);
     st->m32_valid = false;
     s.t += dt;
     s.steps++;
@@ -1921,6 +1931,173 @@ int maf_string_image(maf_string h, int i, maf_state* image) {
         check(h && image, "NULL argument");
         check(i >= 0 && i < h->n_interp, "maf_string_image: image index out of range");
         *image = h->images[i].get();
+    });
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Batched stochastic ensembles: every member (integrator i steps state i) is
+// advanced by one CUDA graph.  The graph holds two steps of every member, each
+// member on its own state's stream between a fork and a join event, so members
+// of uneven meshes run concurrently and two steps of the whole ensemble cost one
+// graph launch.  Two steps because a step swaps the state and candidate buffers:
+// after two the buffers are back where the graph expects them.  The noise
+// stream index comes from a device step counter per member that the graph
+// advances, so every replay draws the next numbers; results are bit-identical
+// to stepping the members one after another.
+// ---------------------------------------------------------------------------
+struct maf_stoch_batch_s {
+    std::vector<maf_stoch_s*> its;
+    std::vector<maf_state_s*> sts;
+    cudaStream_t root = nullptr;
+    cudaEvent_t fork = nullptr, done = nullptr;
+    std::vector<cudaEvent_t> join;
+    DevBuf q;  // per-member step counters (device)
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    std::vector<const void*> m_at_capture;  // state buffers the graph was captured with
+    bool warm = false;
+    ~maf_stoch_batch_s() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        for (auto e : join) cudaEventDestroy(e);
+        if (fork) cudaEventDestroy(fork);
+        if (done) cudaEventDestroy(done);
+        if (root) cudaStreamDestroy(root);
+    }
+};
+
+namespace {
+
+void batch_drop_graph(maf_stoch_batch_s* b) {
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    b->exec = nullptr;
+    b->graph = nullptr;
+}
+
+// device counters <- host step counts
+void batch_upload_counters(maf_stoch_batch_s* b) {
+    std::vector<unsigned long long> q(b->its.size());
+    for (size_t i = 0; i < q.size(); ++i) q[i] = b->its[i]->calls;
+    MAF_CUDA(cudaMemcpyAsync(b->q.p, q.data(), sizeof(unsigned long long) * q.size(), cudaMemcpyHostToDevice,
+                             b->root));
+    MAF_CUDA(cudaStreamSynchronize(b->root));
+}
+
+void batch_capture(maf_stoch_batch_s* b) {
+    batch_drop_graph(b);
+    const size_t n = b->its.size();
+    auto* q = b->q.as<unsigned long long>();
+    // host-side state advances while the work is only recorded: restore it
+    std::vector<double> t(n);
+    std::vector<unsigned long long> steps(n), calls(n);
+    for (size_t i = 0; i < n; ++i) {
+        t[i] = b->sts[i]->s.t;
+        steps[i] = b->sts[i]->s.steps;
+        calls[i] = b->its[i]->calls;
+    }
+    MAF_CUDA(cudaStreamBeginCapture(b->root, cudaStreamCaptureModeThreadLocal));
+    try {
+        MAF_CUDA(cudaEventRecord(b->fork, b->root));
+        for (size_t i = 0; i < n; ++i) {
+            cudaStream_t s = b->sts[i]->s.stream;
+            MAF_CUDA(cudaStreamWaitEvent(s, b->fork, 0));
+            stoch_step(b->its[i], b->sts[i], q + i);
+            stoch_step(b->its[i], b->sts[i], q + i);
+            MAF_CUDA(cudaEventRecord(b->join[i], s));
+            MAF_CUDA(cudaStreamWaitEvent(b->root, b->join[i], 0));
+        }
+    } catch (...) {
+        cudaGraph_t g = nullptr;
+        cudaStreamEndCapture(b->root, &g);
+        if (g) cudaGraphDestroy(g);
+        cudaGetLastError();
+        throw;
+    }
+    MAF_CUDA(cudaStreamEndCapture(b->root, &b->graph));
+    MAF_CUDA(cudaGraphInstantiate(&b->exec, b->graph, 0));
+    b->m_at_capture.clear();
+    for (size_t i = 0; i < n; ++i) {
+        b->sts[i]->s.t = t[i];
+        b->sts[i]->s.steps = steps[i];
+        b->its[i]->calls = calls[i];
+        b->m_at_capture.push_back(b->sts[i]->s.m64.p);
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+int maf_stoch_batch_create(maf_stoch_batch* out, const maf_stoch* integrators, const maf_state* states, int n) {
+    return guarded([&] {
+        check(out && integrators && states && n > 0, "maf_stoch_batch_create: bad argument");
+        auto b = std::make_unique<maf_stoch_batch_s>();
+        for (int i = 0; i < n; ++i) {
+            check(integrators[i] && states[i], "maf_stoch_batch_create: NULL member");
+            check(!integrators[i]->terms.empty(), "Stochastic_LLG: no field terms");
+            check(!states[i]->s.has_Ms_field, "Stochastic_LLG uses the scalar Ms (stochastic_integrator.cpp:9-10)");
+            for (int j = 0; j < i; ++j) {
+                check(states[j] != states[i], "maf_stoch_batch_create: a state appears twice");
+                check(integrators[j] != integrators[i], "maf_stoch_batch_create: an integrator appears twice");
+                check(states[j]->s.stream != states[i]->s.stream,
+                      "maf_stoch_batch_create: members must run on distinct streams");
+            }
+            b->its.push_back(integrators[i]);
+            b->sts.push_back(states[i]);
+        }
+        MAF_CUDA(cudaStreamCreateWithFlags(&b->root, cudaStreamNonBlocking));
+        MAF_CUDA(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming));
+        MAF_CUDA(cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming));
+        b->join.resize(n);
+        for (int i = 0; i < n; ++i) MAF_CUDA(cudaEventCreateWithFlags(&b->join[i], cudaEventDisableTiming));
+        b->q.alloc(sizeof(unsigned long long) * n);
+        *out = b.release();
+    });
+}
+
+int maf_stoch_batch_destroy(maf_stoch_batch b) {
+    return guarded([&] { delete b; });
+}
+
+int maf_stoch_batch_steps(maf_stoch_batch b, int nsteps) {
+    return guarded([&] {
+        check(b && nsteps >= 0, "maf_stoch_batch_steps: bad argument");
+        const size_t n = b->its.size();
+        int left = nsteps;
+        for (auto* st : b->sts) MAF_CUDA(cudaStreamSynchronize(st->s.stream));
+        // the first step runs eagerly: it sizes every work buffer before a capture
+        if (left > 0 && !b->warm) {
+            for (size_t i = 0; i < n; ++i) stoch_step(b->its[i], b->sts[i]);
+            --left;
+            b->warm = true;
+        }
+        if (left >= 2) {
+            bool stale = !b->exec;
+            for (size_t i = 0; i < n && !stale; ++i) stale = b->sts[i]->s.m64.p != b->m_at_capture[i];
+            for (auto* st : b->sts) MAF_CUDA(cudaStreamSynchronize(st->s.stream));
+            batch_upload_counters(b);
+            if (stale) batch_capture(b);
+            while (left >= 2) {
+                MAF_CUDA(cudaGraphLaunch(b->exec, b->root));
+                for (size_t i = 0; i < n; ++i) {
+                    b->sts[i]->s.t += b->its[i]->dt;  // twice, as two single steps add it
+                    b->sts[i]->s.t += b->its[i]->dt;
+                    b->sts[i]->s.steps += 2;
+                    b->its[i]->calls += 2;
+                    b->sts[i]->m32_valid = false;
+                }
+                left -= 2;
+            }
+            MAF_CUDA(cudaEventRecord(b->done, b->root));
+            for (auto* st : b->sts) MAF_CUDA(cudaStreamWaitEvent(st->s.stream, b->done, 0));
+        }
+        for (; left > 0; --left)
+            for (size_t i = 0; i < n; ++i) stoch_step(b->its[i], b->sts[i]);
+        for (auto* st : b->sts) MAF_CUDA(cudaStreamSynchronize(st->s.stream));
+        MAF_CUDA(cudaStreamSynchronize(b->root));
     });
 }
 

@@ -78,6 +78,17 @@ struct LLGParams {
     unsigned long long seed = 0;
     unsigned member = 0;
     unsigned long long noise_index = 0;
+    // when set, the stream index is noise_mul * (*noise_base) + noise_index, read on
+    // the device: a captured CUDA graph replays with the step counter it advances
+    const unsigned long long* noise_base = nullptr;
+    unsigned noise_mul = 0;
+    __host__ __device__ unsigned long long stream_index() const {
+#ifdef __CUDA_ARCH__
+        return noise_base ? noise_mul * (*noise_base) + noise_index : noise_index;
+#else
+        return noise_index;
+#endif
+    }
 };
 
 struct EpilogueArgs {

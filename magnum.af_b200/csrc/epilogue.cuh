@@ -91,7 +91,7 @@ __device__ __forceinline__ void epilogue_cell(const Geom& g, int x, int y, int z
             if (ep.llg.sigma != 0.0) {
                 // Heff + h_th (stochastic_llg.cpp:19-22), h_th = sqrt(2D/dt) N(0,1)
                 double xi[3];
-                normal3(ep.llg.seed, ep.llg.member, ep.llg.noise_index, (uint64_t)cell, xi);
+                normal3(ep.llg.seed, ep.llg.member, ep.llg.stream_index(), (uint64_t)cell, xi);
                 H0 += ep.llg.sigma * xi[0];
                 H1 += ep.llg.sigma * xi[1];
                 H2 += ep.llg.sigma * xi[2];
@@ -318,7 +318,7 @@ __device__ __forceinline__ void runN_epilogue(const TermList& tl, const Geom& g,
             if constexpr (EPI == EPI_LLG) {
                 if (ep.llg.sigma != 0.0) {
                     double xi[3];
-                    normal3(ep.llg.seed, ep.llg.member, ep.llg.noise_index, (uint64_t)(cell0 + i), xi);
+                    normal3(ep.llg.seed, ep.llg.member, ep.llg.stream_index(), (uint64_t)(cell0 + i), xi);
                     H0 += ep.llg.sigma * xi[0];
                     H1 += ep.llg.sigma * xi[1];
                     H2 += ep.llg.sigma * xi[2];

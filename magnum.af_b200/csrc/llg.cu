@@ -306,6 +306,15 @@ void lerp(double* out, const double* a, const double* b, double c1, double c2, i
     MAF_LAUNCH_CHECK();
 }
 
+__global__ void k_inc_counter(unsigned long long* c) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) *c += 1;
+}
+
+void inc_counter(unsigned long long* c, cudaStream_t st) {
+    k_inc_counter<<<1, 32, 0, st>>>(c);
+    MAF_LAUNCH_CHECK();
+}
+
 __global__ void k_axpby(double* out, double a, const double* x, double b, const double* y, int64_t n) {
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         const double v = a * x[i];

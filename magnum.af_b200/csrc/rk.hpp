@@ -28,5 +28,7 @@ void normalize_combine(double* m, const double* wa, double stp, const double* s,
 // string method: sum (a-b)^2 over n values (synchronises), out = a + (c1 (b - a)) / c2
 double sqdiff_host(const double* a, const double* b, int64_t n, double* scratch, cudaStream_t st);
 void lerp(double* out, const double* a, const double* b, double c1, double c2, int64_t n, cudaStream_t st);
+// *c += 1 on the device (the step counter of a captured stochastic step)
+void inc_counter(unsigned long long* c, cudaStream_t st);
 
 }  // namespace mafb

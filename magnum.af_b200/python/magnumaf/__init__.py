@@ -105,6 +105,9 @@ _SIGS = {
     "maf_llg_get_h": (_I, [_P, _DP]),
     "maf_llg_counters": (_I, [_P, C.POINTER(C.c_ulonglong)]),
     "maf_mean_m_noalloc": (_I, [_P, C.c_longlong, _DP, _P]),
+    "maf_stoch_batch_create": (_I, [C.POINTER(_P), C.POINTER(_P), C.POINTER(_P), _I]),
+    "maf_stoch_batch_destroy": (_I, [_P]),
+    "maf_stoch_batch_steps": (_I, [_P, _I]),
     "maf_string_create": (_I, [C.POINTER(_P), _P, C.POINTER(_P), _I, _I, _D, _P]),
     "maf_string_destroy": (_I, [_P]),
     "maf_string_step": (_I, [_P]),
@@ -595,6 +598,27 @@ class LBFGS_Minimizer:
         g = C.c_double()
         _ck(lib.maf_lbfgs_stats(self._h, C.byref(it), C.byref(fe), C.byref(g)))
         return {"iterations": it.value, "fevals": fe.value, "grad_max": g.value}
+
+
+class StochasticBatch:
+    """Members (Stochastic_LLG, State) advanced together: after one eager step,
+    pairs of steps of every member replay one captured CUDA graph with each member
+    on its own stream.  Bit-identical to stepping the members one by one."""
+
+    def __init__(self, members):
+        self._members = list(members)
+        its = (_P * len(self._members))(*[it._h for it, _ in self._members])
+        sts = (_P * len(self._members))(*[st._h for _, st in self._members])
+        self._h = _P()
+        _ck(lib.maf_stoch_batch_create(C.byref(self._h), its, sts, len(self._members)))
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib.maf_stoch_batch_destroy(self._h)
+            self._h = None
+
+    def steps(self, n: int):
+        _ck(lib.maf_stoch_batch_steps(self._h, int(n)))
 
 
 class StringMethod:
