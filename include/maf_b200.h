@@ -252,6 +252,29 @@ int maf_string_get_x(maf_string h, double* x, double* x_interp);
 /* image i as a state handle owned by the string (do not destroy it) */
 int maf_string_image(maf_string h, int i, maf_state* image);
 
+/* ------------------------------------------------ learned warm start ---
+ * No counterpart in the reference.  A small convolutional network proposes a
+ * relaxed magnetisation that the LBFGS minimiser then finishes:
+ * y = normalize(m + conv_L(relu(...relu(conv_1(x))))), 3x3 convolutions with zero
+ * padding, cin input channels (the first three are m, the others parameter
+ * maps), `width` channels in the hidden layers, `depth` layers, FP32.  All
+ * array arguments are DEVICE pointers, NCHW: x [B][cin][H][W], y and target
+ * [B][3][H][W].  Parameters: per layer W[cout][cin][3][3] then b[cout]. */
+typedef struct maf_cnn_s* maf_cnn;
+int maf_cnn_create(maf_cnn* out, int cin, int width, int depth, unsigned long long seed);
+int maf_cnn_destroy(maf_cnn h);
+int maf_cnn_n_params(maf_cnn h, long long* n);
+int maf_cnn_get_params(maf_cnn h, float* host);
+/* also resets the Adam moments */
+int maf_cnn_set_params(maf_cnn h, const float* host);
+int maf_cnn_forward(maf_cnn h, const float* x_dev, int B, int H, int W, float* y_dev);
+/* loss = mean over the B*H*W cells of |y - target|^2, gradient of every parameter (host, optional) */
+int maf_cnn_loss_grad(maf_cnn h, const float* x_dev, const float* target_dev, int B, int H, int W, float* loss,
+                      float* grad_host);
+/* one Adam step (beta 0.9 / 0.999, eps 1e-8) with learning rate lr; returns the loss before the step */
+int maf_cnn_train_step(maf_cnn h, const float* x_dev, const float* target_dev, int B, int H, int W, float lr,
+                       float* loss);
+
 /* ------------------------------------------------- no-allocation mean ---
  * No counterpart in the reference.  <m> of a device-resident FP64 field
  * m_dev[3][ncells] (e.g. from maf_state_device_m), with the definition of

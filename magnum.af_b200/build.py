@@ -32,6 +32,7 @@ SOURCES = {
     "newell.cu": ["-fmad=false"],
     "capi.cu": [],
     "noalloc.cu": [],
+    "cnn.cu": [],
 }
 
 

@@ -105,6 +105,14 @@ _SIGS = {
     "maf_llg_get_h": (_I, [_P, _DP]),
     "maf_llg_counters": (_I, [_P, C.POINTER(C.c_ulonglong)]),
     "maf_mean_m_noalloc": (_I, [_P, C.c_longlong, _DP, _P]),
+    "maf_cnn_create": (_I, [C.POINTER(_P), _I, _I, _I, C.c_ulonglong]),
+    "maf_cnn_destroy": (_I, [_P]),
+    "maf_cnn_n_params": (_I, [_P, C.POINTER(C.c_longlong)]),
+    "maf_cnn_get_params": (_I, [_P, _FP]),
+    "maf_cnn_set_params": (_I, [_P, _FP]),
+    "maf_cnn_forward": (_I, [_P, _P, _I, _I, _I, _P]),
+    "maf_cnn_loss_grad": (_I, [_P, _P, _P, _I, _I, _I, _FP, _FP]),
+    "maf_cnn_train_step": (_I, [_P, _P, _P, _I, _I, _I, C.c_float, _FP]),
     "maf_stoch_batch_create": (_I, [C.POINTER(_P), C.POINTER(_P), C.POINTER(_P), _I]),
     "maf_stoch_batch_destroy": (_I, [_P]),
     "maf_stoch_batch_steps": (_I, [_P, _I]),
@@ -598,6 +606,56 @@ class LBFGS_Minimizer:
         g = C.c_double()
         _ck(lib.maf_lbfgs_stats(self._h, C.byref(it), C.byref(fe), C.byref(g)))
         return {"iterations": it.value, "fevals": fe.value, "grad_max": g.value}
+
+
+class ConvNet:
+    """The learned warm-start network (maf_cnn_*): 3x3 convolutions with ReLU,
+    output normalize(m + conv_L(...)), trained with the library's own kernels.
+    Array arguments are device pointers (e.g. torch CUDA tensors' data_ptr()),
+    NCHW float32: x [B][cin][H][W] with m in channels 0..2, y and targets [B][3][H][W]."""
+
+    def __init__(self, cin: int, width: int = 16, depth: int = 4, seed: int = 0):
+        self.cin, self.width, self.depth = int(cin), int(width), int(depth)
+        self._h = _P()
+        _ck(lib.maf_cnn_create(C.byref(self._h), self.cin, self.width, self.depth, int(seed)))
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib.maf_cnn_destroy(self._h)
+            self._h = None
+
+    @property
+    def n_params(self) -> int:
+        n = C.c_longlong()
+        _ck(lib.maf_cnn_n_params(self._h, C.byref(n)))
+        return n.value
+
+    def get_params(self) -> np.ndarray:
+        out = np.empty(self.n_params, dtype=np.float32)
+        _ck(lib.maf_cnn_get_params(self._h, out.ctypes.data_as(_FP)))
+        return out
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        if p.size != self.n_params:
+            raise ValueError("expected %d parameters" % self.n_params)
+        _ck(lib.maf_cnn_set_params(self._h, p.ctypes.data_as(_FP)))
+
+    def forward(self, x_ptr: int, B: int, H: int, W: int, y_ptr: int):
+        _ck(lib.maf_cnn_forward(self._h, C.c_void_p(x_ptr), B, H, W, C.c_void_p(y_ptr)))
+
+    def loss_grad(self, x_ptr: int, t_ptr: int, B: int, H: int, W: int, want_grad: bool = True):
+        loss = C.c_float()
+        g = np.empty(self.n_params, dtype=np.float32) if want_grad else None
+        _ck(lib.maf_cnn_loss_grad(self._h, C.c_void_p(x_ptr), C.c_void_p(t_ptr), B, H, W, C.byref(loss),
+                                  g.ctypes.data_as(_FP) if want_grad else None))
+        return loss.value, g
+
+    def train_step(self, x_ptr: int, t_ptr: int, B: int, H: int, W: int, lr: float) -> float:
+        loss = C.c_float()
+        _ck(lib.maf_cnn_train_step(self._h, C.c_void_p(x_ptr), C.c_void_p(t_ptr), B, H, W, float(lr),
+                                   C.byref(loss)))
+        return loss.value
 
 
 class StochasticBatch:

@@ -1,0 +1,207 @@
+"""Learned warm start for the LBFGS minimiser.
+
+A small convolutional network (``magnumaf.ConvNet``, trained with the library's
+own CUDA kernels) maps an initial magnetisation and the material/field
+parameters to a proposal for the relaxed state; LBFGS then finishes from the
+proposal.  Plain LBFGS from the user's initial state stays both the fallback
+(a proposal with non-finite values or a higher energy than the initial state
+is discarded) and the judge: the minimiser's own stopping criteria decide when
+a state is relaxed, and the final energy and residual torque max|m x H|/Ms are
+reported for both starts.
+
+Workload (thin film, 2 nm cells, one layer): exchange A, interface DMI D
+(axis z), uniaxial anisotropy Ku (axis z), Zeeman field Bz along z, each drawn
+uniformly per sample from PARAM_RANGES; the initial state is a smooth random
+field (a few low Fourier modes).  Training pairs come from the GPU LBFGS run
+from those initial states.
+
+    python -m magnumaf.warmstart --n-train 512 --n-test 32 --mesh 64 64 --out result.json
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import time
+from typing import Dict, List
+
+import numpy as np
+
+import magnumaf as M
+
+PARAM_RANGES = {
+    "Ms": (5.0e5, 1.2e6),   # A/m
+    "A": (1.0e-11, 2.0e-11),  # J/m
+    "D": (1.0e-3, 4.0e-3),  # J/m^2
+    "Ku": (5.0e5, 1.2e6),   # J/m^3
+    "Bz": (0.0, 0.2),       # T
+}
+SCALE = {"Ms": 1e6, "A": 1e-11, "D": 1e-3, "Ku": 1e6, "Bz": 0.1}
+KEYS = ["Ms", "A", "D", "Ku", "Bz"]
+CIN = 3 + len(KEYS)
+DX = 2e-9
+
+
+def sample_params(rng) -> Dict[str, float]:
+    return {k: float(rng.uniform(*PARAM_RANGES[k])) for k in KEYS}
+
+
+def smooth_random_m(rng, nx: int, ny: int, kmax: int = 4) -> np.ndarray:
+    """(nx, ny, 1, 3) unit vectors from a sum of random low-order Fourier modes."""
+    x = np.arange(nx)[:, None] / nx
+    y = np.arange(ny)[None, :] / ny
+    m = np.zeros((nx, ny, 3))
+    for c in range(3):
+        f = np.zeros((nx, ny))
+        for kx in range(kmax + 1):
+            for ky in range(kmax + 1):
+                a, ph = rng.normal() / (1 + kx + ky), rng.uniform(0, 2 * math.pi)
+                f += a * np.cos(2 * math.pi * (kx * x + ky * y) + ph)
+        m[..., c] = f
+    m /= np.linalg.norm(m, axis=2, keepdims=True)
+    return m[:, :, None, :]
+
+
+def terms_for(p: Dict[str, float]) -> list:
+    return [M.ExchangeField(p["A"]), M.DmiField(p["D"]), M.UniaxialAnisotropyField(p["Ku"]),
+            M.ExternalField.uniform(0.0, 0.0, p["Bz"] / M.Constants.mu0)]
+
+
+def to_chw(m: np.ndarray) -> np.ndarray:
+    """(nx, ny, 1, 3) -> [3][ny][nx]"""
+    return np.ascontiguousarray(np.transpose(m[:, :, 0, :], (2, 1, 0)))
+
+
+def from_chw(y: np.ndarray) -> np.ndarray:
+    """[3][ny][nx] -> (nx, ny, 1, 3)"""
+    return np.ascontiguousarray(np.transpose(y, (2, 1, 0))[:, :, None, :])
+
+
+def features(m: np.ndarray, p: Dict[str, float]) -> np.ndarray:
+    """[CIN][ny][nx] float32: m, then one constant map per scaled parameter."""
+    mc = to_chw(m)
+    maps = [np.full(mc.shape[1:], p[k] / SCALE[k]) for k in KEYS]
+    return np.concatenate([mc, np.stack(maps)]).astype(np.float32)
+
+
+def relax(m0: np.ndarray, p: Dict[str, float], cnn: M.ConvNet = None, tol: float = 1e-6, maxiter: int = 1000):
+    """LBFGS relaxation from m0, or from the network's proposal when cnn is given.
+    Returns (m, info): info has E, iterations, fevals, torque = max|m x H|/Ms, seconds
+    (network included), used_proposal."""
+    import torch
+
+    nx, ny = m0.shape[0], m0.shape[1]
+    mesh = M.Mesh(nx, ny, 1, DX, DX, DX)
+    terms = terms_for(p)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    start = m0
+    used = False
+    if cnn is not None:
+        x = torch.from_numpy(features(m0, p)[None]).cuda()
+        y = torch.empty((1, 3, ny, nx), dtype=torch.float32, device="cuda")
+        cnn.forward(x.data_ptr(), 1, ny, nx, y.data_ptr())
+        prop = from_chw(y[0].double().cpu().numpy())
+        if np.all(np.isfinite(prop)):
+            s0 = M.State(mesh, p["Ms"], m0)
+            s1 = M.State(mesh, p["Ms"], prop)
+            e0 = sum(t.Energy_in_J(s0) for t in terms)
+            e1 = sum(t.Energy_in_J(s1) for t in terms)
+            if e1 <= e0:
+                start, used = prop, True
+    state = M.State(mesh, p["Ms"], start)
+    mini = M.LBFGS_Minimizer(terms, tol=tol, maxiter=maxiter)
+    E = mini.minimize(state)
+    torch.cuda.synchronize()
+    dt = time.perf_counter() - t0
+    st = mini.stats()
+    return np.asarray(state.m), {"E": E, "iterations": st["iterations"], "fevals": st["fevals"],
+                                 "torque": st["grad_max"] / p["Ms"], "seconds": dt, "used_proposal": used}
+
+
+def generate(n: int, nx: int, ny: int, seed: int, tol: float = 1e-6, maxiter: int = 1000):
+    """n samples (x [CIN][ny][nx], target [3][ny][nx], params, m0, info) relaxed by the GPU LBFGS."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        p = sample_params(rng)
+        m0 = smooth_random_m(rng, nx, ny)
+        m, info = relax(m0, p, None, tol, maxiter)
+        out.append((features(m0, p), to_chw(m).astype(np.float32), p, m0, info))
+    return out
+
+
+def train(cnn: M.ConvNet, samples, steps: int, batch: int, lr: float, seed: int = 0) -> List[float]:
+    """Adam on random minibatches; the dataset stays on the device.  Returns the losses."""
+    import torch
+
+    X = torch.from_numpy(np.stack([s[0] for s in samples])).cuda()
+    T = torch.from_numpy(np.stack([s[1] for s in samples])).cuda()
+    n, _, H, W = X.shape
+    g = torch.Generator(device="cpu").manual_seed(seed)
+    losses = []
+    for k in range(steps):
+        idx = torch.randint(0, n, (batch,), generator=g).cuda()
+        xb = X.index_select(0, idx).contiguous()
+        tb = T.index_select(0, idx).contiguous()
+        lr_k = lr * 0.5 * (1 + math.cos(math.pi * k / steps))
+        losses.append(cnn.train_step(xb.data_ptr(), tb.data_ptr(), batch, H, W, lr_k))
+    return losses
+
+
+def evaluate(cnn: M.ConvNet, tests, tol: float = 1e-6, maxiter: int = 1000) -> dict:
+    rows = []
+    for x, t, p, m0, _ in tests:
+        _, plain = relax(m0, p, None, tol, maxiter)
+        _, warm = relax(m0, p, cnn, tol, maxiter)
+        rows.append((plain, warm))
+    tp = sum(r[0]["seconds"] for r in rows)
+    tw = sum(r[1]["seconds"] for r in rows)
+    dE = [abs(r[1]["E"] - r[0]["E"]) / abs(r[0]["E"]) for r in rows]
+    return {
+        "samples": len(rows),
+        "plain_seconds": tp, "warm_seconds": tw, "speedup": tp / tw,
+        "plain_iterations": float(np.mean([r[0]["iterations"] for r in rows])),
+        "warm_iterations": float(np.mean([r[1]["iterations"] for r in rows])),
+        "proposals_used": int(sum(r[1]["used_proposal"] for r in rows)),
+        "rel_energy_diff_median": float(np.median(dE)), "rel_energy_diff_max": float(np.max(dE)),
+        "torque_plain_max": float(max(r[0]["torque"] for r in rows)),
+        "torque_warm_max": float(max(r[1]["torque"] for r in rows)),
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--n-train", type=int, default=512)
+    ap.add_argument("--n-test", type=int, default=32)
+    ap.add_argument("--mesh", type=int, nargs=2, default=[64, 64])
+    ap.add_argument("--steps", type=int, default=3000)
+    ap.add_argument("--batch", type=int, default=16)
+    ap.add_argument("--lr", type=float, default=2e-3)
+    ap.add_argument("--width", type=int, default=16)
+    ap.add_argument("--depth", type=int, default=5)
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--out", default=None)
+    a = ap.parse_args()
+    t0 = time.perf_counter()
+    train_set = generate(a.n_train, a.mesh[0], a.mesh[1], a.seed)
+    test_set = generate(a.n_test, a.mesh[0], a.mesh[1], a.seed + 10_000)
+    t1 = time.perf_counter()
+    cnn = M.ConvNet(CIN, a.width, a.depth, seed=a.seed)
+    losses = train(cnn, train_set, a.steps, a.batch, a.lr, a.seed)
+    t2 = time.perf_counter()
+    res = evaluate(cnn, test_set)
+    res.update({"mesh": a.mesh, "n_train": a.n_train, "train_steps": a.steps, "batch": a.batch,
+                "width": a.width, "depth": a.depth, "params": cnn.n_params,
+                "loss_first": float(np.mean(losses[:20])), "loss_last": float(np.mean(losses[-20:])),
+                "generate_seconds": t1 - t0, "train_seconds": t2 - t1})
+    line = json.dumps(res)
+    print(line, flush=True)
+    if a.out:
+        with open(a.out, "w") as f:
+            f.write(line + "\n")
+        np.save(a.out + ".params.npy", cnn.get_params())
+
+
+if __name__ == "__main__":
+    main()
