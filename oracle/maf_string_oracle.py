@@ -24,12 +24,16 @@ import maf_oracle as O
 
 
 class StringMethod:
-    def __init__(self, state, inputimages, n_interp, dt, llg):
+    def __init__(self, state, inputimages, n_interp, dt, llg, per_image_integrators=False):
         """state: template State (mesh, Ms / Ms_field); inputimages: list of
-        States or m arrays (nx, ny, nz, 3)."""
+        States or m arrays (nx, ny, nz, 3).  per_image_integrators: every image
+        gets its own copy of llg (its own controller state) instead of the
+        reference's one integrator shared in image order; the sharded string
+        method (magnumaf/string_sharded.py) uses that policy."""
         if not inputimages or len(inputimages) < 2:
             raise RuntimeError("StringMethod: at least two input images are needed")
         self.llg = llg
+        self.per_image = per_image_integrators
         self.n_interp = int(n_interp)
         self.dt = float(dt)
         inputs = []
@@ -55,6 +59,8 @@ class StringMethod:
             self.images.append(img)
         self._normalize()
         self.E = []
+        import copy
+        self.llgs = [copy.deepcopy(llg) for _ in range(self.n_interp)] if per_image_integrators else None
 
     def _calc_x(self, ms):
         self.x = [0.0]
@@ -75,10 +81,11 @@ class StringMethod:
             img.m = O.normalize(img.m)
 
     def integrate(self):
-        for img in self.images:
+        for i, img in enumerate(self.images):
+            llg = self.llgs[i] if self.per_image else self.llg
             t0 = img.t
             while img.t < t0 + self.dt:
-                self.llg.step(img)
+                llg.step(img)
 
     def lin_interpolate(self):
         tmp = [img.copy() for img in self.images]
