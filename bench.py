@@ -212,8 +212,11 @@ def run_reference(args):
         "metric": METRIC, "value": value, "unit": "evals/s", "impl": "reference", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
-        "config": {"workload": "H_eff demag+exchange+cubic+Zeeman, 1024x1024x16 cells of 3 nm",
-                   "cells": NX * NY * NZ, "sample_layers": nzs},
+        "config": {"workload": "H_eff demag+exchange+cubic+Zeeman, %dx%dx%d cells of 3 nm (FP32-field form)"
+                               % (NX, NY, NZ),
+                   "cells": NX * NY * NZ, "parallelism": "replicas x1",
+                   "l2": "inputs larger than L2 (m 201 MB, spectra 403-806 MB per pass)",
+                   "sample_layers": nzs},
         "cpu_baseline": {"value": value, "unit": "evals/s", "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": "evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
