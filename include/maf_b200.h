@@ -152,6 +152,12 @@ int maf_llg_heff_f32(maf_llg l, maf_state s, float* H_host);
 /* Effective field from a device-resident m (float* for FP32-field states, double* for FP64 states)
  * into a device-resident H of the same type, on the state's stream; no synchronisation. */
 int maf_llg_heff_device(maf_llg l, maf_state s, const void* m_dev, void* H_dev);
+/* LLGIntegrator::fheff over n host magnetisations in a row (each normalised as by maf_state_set_m):
+ * m_host[i] double [3][N] -> H_host[i] (float [3][N] for FP32-field states, double for FP64).  The
+ * copy of m[i+1] in, the evaluation of m[i] and the copy of H[i-1] out overlap on three streams (use
+ * pinned host memory for full link bandwidth).  The state keeps the last m.  No counterpart in the
+ * reference beyond calling H_in_Apm n times. */
+int maf_llg_heff_pipeline(maf_llg l, maf_state s, const double* const* m_host, void* const* H_host, int n);
 /* maf_llg_heff_device with a CUDA event after every pass kernel: synchronises and
  * returns each pass's duration in ms (the instrumentation LLGIntegrator::time_heff,
  * llg_integrator.cpp:11-16, and the per-term timers of field_term.hpp:49-86 provide,

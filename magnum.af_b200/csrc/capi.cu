@@ -181,11 +181,30 @@ int mafb::capi_run(const std::function<void()>& f) {
 // ---------------------------------------------------------------------------
 // handle structs
 // ---------------------------------------------------------------------------
+// Buffers and streams of the pipelined evaluation (maf_llg_heff_pipeline).
+struct HeffPipe {
+    DevBuf m[2], h[2], m32;
+    cudaStream_t up = nullptr, down = nullptr;
+    cudaEvent_t up_done[2] = {}, comp_done[2] = {}, down_done[2] = {};
+    ~HeffPipe() {
+        for (int b = 0; b < 2; ++b) {
+            if (up_done[b]) cudaEventDestroy(up_done[b]);
+            if (comp_done[b]) cudaEventDestroy(comp_done[b]);
+            if (down_done[b]) cudaEventDestroy(down_done[b]);
+        }
+        if (up) cudaStreamDestroy(up);
+        if (down) cudaStreamDestroy(down);
+    }
+};
+
 struct maf_state_s {
     StateD s;
     DevBuf scratch;  // reductions
     bool m32_valid = false;
+    std::unique_ptr<HeffPipe> pipe;
     ~maf_state_s() {
+        if (s.stream) cudaStreamSynchronize(s.stream);
+        pipe.reset();
         if (s.own_stream && s.stream) cudaStreamDestroy(s.stream);
     }
 };
@@ -1303,6 +1322,73 @@ int maf_llg_heff_f32(maf_llg l, maf_state s, float* H) {
         check_llg_state(l, s);
         check(H, "NULL argument");
         H_to_host(s, raw_terms(l->terms), nullptr, H, g_tmp);
+    });
+}
+
+// H_eff of n magnetisations in a row through pinned host memory: the copy of
+// m[i+1] to the device, the evaluation of m[i] and the copy of H[i-1] to the
+// host run on three streams with double-buffered device buffers, so the host
+// link carries both directions while the field is computed.
+int maf_llg_heff_pipeline(maf_llg l, maf_state s, const double* const* m_host, void* const* H_host, int n) {
+    return guarded([&] {
+        check_llg_state(l, s);
+        check(n >= 0 && (n == 0 || (m_host && H_host)), "maf_llg_heff_pipeline: bad argument");
+        StateD& st = s->s;
+        const int64_t N = st.md.N(), n3 = 3 * N;
+        const bool f32 = st.precision == PREC_FP32_FIELD;
+        const size_t hsz = (f32 ? sizeof(float) : sizeof(double)) * n3;
+        if (!s->pipe) {
+            auto p = std::make_unique<HeffPipe>();
+            MAF_CUDA(cudaStreamCreateWithFlags(&p->up, cudaStreamNonBlocking));
+            MAF_CUDA(cudaStreamCreateWithFlags(&p->down, cudaStreamNonBlocking));
+            for (int b = 0; b < 2; ++b) {
+                MAF_CUDA(cudaEventCreateWithFlags(&p->up_done[b], cudaEventDisableTiming));
+                MAF_CUDA(cudaEventCreateWithFlags(&p->comp_done[b], cudaEventDisableTiming));
+                MAF_CUDA(cudaEventCreateWithFlags(&p->down_done[b], cudaEventDisableTiming));
+                p->m[b].alloc(sizeof(double) * n3);
+                p->h[b].alloc(hsz);
+            }
+            if (f32) p->m32.alloc(sizeof(float) * n3);
+            s->pipe = std::move(p);
+        }
+        HeffPipe& p = *s->pipe;
+        const auto terms = raw_terms(l->terms);
+        MAF_CUDA(cudaStreamSynchronize(st.stream));
+        for (int i = 0; i < n; ++i) {
+            const int b = i & 1;
+            check(m_host[i] && H_host[i], "maf_llg_heff_pipeline: NULL buffer");
+            // host -> device, once the evaluation two steps back has released m[b]
+            MAF_CUDA(cudaStreamWaitEvent(p.up, p.comp_done[b], 0));
+            MAF_CUDA(cudaMemcpyAsync(p.m[b].p, m_host[i], sizeof(double) * n3, cudaMemcpyHostToDevice, p.up));
+            MAF_CUDA(cudaEventRecord(p.up_done[b], p.up));
+            // normalise (as maf_state_set_m) and evaluate once H[b] has gone to the host
+            MAF_CUDA(cudaStreamWaitEvent(st.stream, p.up_done[b], 0));
+            MAF_CUDA(cudaStreamWaitEvent(st.stream, p.down_done[b], 0));
+            normalize_m(p.m[b].as<double>(), N, 2, nullptr, st.stream);
+            EpilogueArgs ep;
+            ep.kind = EPI_H;
+            ep.out = p.h[b].p;
+            if (f32) {
+                stage_m32(p.m[b].as<double>(), p.m32.as<float>(), n3, st.stream);
+                eval_terms<float>(terms, st.md, p.m32.as<float>(), st.msinfo(), ep, st.stream, s->scratch, nullptr);
+            } else {
+                eval_terms<double>(terms, st.md, p.m[b].as<double>(), st.msinfo(), ep, st.stream, s->scratch,
+                                   nullptr);
+            }
+            MAF_CUDA(cudaEventRecord(p.comp_done[b], st.stream));
+            // device -> host
+            MAF_CUDA(cudaStreamWaitEvent(p.down, p.comp_done[b], 0));
+            MAF_CUDA(cudaMemcpyAsync(H_host[i], p.h[b].p, hsz, cudaMemcpyDeviceToHost, p.down));
+            MAF_CUDA(cudaEventRecord(p.down_done[b], p.down));
+        }
+        if (n > 0) {  // the state keeps the last magnetisation, as after maf_state_set_m
+            MAF_CUDA(cudaMemcpyAsync(st.m64.p, p.m[(n - 1) & 1].p, sizeof(double) * n3, cudaMemcpyDeviceToDevice,
+                                     st.stream));
+            s->m32_valid = false;
+        }
+        MAF_CUDA(cudaStreamSynchronize(p.down));
+        MAF_CUDA(cudaStreamSynchronize(p.up));
+        MAF_CUDA(cudaStreamSynchronize(st.stream));
     });
 }
 

@@ -83,6 +83,7 @@ _SIGS = {
     "maf_llg_heff": (_I, [_P, _P, _DP]),
     "maf_llg_heff_f32": (_I, [_P, _P, _FP]),
     "maf_llg_heff_device": (_I, [_P, _P, _P, _P]),
+    "maf_llg_heff_pipeline": (_I, [_P, _P, C.POINTER(_P), C.POINTER(_P), _I]),
     "maf_llg_heff_device_profile": (_I, [_P, _P, _P, _P, _DP, _I, C.POINTER(_I)]),
     "maf_llg_pass_name": (_I, [_P, _P, _I, C.c_char_p, _I]),
     "maf_llg_dmdt": (_I, [_P, _P, _DP]),
@@ -562,6 +563,17 @@ class LLGIntegrator:
     def heff_device(self, state: State, m_dev_ptr: int, H_dev_ptr: int):
         """Field of a device-resident m into a device-resident H (no sync)."""
         _ck(lib.maf_llg_heff_device(self._h, state._h, C.c_void_p(m_dev_ptr), C.c_void_p(H_dev_ptr)))
+
+    def heff_pipeline(self, state: State, m_host_ptrs, H_host_ptrs):
+        """Fields of several host magnetisations in a row, host copies overlapped
+        with the evaluations (pass pinned buffers): m_host_ptrs[i] -> H_host_ptrs[i]
+        (addresses of double [3][N] inputs and of float/double [3][N] outputs)."""
+        n = len(m_host_ptrs)
+        if len(H_host_ptrs) != n:
+            raise ValueError("as many outputs as inputs")
+        mp = (_P * max(n, 1))(*[C.c_void_p(p) for p in m_host_ptrs])
+        hp = (_P * max(n, 1))(*[C.c_void_p(p) for p in H_host_ptrs])
+        _ck(lib.maf_llg_heff_pipeline(self._h, state._h, mp, hp, n))
 
     def heff_device_profile(self, state: State, m_dev_ptr: int, H_dev_ptr: int):
         """One field evaluation with per-pass CUDA-event timing: [(name, ms), ...]."""

@@ -1,0 +1,34 @@
+"""maf_llg_heff_pipeline (overlapped host copies) against one maf_state_set_m +
+maf_llg_heff(_f32) call per input: bit-identical fields, the state left at the
+last input."""
+import numpy as np
+import pytest
+
+from helpers import random_m
+
+M = pytest.importorskip("magnumaf")
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("precision", ["fp32_field", "fp64"])
+def test_pipeline_equals_single_calls(precision):
+    shape = (64, 48, 4)
+    mesh = M.Mesh(*shape, 3e-9, 3e-9, 3e-9)
+    terms = [M.DemagField(mesh), M.ExchangeField(1.3e-11), M.CubicAnisotropyField(-1e4),
+             M.ExternalField.uniform(1e4, -2e4, 3e4)]
+    llg = M.LLGIntegrator(0.01, terms, "DP45")
+    ms = [random_m(shape, 50 + i) for i in range(5)]
+    s = M.State(mesh, 8.6e5, ms[0], precision=precision)
+    f32 = precision == "fp32_field"
+    ref = []
+    for m in ms:
+        s.m = m
+        ref.append(llg.H_in_Apm_f32(s) if f32 else llg.H_in_Apm(s))
+    # inputs/outputs in the library's [3][nz][ny][nx] layout (Fortran order of (nx,ny,nz,3))
+    ins = [np.asfortranarray(m).ravel(order="F").copy() for m in ms]
+    outs = [np.empty(3 * np.prod(shape), dtype=np.float32 if f32 else np.float64) for _ in ms]
+    llg.heff_pipeline(s, [a.ctypes.data for a in ins], [o.ctypes.data for o in outs])
+    for o, r in zip(outs, ref):
+        assert np.array_equal(o, np.asarray(r).ravel(order="F"))
+    np.testing.assert_array_equal(np.asarray(s.m), np.asarray(M.State(mesh, 8.6e5, ms[-1]).m))
