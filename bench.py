@@ -288,6 +288,10 @@ def run_ours(args):
             ms = float(t.item())
         return ms
 
+    tune = None
+    if not args.no_autotune:  # kernel variants per pass, measured on this mesh (FP32-field form)
+        tune = llg.autotune(s32, reps=3)
+
     f32 = lambda: llg.heff_device(s32, m32_dev.data_ptr(), H32.data_ptr())
     f64 = lambda: llg.heff_device(s64, m64_dev.data_ptr(), H64.data_ptr())
 
@@ -370,7 +374,8 @@ def run_ours(args):
         "config": {"workload": "H_eff demag+exchange+cubic+Zeeman, %dx%dx%d cells of 3 nm (FP32-field form)"
                                % (NX, NY, NZ),
                    "cells": NX * NY * NZ, "parallelism": "replicas x%d" % world,
-                   "l2": "inputs larger than L2 (m 201 MB, spectra 403-806 MB per pass)"},
+                   "l2": "inputs larger than L2 (m 201 MB, spectra 403-806 MB per pass)",
+                   "tune": None if tune is None else {k: tune[k] for k in ("cols_wide", "convz_reg", "xinv_run")}},
         "fp64_form": {"value": world * args.steps / (ms64 * 1e-3), "ms_per_step": ms64 / args.steps,
                       "fp32_speedup": ms64 / ms32},
         "rel_err_fp32_vs_fp64": {"l2": rel_err, "max": rel_max},
@@ -408,6 +413,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default kernel variants")
     ap.add_argument("--mesh", type=int, nargs=3, default=None, metavar=("NX", "NY", "NZ"),
                     help="smaller mesh for profiling captures (the reported metric is defined at 1024 1024 16)")
     args = ap.parse_args()

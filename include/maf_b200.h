@@ -158,6 +158,17 @@ int maf_llg_heff_device(maf_llg l, maf_state s, const void* m_dev, void* H_dev);
  * pinned host memory for full link bandwidth).  The state keeps the last m.  No counterpart in the
  * reference beyond calling H_in_Apm n times. */
 int maf_llg_heff_pipeline(maf_llg l, maf_state s, const double* const* m_host, void* const* H_host, int n);
+/* Autotuner (no counterpart in the reference): the compile-time passes have two kernel variants each --
+ * y-pass column tile (choices[0]: 0 default, 1 doubled), z convolution (choices[1]: 1 transforms in
+ * registers, 0 shared-memory stages), x-inverse epilogue run length (choices[2]: 2 or 4 cells, 0 = the
+ * build's default).  Times both configurations on this state's mesh and precision (one warm-up, then the
+ * mean of reps evaluations, CUDA events between passes), keeps the faster variant per pass in the
+ * DemagField (shared by every integrator that holds it) and returns the choices; pass_ms (optional, 10
+ * values) receives the per-pass times of the two configurations.  Every variant computes the same field
+ * up to rounding. */
+int maf_llg_autotune(maf_llg l, maf_state s, int reps, int choices[3], double* pass_ms);
+int maf_term_demag_get_tune(maf_term t, int choices[3]);
+int maf_term_demag_set_tune(maf_term t, const int choices[3]);
 /* maf_llg_heff_device with a CUDA event after every pass kernel: synchronises and
  * returns each pass's duration in ms (the instrumentation LLGIntegrator::time_heff,
  * llg_integrator.cpp:11-16, and the per-term timers of field_term.hpp:49-86 provide,

@@ -1436,6 +1436,91 @@ int maf_llg_heff_device_profile(maf_llg l, maf_state s, const void* m_dev, void*
     });
 }
 
+// Autotuner: times both kernel configurations of every tunable pass on this
+// state's mesh and precision (one warm-up, then the mean of `reps` evaluations
+// with CUDA events between the passes) and keeps the faster variant per pass.
+int maf_llg_autotune(maf_llg l, maf_state s, int reps, int choices[3], double* pass_ms) {
+    return guarded([&] {
+        check_llg_state(l, s);
+        check(choices && reps > 0, "maf_llg_autotune: bad argument");
+        Demag* dm = nullptr;
+        for (auto& t : l->terms)
+            if (t->kind == TK_DEMAG) dm = t->demag.get();
+        TuneChoice best;
+        if (dm) {
+            StateD& st = s->s;
+            const bool f32 = st.precision == PREC_FP32_FIELD;
+            const int64_t n3 = 3 * st.md.N();
+            g_tmp.ensure((f32 ? sizeof(float) : sizeof(double)) * n3);
+            if (f32) ensure_m32(s);
+            const auto terms = raw_terms(l->terms);
+            auto run = [&](const TuneChoice& c) {
+                dm->tune = c;
+                std::vector<double> acc;
+                for (int r = -1; r < reps; ++r) {  // r = -1: warm-up
+                    EpilogueArgs ep;
+                    ep.kind = EPI_H;
+                    ep.out = g_tmp.p;
+                    PassMarks marks;
+                    if (f32)
+                        eval_terms<float>(terms, st.md, st.m32.as<float>(), st.msinfo(), ep, st.stream, s->scratch,
+                                          nullptr, &marks);
+                    else
+                        eval_terms<double>(terms, st.md, st.m64.as<double>(), st.msinfo(), ep, st.stream, s->scratch,
+                                           nullptr, &marks);
+                    MAF_CUDA(cudaStreamSynchronize(st.stream));
+                    if (r < 0) continue;
+                    acc.resize(marks.ev.size() - 1, 0.0);
+                    for (size_t i = 1; i < marks.ev.size(); ++i) {
+                        float ms = 0;
+                        MAF_CUDA(cudaEventElapsedTime(&ms, marks.ev[i - 1], marks.ev[i]));
+                        acc[i - 1] += ms / reps;
+                    }
+                }
+                return acc;
+            };
+            const TuneChoice A{0, 1, 2}, B{1, 0, 4};
+            const std::vector<double> ta = run(A), tb = run(B);
+            if (st.md.nz > 1 && ta.size() == 5 && tb.size() == 5) {
+                best.cols_wide = tb[1] + tb[3] < ta[1] + ta[3] ? 1 : 0;
+                best.convz_reg = ta[2] <= tb[2] ? 1 : 0;
+                best.xinv_run = ta[4] <= tb[4] ? 2 : 4;
+            } else if (ta.size() == 3 && tb.size() == 3) {
+                best.xinv_run = ta[2] <= tb[2] ? 2 : 4;
+            }
+            dm->tune = best;
+            if (pass_ms)
+                for (size_t i = 0; i < 5; ++i) {
+                    pass_ms[i] = i < ta.size() ? ta[i] : 0.0;
+                    pass_ms[5 + i] = i < tb.size() ? tb[i] : 0.0;
+                }
+        }
+        choices[0] = best.cols_wide;
+        choices[1] = best.convz_reg;
+        choices[2] = best.xinv_run;
+    });
+}
+
+int maf_term_demag_get_tune(maf_term t, int choices[3]) {
+    return guarded([&] {
+        check(t && choices && t->t->kind == TK_DEMAG, "maf_term_demag_get_tune: not a DemagField");
+        const TuneChoice& c = t->t->demag->tune;
+        choices[0] = c.cols_wide;
+        choices[1] = c.convz_reg;
+        choices[2] = c.xinv_run;
+    });
+}
+
+int maf_term_demag_set_tune(maf_term t, const int choices[3]) {
+    return guarded([&] {
+        check(t && choices && t->t->kind == TK_DEMAG, "maf_term_demag_set_tune: not a DemagField");
+        check((choices[0] == 0 || choices[0] == 1) && (choices[1] == 0 || choices[1] == 1) &&
+                  (choices[2] == 0 || choices[2] == 2 || choices[2] == 4),
+              "maf_term_demag_set_tune: choices are {0|1, 0|1, 0|2|4}");
+        t->t->demag->tune = TuneChoice{choices[0], choices[1], choices[2]};
+    });
+}
+
 int maf_llg_pass_name(maf_llg l, maf_state s, int index, char* buf, int buflen) {
     return guarded([&] {
         check_llg_state(l, s);

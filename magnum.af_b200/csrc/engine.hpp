@@ -122,10 +122,21 @@ struct MsInfo {
     const float* field32 = nullptr;
 };
 
+// Kernel variants of the compile-time passes, chosen per demag plan (defaults,
+// or measured by maf_llg_autotune): y-pass column tile doubled, z convolution
+// with register transforms (nz <= 16) or shared-memory stages, x-inverse
+// epilogue on runs of 2 or 4 cells (0: the build's default).
+struct TuneChoice {
+    int cols_wide = 0;
+    int convz_reg = 1;
+    int xinv_run = 0;
+};
+
 // Demag plan: the symmetry-reduced real spectral Newell tensor and the
 // spectral work buffers for one mesh.
 class Demag {
   public:
+    TuneChoice tune;
     explicit Demag(const MeshDims& md, cudaStream_t st);
     const MeshDims& mesh() const { return md_; }
     int Px() const { return 2 * md_.nx; }

@@ -420,8 +420,9 @@ static void launch_xfwd(const R* in, int n_in, int64_t rows, int64_t rows_pc, co
 
 template <typename R, int DIR>
 static void launch_cols(const cplx_t<R>* in, cplx_t<R>* out, int L, int n_in, int n_out, int ncols, int64_t in_si,
-                        int64_t out_si, int64_t in_sbat, int64_t out_sbat, int nbat, Twiddles& tw, cudaStream_t st) {
-    if (ct_cols<R, DIR>(in, out, L, n_in, n_out, ncols, in_si, out_si, in_sbat, out_sbat, nbat, tw, st)) return;
+                        int64_t out_si, int64_t in_sbat, int64_t out_sbat, int nbat, Twiddles& tw,
+                        const TuneChoice& tc, cudaStream_t st) {
+    if (ct_cols<R, DIR>(in, out, L, n_in, n_out, ncols, in_si, out_si, in_sbat, out_sbat, nbat, tw, tc, st)) return;
     const bool f64 = sizeof(R) == 8;
     FFTPlan plan = make_fft_plan(L, tw.get(L, f64));
     int nb = pick_nb(L, tile_target<R>(), ncols, 32);
@@ -473,10 +474,11 @@ void Demag::build_tensor(cudaStream_t st) {
         launch_xfwd<double>(real.as<double>(), Px_, (int64_t)Py_ * Pz_, (int64_t)Py_ * Pz_, nullptr, 1.0,
                             spec.as<double2>(), pitch_, Px_, tw_, st);
         launch_cols<double, -1>(spec.as<double2>(), spec.as<double2>(), Py_, Py_, Py_, nxh(), pitch_, pitch_,
-                                (int64_t)Py_ * pitch_, (int64_t)Py_ * pitch_, Pz_, tw_, st);
+                                (int64_t)Py_ * pitch_, (int64_t)Py_ * pitch_, Pz_, tw_, tune, st);
         if (Pz_ > 1)
             launch_cols<double, -1>(spec.as<double2>(), spec.as<double2>(), Pz_, Pz_, Pz_, nxh(),
-                                    (int64_t)Py_ * pitch_, (int64_t)Py_ * pitch_, pitch_, pitch_, Py_, tw_, st);
+                                    (int64_t)Py_ * pitch_, (int64_t)Py_ * pitch_, pitch_, pitch_, Py_, tw_, tune,
+                                    st);
         const int64_t total = cstride;
         const int64_t blocks = std::min<int64_t>(ceil_div(total, 256), 148LL * 16);
         k_reduce_tensor<<<(unsigned)blocks, 256, 0, st>>>(spec.as<double2>(), Nred64_.as<double>() + ci * cstride,
@@ -550,10 +552,10 @@ template <typename R> void Demag::forward_conv(const R* m, const MsInfo& ms, cud
         C* s2 = S2<R>();
         // pass 2: y forward, S1 [3*nz][ny][pitch] -> S2 [3*nz][Py][pitch]
         launch_cols<R, -1>(s1, s2, Py(), ny, Py(), nxh(), pitch_, pitch_, (int64_t)ny * pitch_,
-                           (int64_t)Py() * pitch_, 3 * nz, tw_, st);
+                           (int64_t)Py() * pitch_, 3 * nz, tw_, tune, st);
         if (marks) marks->mark(st, "y_fwd");
         // pass 3: z forward . tensor . z inverse, in place on S2
-        if (!ct_convz<R>(s2, Nr, nz, ny, nxh(), pitch_, tw_, st)) {
+        if (!ct_convz<R>(s2, Nr, nz, ny, nxh(), pitch_, tw_, tune, st)) {
             const int L = Pz();
             FFTPlan fp = make_fft_plan(L, tw_.get(L, f64));
             FFTPlan ip = fp;
@@ -575,7 +577,7 @@ template <typename R> void Demag::forward_conv(const R* m, const MsInfo& ms, cud
         if (marks) marks->mark(st, "z_conv");
         // pass 4: y inverse, S2 -> S1, keep ky rows [0, ny)
         launch_cols<R, 1>(s2, s1, Py(), Py(), ny, nxh(), pitch_, pitch_, (int64_t)Py() * pitch_,
-                          (int64_t)ny * pitch_, 3 * nz, tw_, st);
+                          (int64_t)ny * pitch_, 3 * nz, tw_, tune, st);
         if (marks) marks->mark(st, "y_inv");
     } else {
         // pass 2 (2-D): y forward . tensor . y inverse, in place on S1
@@ -612,7 +614,7 @@ void Demag::inverse_x_epilogue(const R* m, const MsInfo& ms, const TermList& tl,
     const int Lc = md_.nx;
     {
         const R scale = (R)(1.0 / ((double)Px() * Py() * Pz()));
-        if (ct_xinv<R>(S1<R>(), pitch_, Px(), tw_, md_.geom(), scale, m, ms, tl, ep, st, nblocks_out)) {
+        if (ct_xinv<R>(S1<R>(), pitch_, Px(), tw_, md_.geom(), scale, m, ms, tl, ep, tune, st, nblocks_out)) {
             if (marks) marks->mark(st, "x_inv_local");
             return;
         }

@@ -313,8 +313,8 @@ __global__ void __launch_bounds__(NT) k_convy_ct(cplx_t<R>* S, const R* __restri
 }
 
 // --------------------------------------------------- x inverse + epilogue
-template <typename R, int EPI, int LC, int NBR, int NT>
-__global__ void __launch_bounds__(NT, (kMinBlocks<R, NT, MAF_XINV_THREADS, 192>)) k_xinv_ct(const cplx_t<R>* __restrict__ S1, int pitch,
+template <typename R, int EPI, int LC, int NBR, int NT, int RN>
+__global__ void __launch_bounds__(NT, (kMinBlocks<R, NT, (RN == 2 ? MAF_XINV_THREADS : 384), 192>)) k_xinv_ct(const cplx_t<R>* __restrict__ S1, int pitch,
                                                 const cplx_t<R>* __restrict__ tw, const cplx_t<R>* __restrict__ twP,
                                                 Geom g, R scale, const R* __restrict__ m, MsInfo ms, TermList tl,
                                                 EpilogueArgs ep, int run4) {
@@ -342,7 +342,6 @@ __global__ void __launch_bounds__(NT, (kMinBlocks<R, NT, MAF_XINV_THREADS, 192>)
     ct_fft_in<R, 1, false, LC, NC, NT>(s, SB, tw, ld, typename CtPlan<LC>::T());
     if constexpr (EPI == EPI_H || EPI == EPI_LLG) {
         if (run4) {
-            constexpr int RN = kRunCells;  // cells per run (2 or 4)
             const int runs = g.nx / RN;
             for (int idx = threadIdx.x; idx < NBR * runs; idx += NT) {
                 const int b = idx / runs;
@@ -482,10 +481,10 @@ static void xfwd_L(const R* in, int n_in, int64_t rows, int64_t rows_pc, const R
     MAF_LAUNCH_CHECK();
 }
 
-template <typename R, int DIR, int L>
+template <typename R, int DIR, int L, int TILE>
 static void cols_L(const cplx_t<R>* in, cplx_t<R>* out, int n_in, int n_out, int ncols, int64_t in_si, int64_t out_si,
                    int64_t in_sbat, int64_t out_sbat, int nbat, const void* tw, cudaStream_t st) {
-    constexpr int NB = pow2floor(cmin(32, cmax(1, kTileCols<R> / L)));
+    constexpr int NB = pow2floor(cmin(32, cmax(1, TILE / L)));
     constexpr int NT = L * NB / kE;
     static_assert(NT <= 1024, "CTA size");
     const size_t smem = sizeof(cplx_t<R>) * (size_t)NB * ((L - 1) + ((L - 1) >> 4) + 1);
@@ -497,13 +496,13 @@ static void cols_L(const cplx_t<R>* in, cplx_t<R>* out, int n_in, int n_out, int
     MAF_LAUNCH_CHECK();
 }
 
-template <typename R, int L>
+template <typename R, int L, bool REG>
 static void convz_L(cplx_t<R>* S, const R* Nred, int nz, int ny, int nxh, int pitch, const void* tw, cudaStream_t st) {
     constexpr int NB = pow2floor(cmin(32, cmax(1, kTileC<R> / (6 * L))));
     constexpr int NT = L * 6 * NB / kE;
     static_assert(NT <= kMaxFftThreads, "CTA size");
     const size_t smem = sizeof(cplx_t<R>) * (size_t)6 * NB * ((L - 1) + ((L - 1) >> 4) + 1);
-    if constexpr (L <= 32) {
+    if constexpr (L <= 32 && REG) {
         // transforms in registers: one thread per column, NB columns of kx
         constexpr int NBR = sizeof(R) == 4 ? 32 : 16;
         constexpr size_t smem_r = sizeof(cplx_t<R>) * (size_t)L * 6 * NBR;
@@ -532,7 +531,7 @@ static void convy_L(cplx_t<R>* S, const R* Nred, int ny, int nxh, int pitch, con
     MAF_LAUNCH_CHECK();
 }
 
-template <typename R, int LC>
+template <typename R, int LC, int RN>
 static void xinv_L(const cplx_t<R>* S1, int pitch, const void* tw, const void* twP, const Geom& g, R scale, const R* m,
                    const MsInfo& ms, const TermList& tl_in, const EpilogueArgs& ep, cudaStream_t st, int* nblocks) {
     // half the column-pass tile: the epilogue's register demand allows one
@@ -553,25 +552,25 @@ static void xinv_L(const cplx_t<R>* S1, int pitch, const void* tw, const void* t
     const auto* tp = static_cast<const cplx_t<R>*>(twP);
     switch (ep.kind) {
         case EPI_H: {
-            auto k = k_xinv_ct<R, EPI_H, LC, NBR, NT>;
+            auto k = k_xinv_ct<R, EPI_H, LC, NBR, NT, RN>;
             ct_smem(k, smem);
             k<<<blocks, NT, smem, st>>>(S1, pitch, t, tp, g, scale, m, ms, tl, ep, run4);
             break;
         }
         case EPI_LLG: {
-            auto k = k_xinv_ct<R, EPI_LLG, LC, NBR, NT>;
+            auto k = k_xinv_ct<R, EPI_LLG, LC, NBR, NT, RN>;
             ct_smem(k, smem);
             k<<<blocks, NT, smem, st>>>(S1, pitch, t, tp, g, scale, m, ms, tl, ep, run4);
             break;
         }
         case EPI_EGRAD: {
-            auto k = k_xinv_ct<R, EPI_EGRAD, LC, NBR, NT>;
+            auto k = k_xinv_ct<R, EPI_EGRAD, LC, NBR, NT, RN>;
             ct_smem(k, smem);
             k<<<blocks, NT, smem, st>>>(S1, pitch, t, tp, g, scale, m, ms, tl, ep, run4);
             break;
         }
         default: {
-            auto k = k_xinv_ct<R, EPI_EDENS, LC, NBR, NT>;
+            auto k = k_xinv_ct<R, EPI_EDENS, LC, NBR, NT, RN>;
             ct_smem(k, smem);
             k<<<blocks, NT, smem, st>>>(S1, pitch, t, tp, g, scale, m, ms, tl, ep, run4);
             break;
@@ -606,18 +605,33 @@ bool ct_xfwd(const R* in, int n_in, int64_t rows, int64_t rows_pc, const R* msf,
 
 template <typename R, int DIR>
 bool ct_cols(const cplx_t<R>* in, cplx_t<R>* out, int L, int n_in, int n_out, int ncols, int64_t in_si, int64_t out_si,
-             int64_t in_sbat, int64_t out_sbat, int nbat, Twiddles& tw, cudaStream_t st) {
+             int64_t in_sbat, int64_t out_sbat, int nbat, Twiddles& tw, const TuneChoice& tc, cudaStream_t st) {
     const bool f64 = sizeof(R) == 8;
-#define X(N) cols_L<R, DIR, N>(in, out, n_in, n_out, ncols, in_si, out_si, in_sbat, out_sbat, nbat, tw.get(N, f64), st)
+#define X(N)                                                                                                    \
+    do {                                                                                                        \
+        if (tc.cols_wide)                                                                                       \
+            cols_L<R, DIR, N, 2 * kTileCols<R>>(in, out, n_in, n_out, ncols, in_si, out_si, in_sbat, out_sbat,   \
+                                                nbat, tw.get(N, f64), st);                                      \
+        else                                                                                                    \
+            cols_L<R, DIR, N, kTileCols<R>>(in, out, n_in, n_out, ncols, in_si, out_si, in_sbat, out_sbat, nbat, \
+                                            tw.get(N, f64), st);                                                \
+    } while (0)
     MAF_CT_SWITCH(L, X)
 #undef X
 }
 
 template <typename R>
-bool ct_convz(cplx_t<R>* S, const R* Nred, int nz, int ny, int nxh, int pitch, Twiddles& tw, cudaStream_t st) {
+bool ct_convz(cplx_t<R>* S, const R* Nred, int nz, int ny, int nxh, int pitch, Twiddles& tw, const TuneChoice& tc,
+              cudaStream_t st) {
     const bool f64 = sizeof(R) == 8;
     const int L = 2 * nz;
-#define X(N) convz_L<R, N>(S, Nred, nz, ny, nxh, pitch, tw.get(N, f64), st)
+#define X(N)                                                                 \
+    do {                                                                     \
+        if (tc.convz_reg)                                                    \
+            convz_L<R, N, true>(S, Nred, nz, ny, nxh, pitch, tw.get(N, f64), st);  \
+        else                                                                 \
+            convz_L<R, N, false>(S, Nred, nz, ny, nxh, pitch, tw.get(N, f64), st); \
+    } while (0)
     switch (L) {
         case 8: X(8); return true;
         case 16: X(16); return true;
@@ -649,10 +663,18 @@ bool ct_convy(cplx_t<R>* S, const R* Nred, int ny, int nxh, int pitch, Twiddles&
 
 template <typename R>
 bool ct_xinv(const cplx_t<R>* S1, int pitch, int Px, Twiddles& tw, const Geom& g, R scale, const R* m,
-             const MsInfo& ms, const TermList& tl, const EpilogueArgs& ep, cudaStream_t st, int* nblocks) {
+             const MsInfo& ms, const TermList& tl, const EpilogueArgs& ep, const TuneChoice& tc, cudaStream_t st,
+             int* nblocks) {
     const int LC = Px / 2;
     const bool f64 = sizeof(R) == 8;
-#define X(N) xinv_L<R, N>(S1, pitch, tw.get(N, f64), tw.get(Px, f64), g, scale, m, ms, tl, ep, st, nblocks)
+    const int run = tc.xinv_run ? tc.xinv_run : kRunCells;
+#define X(N)                                                                                                    \
+    do {                                                                                                        \
+        if (run == 4)                                                                                           \
+            xinv_L<R, N, 4>(S1, pitch, tw.get(N, f64), tw.get(Px, f64), g, scale, m, ms, tl, ep, st, nblocks);  \
+        else                                                                                                    \
+            xinv_L<R, N, 2>(S1, pitch, tw.get(N, f64), tw.get(Px, f64), g, scale, m, ms, tl, ep, st, nblocks);  \
+    } while (0)
     switch (LC) {
         case 16: X(16); return true;
         case 32: X(32); return true;
@@ -671,13 +693,14 @@ bool ct_xinv(const cplx_t<R>* S1, int pitch, int Px, Twiddles& tw, const Geom& g
     template bool ct_xfwd<R>(const R*, int, int64_t, int64_t, const R*, R, cplx_t<R>*, int, int, Twiddles&,          \
                              cudaStream_t);                                                                          \
     template bool ct_cols<R, -1>(const cplx_t<R>*, cplx_t<R>*, int, int, int, int, int64_t, int64_t, int64_t,        \
-                                 int64_t, int, Twiddles&, cudaStream_t);                                             \
+                                 int64_t, int, Twiddles&, const TuneChoice&, cudaStream_t);                          \
     template bool ct_cols<R, 1>(const cplx_t<R>*, cplx_t<R>*, int, int, int, int, int64_t, int64_t, int64_t, int64_t, \
-                                int, Twiddles&, cudaStream_t);                                                       \
-    template bool ct_convz<R>(cplx_t<R>*, const R*, int, int, int, int, Twiddles&, cudaStream_t);                    \
+                                int, Twiddles&, const TuneChoice&, cudaStream_t);                                    \
+    template bool ct_convz<R>(cplx_t<R>*, const R*, int, int, int, int, Twiddles&, const TuneChoice&,                \
+                              cudaStream_t);                                                                         \
     template bool ct_convy<R>(cplx_t<R>*, const R*, int, int, int, Twiddles&, cudaStream_t);                         \
     template bool ct_xinv<R>(const cplx_t<R>*, int, int, Twiddles&, const Geom&, R, const R*, const MsInfo&,          \
-                             const TermList&, const EpilogueArgs&, cudaStream_t, int*);
+                             const TermList&, const EpilogueArgs&, const TuneChoice&, cudaStream_t, int*);
 MAF_INST(float)
 MAF_INST(double)
 

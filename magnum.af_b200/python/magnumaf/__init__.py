@@ -84,6 +84,9 @@ _SIGS = {
     "maf_llg_heff_f32": (_I, [_P, _P, _FP]),
     "maf_llg_heff_device": (_I, [_P, _P, _P, _P]),
     "maf_llg_heff_pipeline": (_I, [_P, _P, C.POINTER(_P), C.POINTER(_P), _I]),
+    "maf_llg_autotune": (_I, [_P, _P, _I, C.POINTER(_I), _DP]),
+    "maf_term_demag_get_tune": (_I, [_P, C.POINTER(_I)]),
+    "maf_term_demag_set_tune": (_I, [_P, C.POINTER(_I)]),
     "maf_llg_heff_device_profile": (_I, [_P, _P, _P, _P, _DP, _I, C.POINTER(_I)]),
     "maf_llg_pass_name": (_I, [_P, _P, _I, C.c_char_p, _I]),
     "maf_llg_dmdt": (_I, [_P, _P, _DP]),
@@ -366,6 +369,18 @@ class DemagField(FieldTerm):
         _ck(lib.maf_term_demag_tensor(self._h, _dptr(out)))
         return out
 
+    @property
+    def tune(self):
+        """Kernel variants of this mesh's passes: (cols_wide, convz_reg, xinv_run), see LLGIntegrator.autotune."""
+        ch = (_I * 3)()
+        _ck(lib.maf_term_demag_get_tune(self._h, ch))
+        return tuple(ch)
+
+    @tune.setter
+    def tune(self, choices):
+        ch = (_I * 3)(*[int(c) for c in choices])
+        _ck(lib.maf_term_demag_set_tune(self._h, ch))
+
     def get_N(self, symmetric=False) -> np.ndarray:
         """Real-space Newell tensor [Px, Py, Pz, 6] (the reference's setup_N layout);
         symmetric=True returns the parity-exact tensor the spectral pipeline uses."""
@@ -563,6 +578,16 @@ class LLGIntegrator:
     def heff_device(self, state: State, m_dev_ptr: int, H_dev_ptr: int):
         """Field of a device-resident m into a device-resident H (no sync)."""
         _ck(lib.maf_llg_heff_device(self._h, state._h, C.c_void_p(m_dev_ptr), C.c_void_p(H_dev_ptr)))
+
+    def autotune(self, state: State, reps: int = 3) -> dict:
+        """Pick the faster kernel variant per demag pass on this state's mesh
+        (see maf_llg_autotune); returns the choices and both configurations'
+        per-pass times in ms."""
+        ch = (_I * 3)()
+        ms = np.zeros(10)
+        _ck(lib.maf_llg_autotune(self._h, state._h, int(reps), ch, _dptr(ms)))
+        return {"cols_wide": ch[0], "convz_reg": ch[1], "xinv_run": ch[2], "pass_ms_default": ms[:5].tolist(),
+                "pass_ms_alternative": ms[5:].tolist()}
 
     def heff_pipeline(self, state: State, m_host_ptrs, H_host_ptrs):
         """Fields of several host magnetisations in a row, host copies overlapped

@@ -1,0 +1,34 @@
+"""Kernel-variant autotuner (maf_llg_autotune, DemagField.tune): every variant
+computes the same field as the defaults up to rounding, and the autotuner
+returns valid choices and keeps them in the DemagField."""
+import numpy as np
+import pytest
+
+from helpers import random_m, rel_l2
+
+M = pytest.importorskip("magnumaf")
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("precision,tol", [("fp32_field", 2e-6), ("fp64", 1e-13)])
+@pytest.mark.parametrize("shape", [(64, 32, 8), (32, 32, 16), (64, 64, 1)])
+def test_variants_agree_and_autotune_picks_valid(precision, tol, shape):
+    mesh = M.Mesh(*shape, 3e-9, 3e-9, 3e-9)
+    d = M.DemagField(mesh)
+    llg = M.LLGIntegrator(0.01, [d, M.ExchangeField(1.3e-11), M.CubicAnisotropyField(-1e4)])
+    s = M.State(mesh, 8.6e5, random_m(shape, 3), precision=precision)
+    f32 = precision == "fp32_field"
+    field = (lambda: llg.H_in_Apm_f32(s)) if f32 else (lambda: llg.H_in_Apm(s))
+    assert d.tune == (0, 1, 0)
+    H0 = np.asarray(field(), dtype=np.float64)
+    for choice in [(1, 1, 2), (0, 0, 4), (1, 0, 2)]:
+        d.tune = choice
+        H = np.asarray(field(), dtype=np.float64)
+        assert rel_l2(H, H0) <= tol, (choice, rel_l2(H, H0))
+    res = llg.autotune(s, reps=2)
+    assert res["cols_wide"] in (0, 1) and res["convz_reg"] in (0, 1) and res["xinv_run"] in (2, 4)
+    assert d.tune == (res["cols_wide"], res["convz_reg"], res["xinv_run"])
+    assert rel_l2(np.asarray(field(), dtype=np.float64), H0) <= tol
+    with pytest.raises(M.MafError):
+        d.tune = (2, 1, 2)
