@@ -63,6 +63,9 @@ int maf_state_destroy(maf_state s);
 int maf_state_get_m(maf_state s, double* m_host);
 /* State::set_m: normalises (state.cpp:131) */
 int maf_state_set_m(maf_state s, const double* m_host);
+/* m copied as it is, without normalisation: restoring a checkpoint or a file (State::_vti_reader,
+ * vtk_io.cpp:255-259, assigns the file's values) */
+int maf_state_load_m(maf_state s, const double* m_host);
 int maf_state_get_t(maf_state s, double* t);
 int maf_state_set_t(maf_state s, double t);
 int maf_state_get_steps(maf_state s, unsigned long long* steps);
@@ -85,6 +88,10 @@ int maf_state_precision(maf_state s, int* precision);
 /* DemagField(Mesh mesh, ...) (magnumaf/src/field_terms/micro/demag_field.cpp:211-213):
  * the Newell tensor is computed on the GPU in FP64 and transformed once. */
 int maf_term_demag_create(maf_term* out, int nx, int ny, int nz, double dx, double dy, double dz);
+/* DemagField from a reduced spectral tensor saved earlier with maf_term_demag_tensor (the disk cache of
+ * get_Nfft(mesh, verbose, caching=true), demag_field.cpp:185-199, and util/cache_manager.cpp:49-116). */
+int maf_term_demag_create_from_tensor(maf_term* out, int nx, int ny, int nz, double dx, double dy, double dz,
+                                      const double* tensor_host);
 /* ExchangeField(double A) (magnumaf/src/field_terms/micro/exchange_field.cpp:115-157) */
 int maf_term_exchange_create(maf_term* out, double A);
 /* DmiField(double D, std::array<double,3> D_axis) (magnumaf/src/field_terms/micro/dmi_field.cpp:15,41-110) */
@@ -241,6 +248,13 @@ int maf_lbfgs_stats(maf_lbfgs h, unsigned long long* iterations, unsigned long l
  * (controller.hpp:26-31) */
 int maf_llg_get_h(maf_llg l, double* h);
 int maf_llg_counters(maf_llg l, unsigned long long out[4]);
+/* Controller state for checkpoints, so that a resumed run takes the same step sizes:
+ * {h, errold, reject, hnext, n_accepted, n_reject, n_hmin, n_hmax, accumulated_steps}
+ * (controller.hpp:26-31, adaptive_runge_kutta.hpp:39) */
+int maf_llg_get_controller_state(maf_llg l, double out[9]);
+int maf_llg_set_controller_state(maf_llg l, const double in[9]);
+/* State::steps, for restoring a checkpoint */
+int maf_state_set_steps(maf_state s, unsigned long long steps);
 
 /* ------------------------------------------------------- String method ---
  * StringMethod(state, inputimages, n_interp, dt, llg)

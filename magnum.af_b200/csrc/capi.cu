@@ -941,6 +941,16 @@ int maf_state_set_m(maf_state st, const double* m_host) {
     });
 }
 
+int maf_state_load_m(maf_state st, const double* m_host) {
+    return guarded([&] {
+        check(st && m_host, "NULL argument");
+        StateD& s = st->s;
+        MAF_CUDA(cudaMemcpyAsync(s.m64.p, m_host, sizeof(double) * 3 * s.md.N(), cudaMemcpyHostToDevice, s.stream));
+        MAF_CUDA(cudaStreamSynchronize(s.stream));
+        st->m32_valid = false;
+    });
+}
+
 int maf_state_get_t(maf_state st, double* t) {
     return guarded([&] { check(st && t, "NULL argument"); *t = st->s.t; });
 }
@@ -998,7 +1008,8 @@ static maf_term new_term(std::shared_ptr<Term> t) {
     return h;
 }
 
-int maf_term_demag_create(maf_term* out, int nx, int ny, int nz, double dx, double dy, double dz) {
+static int demag_create(maf_term* out, int nx, int ny, int nz, double dx, double dy, double dz,
+                        const double* tensor_host) {
     return guarded([&] {
         check(out, "NULL argument");
         check(nx > 0 && ny > 0 && nz > 0 && dx > 0 && dy > 0 && dz > 0, "DemagField: invalid mesh");
@@ -1009,7 +1020,7 @@ int maf_term_demag_create(maf_term* out, int nx, int ny, int nz, double dx, doub
         cudaStream_t st;
         MAF_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
         try {
-            t->demag = std::make_unique<Demag>(t->demag_mesh, st);
+            t->demag = std::make_unique<Demag>(t->demag_mesh, st, tensor_host);
         } catch (...) {
             cudaStreamDestroy(st);
             throw;
@@ -1018,6 +1029,16 @@ int maf_term_demag_create(maf_term* out, int nx, int ny, int nz, double dx, doub
         cudaStreamDestroy(st);
         *out = new_term(t);
     });
+}
+
+int maf_term_demag_create(maf_term* out, int nx, int ny, int nz, double dx, double dy, double dz) {
+    return demag_create(out, nx, ny, nz, dx, dy, dz, nullptr);
+}
+
+int maf_term_demag_create_from_tensor(maf_term* out, int nx, int ny, int nz, double dx, double dy, double dz,
+                                      const double* tensor_host) {
+    if (!tensor_host) return fail(MAF_ERR_BADARG, "maf_term_demag_create_from_tensor: NULL tensor");
+    return demag_create(out, nx, ny, nz, dx, dy, dz, tensor_host);
 }
 
 int maf_term_exchange_create(maf_term* out, double A) {
@@ -1745,6 +1766,37 @@ int maf_lbfgs_stats(maf_lbfgs h, unsigned long long* iterations, unsigned long l
 
 int maf_llg_get_h(maf_llg l, double* h) {
     return guarded([&] { check(l && h, "NULL argument"); *h = l->h; });
+}
+
+int maf_llg_get_controller_state(maf_llg l, double out[9]) {
+    return guarded([&] {
+        check(l && out, "NULL argument");
+        const Controller& c = l->ctrl;
+        const double v[9] = {l->h, c.errold, c.reject ? 1.0 : 0.0, c.hnext, (double)c.n_accepted, (double)c.n_reject,
+                             (double)c.n_hmin, (double)c.n_hmax, (double)l->accumulated_steps};
+        std::copy(v, v + 9, out);
+    });
+}
+
+int maf_llg_set_controller_state(maf_llg l, const double in[9]) {
+    return guarded([&] {
+        check(l && in, "NULL argument");
+        check(in[0] > 0 && std::isfinite(in[0]), "maf_llg_set_controller_state: step size must be positive");
+        Controller& c = l->ctrl;
+        l->h = in[0];
+        c.errold = in[1];
+        c.reject = in[2] != 0.0;
+        c.hnext = in[3];
+        c.n_accepted = (unsigned long long)in[4];
+        c.n_reject = (unsigned long long)in[5];
+        c.n_hmin = (unsigned long long)in[6];
+        c.n_hmax = (unsigned long long)in[7];
+        l->accumulated_steps = (unsigned long long)in[8];
+    });
+}
+
+int maf_state_set_steps(maf_state st, unsigned long long steps) {
+    return guarded([&] { check(st, "NULL argument"); st->s.steps = steps; });
 }
 
 int maf_llg_counters(maf_llg l, unsigned long long out[4]) {

@@ -137,7 +137,9 @@ struct TuneChoice {
 class Demag {
   public:
     TuneChoice tune;
-    explicit Demag(const MeshDims& md, cudaStream_t st);
+    // tensor_host: a reduced spectral tensor from download_tensor (e.g. a disk
+    // cache) to upload instead of computing it
+    Demag(const MeshDims& md, cudaStream_t st, const double* tensor_host = nullptr);
     const MeshDims& mesh() const { return md_; }
     int Px() const { return 2 * md_.nx; }
     int Py() const { return 2 * md_.ny; }

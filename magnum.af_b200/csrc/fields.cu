@@ -445,7 +445,7 @@ static void launch_cols(const cplx_t<R>* in, cplx_t<R>* out, int L, int n_in, in
 // ---------------------------------------------------------------------------
 // Demag
 // ---------------------------------------------------------------------------
-Demag::Demag(const MeshDims& md, cudaStream_t st) : md_(md) {
+Demag::Demag(const MeshDims& md, cudaStream_t st, const double* tensor_host) : md_(md) {
     if (md.nx < 1 || md.ny < 1 || md.nz < 1) throw Error(1, "DemagField: empty mesh");
     // complex pitch: multiple of 4 so that tiles of 4 complex values start on 32 B
     pitch_ = (nxh() + 3) / 4 * 4;
@@ -453,7 +453,13 @@ Demag::Demag(const MeshDims& md, cudaStream_t st) : md_(md) {
     make_fft_plan(Px() / 2, nullptr);
     make_fft_plan(Py(), nullptr);
     make_fft_plan(Pz(), nullptr);
-    build_tensor(st);
+    if (tensor_host) {
+        Nred64_.alloc(sizeof(double) * tensor_elems());
+        MAF_CUDA(cudaMemcpyAsync(Nred64_.p, tensor_host, sizeof(double) * tensor_elems(), cudaMemcpyHostToDevice, st));
+        MAF_CUDA(cudaStreamSynchronize(st));
+    } else {
+        build_tensor(st);
+    }
 }
 
 void Demag::build_tensor(cudaStream_t st) {

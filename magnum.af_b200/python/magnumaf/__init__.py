@@ -48,6 +48,7 @@ _SIGS = {
     "maf_state_destroy": (_I, [_P]),
     "maf_state_get_m": (_I, [_P, _DP]),
     "maf_state_set_m": (_I, [_P, _DP]),
+    "maf_state_load_m": (_I, [_P, _DP]),
     "maf_state_get_t": (_I, [_P, _DP]),
     "maf_state_set_t": (_I, [_P, _D]),
     "maf_state_get_steps": (_I, [_P, C.POINTER(C.c_ulonglong)]),
@@ -58,6 +59,7 @@ _SIGS = {
     "maf_state_device_m": (_I, [_P, C.POINTER(_P)]),
     "maf_state_precision": (_I, [_P, C.POINTER(_I)]),
     "maf_term_demag_create": (_I, [C.POINTER(_P), _I, _I, _I, _D, _D, _D]),
+    "maf_term_demag_create_from_tensor": (_I, [C.POINTER(_P), _I, _I, _I, _D, _D, _D, _DP]),
     "maf_term_exchange_create": (_I, [C.POINTER(_P), _D]),
     "maf_term_dmi_create": (_I, [C.POINTER(_P), _D, _D, _D, _D]),
     "maf_term_dmi_field_create": (_I, [C.POINTER(_P), _I, _I, _I, _DP, _D, _D, _D]),
@@ -108,6 +110,9 @@ _SIGS = {
     "maf_lbfgs_stats": (_I, [_P, C.POINTER(C.c_ulonglong), C.POINTER(C.c_ulonglong), _DP]),
     "maf_llg_get_h": (_I, [_P, _DP]),
     "maf_llg_counters": (_I, [_P, C.POINTER(C.c_ulonglong)]),
+    "maf_llg_get_controller_state": (_I, [_P, _DP]),
+    "maf_llg_set_controller_state": (_I, [_P, _DP]),
+    "maf_state_set_steps": (_I, [_P, C.c_ulonglong]),
     "maf_mean_m_noalloc": (_I, [_P, C.c_longlong, _DP, _P]),
     "maf_cnn_create": (_I, [C.POINTER(_P), _I, _I, _I, C.c_ulonglong]),
     "maf_cnn_destroy": (_I, [_P]),
@@ -254,6 +259,11 @@ class State:
         mf = _vec_soa(m_in, self.mesh)
         _ck(lib.maf_state_set_m(self._h, _dptr(mf)))
 
+    def load_m(self, m_in):
+        """Set m exactly as given, without normalising (checkpoints, files)."""
+        mf = _vec_soa(m_in, self.mesh)
+        _ck(lib.maf_state_load_m(self._h, _dptr(mf)))
+
     @property
     def t(self) -> float:
         v = C.c_double()
@@ -269,6 +279,23 @@ class State:
         v = C.c_ulonglong()
         _ck(lib.maf_state_get_steps(self._h, C.byref(v)))
         return v.value
+
+    @steps.setter
+    def steps(self, value: int):
+        _ck(lib.maf_state_set_steps(self._h, int(value)))
+
+    def write_vti(self, outputname):
+        """State::write_vti: m as a cell-centred VTK image (magnumaf.io.write_vti)."""
+        from . import io
+        return io.write_vti(self.m, self.mesh.dx, self.mesh.dy, self.mesh.dz, outputname)
+
+    def read_vti(self, inputname):
+        """State::_vti_reader: m from a .vti file of the same mesh, as stored."""
+        from . import io
+        a, _ = io.read_vti(inputname)
+        if a.shape[:3] != (self.mesh.nx, self.mesh.ny, self.mesh.nz) or a.shape[3] != 3:
+            raise ValueError("read_vti: the file holds a %s field" % (a.shape,))
+        self.load_m(a)
 
     @property
     def Ms(self) -> float:
@@ -350,15 +377,75 @@ class FieldTerm:
         return self.Energy_in_J(state) / 1.6021766208e-19
 
 
+_TENSOR_CACHE_MAX = 4 << 30     # bytes kept in the tensor cache before it is shrunk
+_TENSOR_CACHE_SHRINK = 2 << 30  # size it is shrunk to (oldest files first)
+
+
+def tensor_cache_dir() -> str:
+    return os.environ.get("MAGNUMAF_CACHE", os.path.join(os.path.expanduser("~"), ".cache", "magnumaf_b200"))
+
+
+def _tensor_cache_file(mesh: Mesh) -> str:
+    return os.path.join(tensor_cache_dir(), "Nred_v1_%d_%d_%d_%r_%r_%r.npy" % (
+        mesh.nx, mesh.ny, mesh.nz, float(mesh.dx), float(mesh.dy), float(mesh.dz)))
+
+
+def _shrink_tensor_cache(verbose=False):
+    d = tensor_cache_dir()
+    files = [os.path.join(d, f) for f in os.listdir(d) if f.startswith("Nred_") and f.endswith(".npy")]
+    files = [f for f in files if os.path.isfile(f)]
+    if sum(os.path.getsize(f) for f in files) <= _TENSOR_CACHE_MAX:
+        return
+    files.sort(key=os.path.getmtime, reverse=True)  # newest first, remove from the back
+    while files and sum(os.path.getsize(f) for f in files) > _TENSOR_CACHE_SHRINK:
+        old = files.pop()
+        if verbose:
+            print("removing cached demag tensor", old)
+        os.remove(old)
+
+
 class DemagField(FieldTerm):
     """DemagField(mesh, verbose=False, caching=False, nthreads=4): the tensor is
-    always assembled on the GPU; ``caching`` and ``nthreads`` are accepted for
-    signature compatibility."""
+    assembled on the GPU.  With ``caching`` the reduced spectral tensor is kept on
+    disk (``tensor_cache_dir()``, key: mesh sizes and spacings; the cache is shrunk
+    oldest-first beyond 4 GiB) and read back on the next construction for the same
+    mesh (the reference's get_Nfft caching, demag_field.cpp:185-199).  ``nthreads``
+    is accepted for signature compatibility."""
 
     def __init__(self, mesh: Mesh, verbose=False, caching=False, nthreads=4):
         self.mesh = mesh
         self._h = _P()
+        if caching:
+            path = _tensor_cache_file(mesh)
+            shape = self._tensor_shape()
+            if os.path.exists(path):
+                try:
+                    N = np.load(path)
+                    if N.shape != shape or N.dtype != np.float64:
+                        raise ValueError("cached tensor has the wrong shape")
+                    _ck(lib.maf_term_demag_create_from_tensor(C.byref(self._h), mesh.nx, mesh.ny, mesh.nz, mesh.dx,
+                                                              mesh.dy, mesh.dz, _dptr(np.ascontiguousarray(N))))
+                    if verbose:
+                        print("read demag tensor from", path)
+                    return
+                except (OSError, ValueError) as e:
+                    if verbose:
+                        print("ignoring cached demag tensor (%s), computing it" % e)
+                    self._h = _P()
         _ck(lib.maf_term_demag_create(C.byref(self._h), mesh.nx, mesh.ny, mesh.nz, mesh.dx, mesh.dy, mesh.dz))
+        if caching:
+            os.makedirs(tensor_cache_dir(), exist_ok=True)
+            tmp = path + ".%d.tmp" % os.getpid()
+            with open(tmp, "wb") as f:
+                np.save(f, self.spectral_tensor())
+            os.replace(tmp, path)
+            if verbose:
+                print("saved demag tensor to", path)
+            _shrink_tensor_cache(verbose)
+
+    def _tensor_shape(self):
+        m = self.mesh
+        return (4 if m.nz == 1 else 6, 1 if m.nz == 1 else m.nz + 1, m.ny + 1, m.nx + 1)
 
     def spectral_tensor(self) -> np.ndarray:
         """Reduced real spectral tensor [ncomp][kz][ky][kx] (C order)."""
@@ -574,6 +661,18 @@ class LLGIntegrator:
         out = (C.c_ulonglong * 4)()
         _ck(lib.maf_llg_counters(self._h, out))
         return {"accepted": out[0], "rejected": out[1], "hmin": out[2], "hmax": out[3]}
+
+    def controller_state(self):
+        """[h, errold, reject, hnext, accepted, rejected, hmin, hmax, accumulated_steps] (for checkpoints)."""
+        out = np.zeros(9)
+        _ck(lib.maf_llg_get_controller_state(self._h, _dptr(out)))
+        return out.tolist()
+
+    def set_controller_state(self, values):
+        v = np.ascontiguousarray(values, dtype=np.float64)
+        if v.size != 9:
+            raise ValueError("9 values expected")
+        _ck(lib.maf_llg_set_controller_state(self._h, _dptr(v)))
 
     def heff_device(self, state: State, m_dev_ptr: int, H_dev_ptr: int):
         """Field of a device-resident m into a device-resident H (no sync)."""
