@@ -111,6 +111,11 @@ int maf_term_uniaxial_field_create(maf_term* out, int nx, int ny, int nz, const 
 /* CubicAnisotropyField(Kc1, Kc2, Kc3, c1, c2) (magnumaf/src/field_terms/micro/cubic_anisotropy_field.cpp:9-22,61-113);
  * returns MAF_ERR_BADARG where the reference exits, i.e. when |c1.c2| > 1e-12 */
 int maf_term_cubic_create(maf_term* out, double Kc1, double Kc2, double Kc3, const double c1[3], const double c2[3]);
+/* SpinTransferTorqueField(polarization, eta_damping, eta_field, j_e, fl_thickness)
+ * (magnumaf/src/field_terms/micro/spin_transfer_torque_field.cpp:7-28): H = -j_e hbar / (2 e mu0 Ms d)
+ * (eta_d m x p + eta_f p) with the normalised polarisation p [3][N]; zero where Ms = 0 */
+int maf_term_stt_create(maf_term* out, int nx, int ny, int nz, const double* polarization_host, double eta_damping,
+                        double eta_field, double j_e, double fl_thickness);
 /* ExternalField(af::array zee) (magnumaf/src/field_terms/micro/external_field.cpp:9,28-48); h is [3][N] */
 int maf_term_external_create(maf_term* out, int nx, int ny, int nz, const double* h_host);
 /* ExternalField with one field vector for every cell (set_homogeneous_field, external_field.cpp:19-25) */

@@ -1088,6 +1088,7 @@ int maf_term_dmi_field_create(maf_term* out, int nx, int ny, int nz, const doubl
         t->p[2] = ay / norm;
         t->p[3] = az / norm;
         upload(t->f0, D_field, (size_t)nx * ny * nz, 0);
+        t->field_cells = (int64_t)nx * ny * nz;
         t->demag_mesh = MeshDims{nx, ny, nz, 0, 0, 0};
         *out = new_term(t);
     });
@@ -1125,6 +1126,7 @@ int maf_term_uniaxial_field_create(maf_term* out, int nx, int ny, int nz, const 
         t->p[0] = Ku1;
         const size_t N = (size_t)nx * ny * nz;
         if (Ku1_field) upload(t->f0, Ku1_field, N, 0);
+        if (Ku1_field || axis_field) t->field_cells = (int64_t)N;
         if (axis_field) {
             // util::normalize on the axis field (uniaxial_anisotropy_field.cpp:24)
             upload(t->f1, axis_field, 3 * N, 0);
@@ -1133,6 +1135,27 @@ int maf_term_uniaxial_field_create(maf_term* out, int nx, int ny, int nz, const 
         } else {
             set_unit_axis(t->p + 1, ax, ay, az, "UniaxialAnisotropyField");
         }
+        *out = new_term(t);
+    });
+}
+
+int maf_term_stt_create(maf_term* out, int nx, int ny, int nz, const double* polarization_host, double eta_damping,
+                        double eta_field, double j_e, double fl_thickness) {
+    return guarded([&] {
+        check(out && polarization_host, "NULL argument");
+        check(nx > 0 && ny > 0 && nz > 0 && fl_thickness > 0, "SpinTransferTorqueField: bad argument");
+        require_device();
+        auto t = std::make_shared<Term>();
+        t->kind = TK_STT;
+        t->p[0] = -j_e * kHbar / (2. * kEneg * kMu0 * fl_thickness);
+        t->p[1] = eta_damping;
+        t->p[2] = eta_field;
+        const size_t N = (size_t)nx * ny * nz;
+        // util::normalize of the polarisation (spin_transfer_torque_field.cpp:9)
+        upload(t->f1, polarization_host, 3 * N, 0);
+        t->field_cells = (int64_t)N;
+        normalize_m(t->f1.as<double>(), (int64_t)N, 2, nullptr, 0);
+        MAF_CUDA(cudaDeviceSynchronize());
         *out = new_term(t);
     });
 }
@@ -1184,6 +1207,7 @@ int maf_term_external_create(maf_term* out, int nx, int ny, int nz, const double
         } else {
             require_device();
             upload(t->f0, h_host, 3 * N, 0);
+            t->field_cells = (int64_t)N;
         }
         t->demag_mesh = MeshDims{nx, ny, nz, 0, 0, 0};
         *out = new_term(t);
@@ -1208,10 +1232,8 @@ int maf_term_destroy(maf_term t) {
 
 static void check_term_state(maf_term t, maf_state s) {
     check(t && s, "NULL argument");
-    if (t->t->f0.p || t->t->f1.p) {
-        check(t->t->demag_mesh.N() == s->s.md.N() || t->t->demag_mesh.N() == 0,
-              "field-term parameter array does not match the state's mesh");
-    }
+    check(t->t->field_cells == 0 || t->t->field_cells == s->s.md.N(),
+          "field-term parameter array does not match the state's mesh");
 }
 
 int maf_term_H(maf_term t, maf_state s, double* H) {

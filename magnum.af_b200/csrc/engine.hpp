@@ -178,6 +178,7 @@ struct Term {
     int kind = TK_DEMAG;
     double p[12] = {};
     DevBuf f0, f1;                   // optional parameter fields (FP64)
+    int64_t field_cells = 0;         // cells of the mesh f0/f1 were given on (0: no field)
     std::unique_ptr<Demag> demag;    // TK_DEMAG
     MeshDims demag_mesh;
     TermDesc desc() const {

@@ -691,6 +691,8 @@ void eval_terms(const std::vector<Term*>& terms, const MeshDims& md, const R* m,
             if (!(t->demag_mesh == md)) throw Error(1, "DemagField mesh differs from the state's mesh");
             demag = t->demag.get();
         }
+        if (t->field_cells && t->field_cells != md.N())
+            throw Error(1, "field-term parameter array does not match the state's mesh");
         if (t->kind == TK_BULKDMI && (md.nx < 2 || md.ny < 2 || md.nz < 2))
             throw Error(1, "BulkDMIExchangeField needs at least 2 cells along x, y and z");
         tl.t[tl.n++] = t->desc();

@@ -27,6 +27,7 @@ enum TermKind : int {
     TK_UNIAXIAL = 4,
     TK_CUBIC = 5,
     TK_ZEEMAN = 6,
+    TK_STT = 7,
 };
 
 constexpr int kMaxTerms = 8;
@@ -255,6 +256,18 @@ __device__ __forceinline__ void add_local_term(const TermDesc& t, const R* __res
             h[0] += hc[0];
             h[1] += hc[1];
             h[2] += hc[2];
+            break;
+        }
+        case TK_STT: {
+            // spin-transfer (spin-orbit) torque field (spin_transfer_torque_field.cpp:17-28):
+            // p[0] = -j_e hbar / (2 e mu0 d), p[1] = eta_damping, p[2] = eta_field,
+            // f1 = unit polarisation [3][N]; H = p[0]/Ms (eta_d m x p + eta_f p), 0 where Ms = 0
+            if (ms_is_field && Ms == (R)0) return;
+            const R p0 = (R)t.f1[cell], p1 = (R)t.f1[g.N + cell], p2 = (R)t.f1[2 * g.N + cell];
+            const R coef = (R)t.p[0] / Ms, ed = (R)t.p[1], ef = (R)t.p[2];
+            h[0] += coef * (ed * (mc[1] * p2 - mc[2] * p1) + ef * p0);
+            h[1] += coef * (ed * (mc[2] * p0 - mc[0] * p2) + ef * p1);
+            h[2] += coef * (ed * (mc[0] * p1 - mc[1] * p0) + ef * p2);
             break;
         }
         case TK_ZEEMAN: {

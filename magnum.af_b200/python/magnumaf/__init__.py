@@ -69,6 +69,7 @@ _SIGS = {
     "maf_term_cubic_create": (_I, [C.POINTER(_P), _D, _D, _D, _DP, _DP]),
     "maf_term_external_create": (_I, [C.POINTER(_P), _I, _I, _I, _DP]),
     "maf_term_external_uniform_create": (_I, [C.POINTER(_P), _D, _D, _D]),
+    "maf_term_stt_create": (_I, [C.POINTER(_P), _I, _I, _I, _DP, _D, _D, _D, _D]),
     "maf_term_destroy": (_I, [_P]),
     "maf_term_H": (_I, [_P, _P, _DP]),
     "maf_term_H_f32": (_I, [_P, _P, _FP]),
@@ -531,6 +532,20 @@ class CubicAnisotropyField(FieldTerm):
         a = np.asarray(c1, dtype=np.float64)
         b = np.asarray(c2, dtype=np.float64)
         _ck(lib.maf_term_cubic_create(C.byref(self._h), float(Kc1), float(Kc2), float(Kc3), _dptr(a), _dptr(b)))
+
+
+class SpinTransferTorqueField(FieldTerm):
+    """SpinTransferTorqueField(pol, eta_damp, eta_field, j_e, fl_thickness) (python/magnumaf.pyx:1690-1730):
+    pol is a (nx, ny, nz, 3) polarisation field (normalised on construction)."""
+
+    def __init__(self, pol, eta_damp: float, eta_field: float, j_e: float, fl_thickness: float):
+        pf = _vec_soa(pol)
+        nx, ny, nz = pf.shape[:3]
+        self.eta_damping, self.eta_field, self.j_e, self.fl_thickness = (float(eta_damp), float(eta_field),
+                                                                          float(j_e), float(fl_thickness))
+        self._h = _P()
+        _ck(lib.maf_term_stt_create(C.byref(self._h), nx, ny, nz, _dptr(pf), self.eta_damping, self.eta_field,
+                                    self.j_e, self.fl_thickness))
 
 
 class ExternalField(FieldTerm):

@@ -39,6 +39,7 @@ kb = 1.38064852e-23
 mu_b = 9.274009994e-24
 e_abs = 1.6021766208e-19
 hbar = 1.0545718e-34
+e_neg = -1.6021766208e-19
 
 
 def to_soa(a: np.ndarray) -> np.ndarray:
@@ -627,6 +628,21 @@ class ExternalField(FieldTerm):
         if h is None:
             h = self.H_in_Apm(state)
         return micro_energy(state, h, factor=-mu0)
+
+
+class SpinTransferTorqueField(FieldTerm):
+    """spin_transfer_torque_field.cpp:7-28: H = -j_e hbar / (2 e mu0 Ms d) (eta_d m x p + eta_f p),
+    p = normalize(polarization); zero where Ms_field == 0; default micro energy."""
+
+    def __init__(self, pol, eta_damping, eta_field, j_e, fl_thickness):
+        self.pol = normalize(np.asarray(pol, dtype=np.float64))
+        self.eta_damping, self.eta_field = float(eta_damping), float(eta_field)
+        self.j_e, self.fl_thickness = float(j_e), float(fl_thickness)
+
+    def H_in_Apm(self, state):
+        pre = -self.j_e * hbar / (2.0 * e_neg * mu0 * self.fl_thickness)
+        h = pre * _inv_Ms(state) * (self.eta_damping * cross4(state.m, self.pol) + self.eta_field * self.pol)
+        return _replace_ms_zero(np.nan_to_num(h, nan=0.0, posinf=0.0, neginf=0.0), state)
 
 
 def Heff_in_Apm(terms: Sequence[FieldTerm], state):
