@@ -116,6 +116,22 @@ int maf_term_cubic_create(maf_term* out, double Kc1, double Kc2, double Kc3, con
  * (eta_d m x p + eta_f p) with the normalised polarisation p [3][N]; zero where Ms = 0 */
 int maf_term_stt_create(maf_term* out, int nx, int ny, int nz, const double* polarization_host, double eta_damping,
                         double eta_field, double j_e, double fl_thickness);
+/* DemagFieldPBC() (magnumaf/src/field_terms/micro/demag_field_pbc.cpp:36-71): periodic demag through the
+ * scalar potential on the mesh's own grid (transforms of nx, ny, nz, no tensor). The plan is made for the
+ * mesh of the first state evaluated (and remade when a state of another mesh is evaluated); nx must be even
+ * (MAF_ERR_UNSUPPORTED otherwise: the reference's C2R returns 2*(nx/2) columns) */
+int maf_term_demag_pbc_create(maf_term* out);
+/* SparseExchangeField(A, mesh) and SparseExchangeField(A_field, mesh)
+ * (magnumaf/src/field_terms/micro/sparse_exchange_field.cpp:8-18,25-101,183-330, COO assembly, the default):
+ * H = (M m) / Ms with the 7-point matrix M of the mesh nx*ny*nz.  A_field_host [nz][ny][nx] or NULL
+ * (then the scalar A: neighbours inside the mesh weigh 2A/(mu0 d^2), no diagonal); with a field the
+ * weights are 2A_i/(mu0 d^2) * 2A_nb/(A_nb+A_i), the diagonal minus their sum, rows with A_i = 0 empty.
+ * The matrix is not stored: the kernel forms each row's weights. Also ExchangeField(A, mesh)
+ * (python/magnumaf.pyx:1172-1195) */
+int maf_term_sparse_exchange_create(maf_term* out, int nx, int ny, int nz, const double* A_field_host, double A);
+/* ExchangeFieldPBC(A, mesh) / (A_field, mesh) (magnumaf/src/field_terms/micro/exchange_field_pbc.cpp:9-19,31-225):
+ * the harmonic-mean matrix above with periodic neighbours in x, y and z, also for a scalar A */
+int maf_term_exchange_pbc_create(maf_term* out, int nx, int ny, int nz, const double* A_field_host, double A);
 /* ExternalField(af::array zee) (magnumaf/src/field_terms/micro/external_field.cpp:9,28-48); h is [3][N] */
 int maf_term_external_create(maf_term* out, int nx, int ny, int nz, const double* h_host);
 /* ExternalField with one field vector for every cell (set_homogeneous_field, external_field.cpp:19-25) */

@@ -1041,6 +1041,17 @@ int maf_term_demag_create_from_tensor(maf_term* out, int nx, int ny, int nz, dou
     return demag_create(out, nx, ny, nz, dx, dy, dz, tensor_host);
 }
 
+int maf_term_demag_pbc_create(maf_term* out) {
+    return guarded([&] {
+        check(out, "NULL argument");
+        require_device();
+        auto t = std::make_shared<Term>();
+        t->kind = TK_DEMAG;
+        t->p[0] = 1.0;  // periodic form; the plan is made for the first state evaluated
+        *out = new_term(t);
+    });
+}
+
 int maf_term_exchange_create(maf_term* out, double A) {
     return guarded([&] {
         check(out, "NULL argument");
@@ -1160,6 +1171,33 @@ int maf_term_stt_create(maf_term* out, int nx, int ny, int nz, const double* pol
     });
 }
 
+// SparseExchangeField and ExchangeFieldPBC: the matrix is not stored; the kernel
+// forms each row's weights from A (or the A field) as the assembly does.
+static int sparse_exchange_create(maf_term* out, int nx, int ny, int nz, const double* A_field, double A,
+                                  bool periodic, const char* who) {
+    return guarded([&] {
+        check(out, "NULL argument");
+        check(nx > 0 && ny > 0 && nz > 0, std::string(who) + ": bad mesh");
+        require_device();
+        auto t = std::make_shared<Term>();
+        t->kind = TK_SPARSE_EXCH;
+        t->p[0] = A;
+        t->p[1] = periodic ? 1.0 : 0.0;
+        const size_t N = (size_t)nx * ny * nz;
+        if (A_field) upload(t->f0, A_field, N, 0);
+        t->field_cells = (int64_t)N;  // the matrix is built for this mesh
+        *out = new_term(t);
+    });
+}
+
+int maf_term_sparse_exchange_create(maf_term* out, int nx, int ny, int nz, const double* A_field_host, double A) {
+    return sparse_exchange_create(out, nx, ny, nz, A_field_host, A, false, "SparseExchangeField");
+}
+
+int maf_term_exchange_pbc_create(maf_term* out, int nx, int ny, int nz, const double* A_field_host, double A) {
+    return sparse_exchange_create(out, nx, ny, nz, A_field_host, A, true, "ExchangeFieldPBC");
+}
+
 int maf_term_cubic_create(maf_term* out, double Kc1, double Kc2, double Kc3, const double c1[3], const double c2[3]) {
     return guarded([&] {
         check(out && c1 && c2, "NULL argument");
@@ -1264,14 +1302,16 @@ int maf_term_E(maf_term t, maf_state s, double* E) {
 
 int maf_term_demag_tensor(maf_term t, double* host) {
     return guarded([&] {
-        check(t && host && t->t->kind == TK_DEMAG, "maf_term_demag_tensor: not a DemagField");
+        check(t && host && t->t->kind == TK_DEMAG && !t->t->demag_pbc(),
+              "maf_term_demag_tensor: not a DemagField");
         t->t->demag->download_tensor(host, 0);
     });
 }
 
 int maf_term_demag_real_tensor(maf_term t, double* host, int symmetric) {
     return guarded([&] {
-        check(t && host && t->t->kind == TK_DEMAG, "maf_term_demag_real_tensor: not a DemagField");
+        check(t && host && t->t->kind == TK_DEMAG && !t->t->demag_pbc(),
+              "maf_term_demag_real_tensor: not a DemagField");
         t->t->demag->download_real_tensor(host, symmetric != 0, 0);
     });
 }
@@ -1488,7 +1528,7 @@ int maf_llg_autotune(maf_llg l, maf_state s, int reps, int choices[3], double* p
         check(choices && reps > 0, "maf_llg_autotune: bad argument");
         Demag* dm = nullptr;
         for (auto& t : l->terms)
-            if (t->kind == TK_DEMAG) dm = t->demag.get();
+            if (t->kind == TK_DEMAG && !t->demag_pbc()) dm = t->demag.get();  // the periodic form has no variants
         TuneChoice best;
         if (dm) {
             StateD& st = s->s;
@@ -1546,7 +1586,8 @@ int maf_llg_autotune(maf_llg l, maf_state s, int reps, int choices[3], double* p
 
 int maf_term_demag_get_tune(maf_term t, int choices[3]) {
     return guarded([&] {
-        check(t && choices && t->t->kind == TK_DEMAG, "maf_term_demag_get_tune: not a DemagField");
+        check(t && choices && t->t->kind == TK_DEMAG && !t->t->demag_pbc(),
+              "maf_term_demag_get_tune: not a DemagField");
         const TuneChoice& c = t->t->demag->tune;
         choices[0] = c.cols_wide;
         choices[1] = c.convz_reg;
@@ -1556,7 +1597,8 @@ int maf_term_demag_get_tune(maf_term t, int choices[3]) {
 
 int maf_term_demag_set_tune(maf_term t, const int choices[3]) {
     return guarded([&] {
-        check(t && choices && t->t->kind == TK_DEMAG, "maf_term_demag_set_tune: not a DemagField");
+        check(t && choices && t->t->kind == TK_DEMAG && !t->t->demag_pbc(),
+              "maf_term_demag_set_tune: not a DemagField");
         check((choices[0] == 0 || choices[0] == 1) && (choices[1] == 0 || choices[1] == 1) &&
                   (choices[2] == 0 || choices[2] == 2 || choices[2] == 4),
               "maf_term_demag_set_tune: choices are {0|1, 0|1, 0|2|4}");

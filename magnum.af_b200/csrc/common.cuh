@@ -9,6 +9,7 @@
 namespace mafb {
 
 constexpr double kMu0 = 4e-7 * 3.14159265358979323846;   // constants.hpp:11
+constexpr double kPi = 3.14159265358979323846;
 constexpr double kGamma = 1.760859644e11 * kMu0;          // constants.hpp:13
 constexpr double kHbar = 1.0545718e-34;                   // constants.hpp:22
 constexpr double kEneg = -1.6021766208e-19;               // constants.hpp:17

@@ -139,12 +139,17 @@ class Demag {
     TuneChoice tune;
     // tensor_host: a reduced spectral tensor from download_tensor (e.g. a disk
     // cache) to upload instead of computing it
-    Demag(const MeshDims& md, cudaStream_t st, const double* tensor_host = nullptr);
+    // pbc: the periodic scalar-potential form of DemagFieldPBC
+    // (demag_field_pbc.cpp:36-71): transforms of the mesh's own lengths, no
+    // tensor; the z (or, for nz == 1, y) pass applies the discrete Poisson
+    // operator instead of the tensor product.
+    Demag(const MeshDims& md, cudaStream_t st, const double* tensor_host = nullptr, bool pbc = false);
     const MeshDims& mesh() const { return md_; }
-    int Px() const { return 2 * md_.nx; }
-    int Py() const { return 2 * md_.ny; }
-    int Pz() const { return md_.nz == 1 ? 1 : 2 * md_.nz; }
-    int nxh() const { return md_.nx + 1; }
+    bool pbc() const { return pbc_; }
+    int Px() const { return pbc_ ? md_.nx : 2 * md_.nx; }
+    int Py() const { return pbc_ ? md_.ny : 2 * md_.ny; }
+    int Pz() const { return md_.nz == 1 ? 1 : (pbc_ ? md_.nz : 2 * md_.nz); }
+    int nxh() const { return Px() / 2 + 1; }
     int ncomp() const { return md_.nz == 1 ? 4 : 6; }
     // Passes 1..4: spectral convolution of Ms*m, result left in the half-spectrum
     // buffer for the fused x-inverse epilogue.
@@ -167,7 +172,8 @@ class Demag {
     void build_tensor(cudaStream_t st);
 
     MeshDims md_;
-    int pitch_;  // complex row pitch of the half spectrum (>= nx+1)
+    bool pbc_ = false;
+    int pitch_;  // complex row pitch of the half spectrum (>= nxh)
     DevBuf Nred64_, Nred32_;
     DevBuf S1_64_, S2_64_, S1_32_, S2_32_;
     Twiddles tw_;
@@ -179,8 +185,9 @@ struct Term {
     double p[12] = {};
     DevBuf f0, f1;                   // optional parameter fields (FP64)
     int64_t field_cells = 0;         // cells of the mesh f0/f1 were given on (0: no field)
-    std::unique_ptr<Demag> demag;    // TK_DEMAG
+    std::unique_ptr<Demag> demag;    // TK_DEMAG (DemagFieldPBC: created for the first state's mesh)
     MeshDims demag_mesh;
+    bool demag_pbc() const { return kind == TK_DEMAG && p[0] != 0.0; }
     TermDesc desc() const {
         TermDesc d;
         d.kind = kind;

@@ -173,13 +173,64 @@ __global__ void __launch_bounds__(kMaxFftThreads) k_fft_cols(const cplx_t<R>* in
     }
 }
 
+// Mesh lengths and spacings of the periodic Poisson operator.
+struct PbcOp {
+    int nx, ny, nz;
+    double dx, dy, dz;
+};
+
+// DemagFieldPBC in k space (demag_field_pbc.cpp:44-68), for the three
+// components M of the transform of Ms*m at (kx, ky, kz):
+//   K_a = 2 pi k_a / n_a,  d_a = 1 - exp(-i K_a) = (1 - cos K_a) + i sin K_a
+//   u = -(sum_a d_a M_a / h_a) / (sum_a 4/h_a^2 sin^2(K_a/2)),  u(0,0,0) = 0
+//   H_a = (1 - exp(i K_a)) u / h_a = conj(d_a) u / h_a
+// Evaluated in FP64 for either transform precision.
+template <typename C>
+__device__ __forceinline__ void pbc_poisson(const PbcOp& op, int kx, int ky, int kz, C& mx, C& my, C& mz) {
+    const double K[3] = {2.0 * kPi * kx / op.nx, 2.0 * kPi * ky / op.ny, 2.0 * kPi * kz / op.nz};
+    const double h[3] = {op.dx, op.dy, op.dz};
+    double dre[3], dim[3], den = 0.0;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        double sn, cs;
+        sincos(K[a], &sn, &cs);
+        dre[a] = 1.0 - cs;
+        dim[a] = sn;
+        const double s2 = sin(K[a] / 2.0);
+        den += 4.0 / (h[a] * h[a]) * (s2 * s2);
+    }
+    const double M[3][2] = {{(double)mx.x, (double)mx.y}, {(double)my.x, (double)my.y}, {(double)mz.x, (double)mz.y}};
+    double divr = 0.0, divi = 0.0;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        divr += (dre[a] * M[a][0] - dim[a] * M[a][1]) / h[a];
+        divi += (dre[a] * M[a][1] + dim[a] * M[a][0]) / h[a];
+    }
+    double ur = 0.0, ui = 0.0;
+    if (kx != 0 || ky != 0 || kz != 0) {
+        ur = -divr / den;
+        ui = -divi / den;
+    }
+    double H[3][2];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        H[a][0] = (dre[a] * ur + dim[a] * ui) / h[a];
+        H[a][1] = (dre[a] * ui - dim[a] * ur) / h[a];
+    }
+    using R = decltype(mx.x);
+    mx = mk((R)H[0][0], (R)H[0][1]);
+    my = mk((R)H[1][0], (R)H[1][1]);
+    mz = mk((R)H[2][0], (R)H[2][1]);
+}
+
 // Spectral convolution along the last transform axis (z for 3-D meshes, y for
 // nz == 1), in place: forward FFT of the three components (zero pad fused),
-// multiply by the symmetric tensor, inverse FFT, keep the first n_in values.
-template <typename R>
+// multiply by the symmetric tensor (or, PBC, apply the periodic Poisson
+// operator), inverse FFT, keep the first n_in values.
+template <typename R, bool PBC>
 __global__ void __launch_bounds__(kMaxFftThreads) k_conv(cplx_t<R>* S, const R* __restrict__ Nred, FFTPlan fplan, FFTPlan iplan,
                                                int n_in, int64_t si, int64_t comp_stride, int64_t other_stride,
-                                               int ncols, int nb, int axis_is_z, int ny, int nz, int nxh) {
+                                               int ncols, int nb, int axis_is_z, int ny, int nz, int nxh, PbcOp pop) {
     using C = cplx_t<R>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C* s = reinterpret_cast<C*>(smem_raw);
@@ -213,6 +264,14 @@ __global__ void __launch_bounds__(kMaxFftThreads) k_conv(cplx_t<R>* S, const R* 
         const int kx = c0 + b;
         int ky, kz;
         if (axis_is_z) { ky = other; kz = kf; } else { ky = kf; kz = 0; }
+        if constexpr (PBC) {
+            C px = s[lay.at(kf, b)], py = s[lay.at(kf, nb + b)], pz = s[lay.at(kf, 2 * nb + b)];
+            pbc_poisson(pop, kx, ky, kz, px, py, pz);
+            s[lay.at(kf, b)] = px;
+            s[lay.at(kf, nb + b)] = py;
+            s[lay.at(kf, 2 * nb + b)] = pz;
+            continue;
+        }
         const int kyr = ky <= ny ? ky : Py - ky;
         const R sy = ky <= ny ? (R)1 : (R)-1;
         int kzr = 0;
@@ -396,8 +455,8 @@ template <typename R> static int tile_target() { return sizeof(R) == 4 ? 8192 : 
 
 template <typename R>
 static void launch_xfwd(const R* in, int n_in, int64_t rows, int64_t rows_pc, const R* msf, R ms, cplx_t<R>* out,
-                        int pitch, int Px, Twiddles& tw, cudaStream_t st) {
-    if (ct_xfwd<R>(in, n_in, rows, rows_pc, msf, ms, out, pitch, Px, tw, st)) return;
+                        int pitch, int Px, Twiddles& tw, cudaStream_t st, bool try_ct = true) {
+    if (try_ct && ct_xfwd<R>(in, n_in, rows, rows_pc, msf, ms, out, pitch, Px, tw, st)) return;
     const bool f64 = sizeof(R) == 8;
     const int Lc = Px / 2;
     FFTPlan plan = make_fft_plan(Lc, tw.get(Lc, f64));
@@ -421,8 +480,9 @@ static void launch_xfwd(const R* in, int n_in, int64_t rows, int64_t rows_pc, co
 template <typename R, int DIR>
 static void launch_cols(const cplx_t<R>* in, cplx_t<R>* out, int L, int n_in, int n_out, int ncols, int64_t in_si,
                         int64_t out_si, int64_t in_sbat, int64_t out_sbat, int nbat, Twiddles& tw,
-                        const TuneChoice& tc, cudaStream_t st) {
-    if (ct_cols<R, DIR>(in, out, L, n_in, n_out, ncols, in_si, out_si, in_sbat, out_sbat, nbat, tw, tc, st)) return;
+                        const TuneChoice& tc, cudaStream_t st, bool try_ct = true) {
+    if (try_ct && ct_cols<R, DIR>(in, out, L, n_in, n_out, ncols, in_si, out_si, in_sbat, out_sbat, nbat, tw, tc, st))
+        return;
     const bool f64 = sizeof(R) == 8;
     FFTPlan plan = make_fft_plan(L, tw.get(L, f64));
     int nb = pick_nb(L, tile_target<R>(), ncols, 32);
@@ -445,8 +505,18 @@ static void launch_cols(const cplx_t<R>* in, cplx_t<R>* out, int L, int n_in, in
 // ---------------------------------------------------------------------------
 // Demag
 // ---------------------------------------------------------------------------
-Demag::Demag(const MeshDims& md, cudaStream_t st, const double* tensor_host) : md_(md) {
+Demag::Demag(const MeshDims& md, cudaStream_t st, const double* tensor_host, bool pbc) : md_(md), pbc_(pbc) {
     if (md.nx < 1 || md.ny < 1 || md.nz < 1) throw Error(1, "DemagField: empty mesh");
+    if (pbc) {
+        // the reference's inverse fftC2R(h, is_odd = false) returns 2*(nx/2) columns,
+        // i.e. the field only has the mesh's shape for even nx (demag_field_pbc.cpp:70)
+        if (md.nx % 2 != 0) throw Error(6, "DemagFieldPBC: nx must be even");
+        pitch_ = (nxh() + 3) / 4 * 4;
+        make_fft_plan(Px() / 2, nullptr);
+        make_fft_plan(Py(), nullptr);
+        make_fft_plan(Pz(), nullptr);
+        return;
+    }
     // complex pitch: multiple of 4 so that tiles of 4 complex values start on 32 B
     pitch_ = (nxh() + 3) / 4 * 4;
     // validate all FFT lengths early
@@ -550,18 +620,21 @@ template <typename R> void Demag::forward_conv(const R* m, const MsInfo& ms, cud
         else msf = reinterpret_cast<const R*>(ms.field64);
     }
     C* s1 = S1<R>();
-    const R* Nr = tensor<R>();
+    // the periodic form has no tensor and runs the run-time plans only
+    const R* Nr = pbc_ ? nullptr : tensor<R>();
+    const bool ct = !pbc_;
+    const PbcOp pop{nx, ny, nz, md_.dx, md_.dy, md_.dz};
     // pass 1: x forward (zero pad fused)
-    launch_xfwd<R>(m, nx, 3 * rows_pc, rows_pc, msf, (R)ms.Ms, s1, pitch_, Px(), tw_, st);
+    launch_xfwd<R>(m, nx, 3 * rows_pc, rows_pc, msf, (R)ms.Ms, s1, pitch_, Px(), tw_, st, ct);
     if (marks) marks->mark(st, "x_fwd");
     if (nz > 1) {
         C* s2 = S2<R>();
         // pass 2: y forward, S1 [3*nz][ny][pitch] -> S2 [3*nz][Py][pitch]
         launch_cols<R, -1>(s1, s2, Py(), ny, Py(), nxh(), pitch_, pitch_, (int64_t)ny * pitch_,
-                           (int64_t)Py() * pitch_, 3 * nz, tw_, tune, st);
+                           (int64_t)Py() * pitch_, 3 * nz, tw_, tune, st, ct);
         if (marks) marks->mark(st, "y_fwd");
         // pass 3: z forward . tensor . z inverse, in place on S2
-        if (!ct_convz<R>(s2, Nr, nz, ny, nxh(), pitch_, tw_, tune, st)) {
+        if (!ct || !ct_convz<R>(s2, Nr, nz, ny, nxh(), pitch_, tw_, tune, st)) {
             const int L = Pz();
             FFTPlan fp = make_fft_plan(L, tw_.get(L, f64));
             FFTPlan ip = fp;
@@ -574,20 +647,28 @@ template <typename R> void Demag::forward_conv(const R* m, const MsInfo& ms, cud
             }
             threads = round_threads(threads);
             const size_t smem = sizeof(C) * (size_t)3 * nb * spad_len(L);
-            set_smem(k_conv<R>, smem);
             dim3 grid((unsigned)ceil_div(nxh(), nb), (unsigned)Py());
-            k_conv<R><<<grid, threads, smem, st>>>(s2, Nr, fp, ip, nz, (int64_t)Py() * pitch_,
-                                                   (int64_t)nz * Py() * pitch_, pitch_, nxh(), nb, 1, ny, nz, nxh());
+            if (pbc_) {
+                set_smem(k_conv<R, true>, smem);
+                k_conv<R, true><<<grid, threads, smem, st>>>(s2, Nr, fp, ip, nz, (int64_t)Py() * pitch_,
+                                                             (int64_t)nz * Py() * pitch_, pitch_, nxh(), nb, 1, ny,
+                                                             nz, nxh(), pop);
+            } else {
+                set_smem(k_conv<R, false>, smem);
+                k_conv<R, false><<<grid, threads, smem, st>>>(s2, Nr, fp, ip, nz, (int64_t)Py() * pitch_,
+                                                              (int64_t)nz * Py() * pitch_, pitch_, nxh(), nb, 1, ny,
+                                                              nz, nxh(), pop);
+            }
             MAF_LAUNCH_CHECK();
         }
         if (marks) marks->mark(st, "z_conv");
         // pass 4: y inverse, S2 -> S1, keep ky rows [0, ny)
         launch_cols<R, 1>(s2, s1, Py(), Py(), ny, nxh(), pitch_, pitch_, (int64_t)Py() * pitch_,
-                          (int64_t)ny * pitch_, 3 * nz, tw_, tune, st);
+                          (int64_t)ny * pitch_, 3 * nz, tw_, tune, st, ct);
         if (marks) marks->mark(st, "y_inv");
     } else {
         // pass 2 (2-D): y forward . tensor . y inverse, in place on S1
-        if (ct_convy<R>(s1, Nr, ny, nxh(), pitch_, tw_, st)) {
+        if (ct && ct_convy<R>(s1, Nr, ny, nxh(), pitch_, tw_, st)) {
             if (marks) marks->mark(st, "y_conv");
             return;
         }
@@ -602,10 +683,16 @@ template <typename R> void Demag::forward_conv(const R* m, const MsInfo& ms, cud
         }
         threads = round_threads(threads);
         const size_t smem = sizeof(C) * (size_t)3 * nb * spad_len(L);
-        set_smem(k_conv<R>, smem);
         dim3 grid((unsigned)ceil_div(nxh(), nb), 1);
-        k_conv<R><<<grid, threads, smem, st>>>(s1, Nr, fp, fp, ny, pitch_, (int64_t)ny * pitch_, 0, nxh(), nb, 0, ny,
-                                               nz, nxh());
+        if (pbc_) {
+            set_smem(k_conv<R, true>, smem);
+            k_conv<R, true><<<grid, threads, smem, st>>>(s1, Nr, fp, fp, ny, pitch_, (int64_t)ny * pitch_, 0, nxh(),
+                                                         nb, 0, ny, nz, nxh(), pop);
+        } else {
+            set_smem(k_conv<R, false>, smem);
+            k_conv<R, false><<<grid, threads, smem, st>>>(s1, Nr, fp, fp, ny, pitch_, (int64_t)ny * pitch_, 0, nxh(),
+                                                          nb, 0, ny, nz, nxh(), pop);
+        }
         MAF_LAUNCH_CHECK();
         if (marks) marks->mark(st, "y_conv");
     }
@@ -617,8 +704,8 @@ template <typename R>
 void Demag::inverse_x_epilogue(const R* m, const MsInfo& ms, const TermList& tl, const EpilogueArgs& ep,
                                cudaStream_t st, int* nblocks_out, PassMarks* marks) {
     const bool f64 = sizeof(R) == 8;
-    const int Lc = md_.nx;
-    {
+    const int Lc = Px() / 2;
+    if (!pbc_) {
         const R scale = (R)(1.0 / ((double)Px() * Py() * Pz()));
         if (ct_xinv<R>(S1<R>(), pitch_, Px(), tw_, md_.geom(), scale, m, ms, tl, ep, tune, st, nblocks_out)) {
             if (marks) marks->mark(st, "x_inv_local");
@@ -688,6 +775,11 @@ void eval_terms(const std::vector<Term*>& terms, const MeshDims& md, const R* m,
     for (Term* t : terms) {
         if (t->kind == TK_DEMAG) {
             if (demag) throw Error(1, "at most one DemagField per term list");
+            if (t->demag_pbc() && !(t->demag && t->demag_mesh == md)) {
+                // DemagFieldPBC takes its mesh from the state: plan it on first use
+                t->demag = std::make_unique<Demag>(md, st, nullptr, true);
+                t->demag_mesh = md;
+            }
             if (!(t->demag_mesh == md)) throw Error(1, "DemagField mesh differs from the state's mesh");
             demag = t->demag.get();
         }

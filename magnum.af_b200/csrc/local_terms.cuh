@@ -28,6 +28,7 @@ enum TermKind : int {
     TK_CUBIC = 5,
     TK_ZEEMAN = 6,
     TK_STT = 7,
+    TK_SPARSE_EXCH = 8,
 };
 
 constexpr int kMaxTerms = 8;
@@ -159,6 +160,60 @@ __device__ __forceinline__ void cubic_h123_sum(const TermDesc& t, const R mc[3],
     for (int i = 0; i < 3; ++i) h[i] = h1[i] + h2[i] + h3[i];
 }
 
+// SparseExchangeField / ExchangeFieldPBC for one cell: H = (M m)_cell / Ms with
+// the 7-point matrix M those terms assemble (sparse_exchange_field.cpp:8-18,
+// exchange_field_pbc.cpp:9-19).  p[0] = scalar A, p[1] != 0 for periodic
+// neighbours, f0 = optional A field [N].
+//   scalar A, open boundary: each neighbour inside the mesh weighs 2A/mu0/d^2
+//     and the row has no diagonal (sparse_exchange_field.cpp:25-101);
+//   A field or periodic: neighbour weight lapA = 2A_i/(mu0 d^2) * 2A_nb/(A_nb + A_i)
+//     (sparse_exchange_field.cpp:183-185), diagonal = minus their sum, rows of
+//     cells with A_i = 0 empty (:189-270; periodic wrap exchange_field_pbc.cpp:60-80).
+// A row with a diagonal is evaluated as sum_nb w (m_nb - m_c): the same value,
+// exactly zero for a uniform m.  The weights are formed in FP64 as assembled.
+template <typename R>
+__device__ __forceinline__ void sparse_exchange_add(const TermDesc& t, const R* __restrict__ m, const Geom& g, int x,
+                                                    int y, int z, int64_t cell, const R mc[3], R Ms, R h[3]) {
+    const bool periodic = t.p[1] != 0.0;
+    const bool diag = periodic || t.f0 != nullptr;
+    const double Ai = t.f0 ? t.f0[cell] : t.p[0];
+    if (diag && Ai == 0.0) return;
+    R acc[3] = {0, 0, 0};
+    auto nb = [&](int xx, int yy, int zz, double d) {
+        const int64_t j = ((int64_t)zz * g.ny + yy) * g.nx + xx;
+        double w;
+        if (diag) {
+            const double Aj = t.f0 ? t.f0[j] : t.p[0];
+            w = 2.0 * Ai / (kMu0 * (d * d)) * 2.0 * Aj / (Aj + Ai);
+        } else {
+            w = 2.0 * Ai / kMu0 / (d * d);
+        }
+        const R wr = (R)w;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const R v = m[c * g.N + j];
+            acc[c] += diag ? wr * (v - mc[c]) : wr * v;
+        }
+    };
+    if (periodic) {
+        nb(x + 1 == g.nx ? 0 : x + 1, y, z, g.dx);
+        nb(x == 0 ? g.nx - 1 : x - 1, y, z, g.dx);
+        nb(x, y + 1 == g.ny ? 0 : y + 1, z, g.dy);
+        nb(x, y == 0 ? g.ny - 1 : y - 1, z, g.dy);
+        nb(x, y, z + 1 == g.nz ? 0 : z + 1, g.dz);
+        nb(x, y, z == 0 ? g.nz - 1 : z - 1, g.dz);
+    } else {
+        if (x < g.nx - 1) nb(x + 1, y, z, g.dx);
+        if (x > 0) nb(x - 1, y, z, g.dx);
+        if (y < g.ny - 1) nb(x, y + 1, z, g.dy);
+        if (y > 0) nb(x, y - 1, z, g.dy);
+        if (z < g.nz - 1) nb(x, y, z + 1, g.dz);
+        if (z > 0) nb(x, y, z - 1, g.dz);
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) h[c] += acc[c] / Ms;
+}
+
 // Adds the field of local term `t` at cell (x,y,z) to h.  Ms is the cell's
 // saturation magnetisation (the scalar Ms or Ms_field[cell]).
 template <typename R>
@@ -268,6 +323,12 @@ __device__ __forceinline__ void add_local_term(const TermDesc& t, const R* __res
             h[0] += coef * (ed * (mc[1] * p2 - mc[2] * p1) + ef * p0);
             h[1] += coef * (ed * (mc[2] * p0 - mc[0] * p2) + ef * p1);
             h[2] += coef * (ed * (mc[0] * p1 - mc[1] * p0) + ef * p2);
+            break;
+        }
+        case TK_SPARSE_EXCH: {
+            // zero where Ms = 0 (the af::replace of sparse_exchange_field.cpp:15)
+            if (ms_is_field && Ms == (R)0) return;
+            sparse_exchange_add(t, m, g, x, y, z, cell, mc, Ms, h);
             break;
         }
         case TK_ZEEMAN: {

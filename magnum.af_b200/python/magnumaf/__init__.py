@@ -70,6 +70,9 @@ _SIGS = {
     "maf_term_external_create": (_I, [C.POINTER(_P), _I, _I, _I, _DP]),
     "maf_term_external_uniform_create": (_I, [C.POINTER(_P), _D, _D, _D]),
     "maf_term_stt_create": (_I, [C.POINTER(_P), _I, _I, _I, _DP, _D, _D, _D, _D]),
+    "maf_term_sparse_exchange_create": (_I, [C.POINTER(_P), _I, _I, _I, _DP, _D]),
+    "maf_term_demag_pbc_create": (_I, [C.POINTER(_P)]),
+    "maf_term_exchange_pbc_create": (_I, [C.POINTER(_P), _I, _I, _I, _DP, _D]),
     "maf_term_destroy": (_I, [_P]),
     "maf_term_H": (_I, [_P, _P, _DP]),
     "maf_term_H_f32": (_I, [_P, _P, _FP]),
@@ -479,11 +482,63 @@ class DemagField(FieldTerm):
         return out.transpose(3, 2, 1, 0)
 
 
+class DemagFieldPBC(FieldTerm):
+    """DemagFieldPBC() (python/magnumaf.pyx:1123-1140, demag_field_pbc.cpp):
+    periodic demag through the scalar potential; the mesh is the evaluated
+    state's (nx must be even)."""
+
+    def __init__(self):
+        self._h = _P()
+        _ck(lib.maf_term_demag_pbc_create(C.byref(self._h)))
+
+
+def _sparse_exchange(term, A, mesh, create, who):
+    if mesh is None:
+        raise MafError(1, who + ": a mesh is required")
+    term._h = _P()
+    if np.ndim(A) == 0:
+        term.A = float(A)
+        _ck(create(C.byref(term._h), mesh.nx, mesh.ny, mesh.nz, None, term.A))
+    else:
+        a = _scalar_soa(A)
+        if a.shape != (mesh.nx, mesh.ny, mesh.nz):
+            raise MafError(1, "%s: A field of shape %s on a %dx%dx%d mesh"
+                           % (who, a.shape, mesh.nx, mesh.ny, mesh.nz))
+        term.A = None
+        _ck(create(C.byref(term._h), mesh.nx, mesh.ny, mesh.nz, _dptr(a), 0.0))
+
+
 class ExchangeField(FieldTerm):
+    """ExchangeField(A) is the zero-padded Laplacian (exchange_field.cpp); with a
+    mesh, ExchangeField(A, mesh) and ExchangeField(A_field, mesh) are the sparse
+    matrix form of SparseExchangeField (python/magnumaf.pyx:1172-1195)."""
+
     def __init__(self, A, mesh: Mesh = None, verbose=False):
+        if mesh is not None:
+            _sparse_exchange(self, A, mesh, lib.maf_term_sparse_exchange_create, "ExchangeField")
+            return
+        if np.ndim(A) != 0:
+            raise MafError(1, "When passing A as an array, you must provide a mesh, "
+                                           "i.e. ExchangeField(A, mesh).")
         self.A = float(A)
         self._h = _P()
         _ck(lib.maf_term_exchange_create(C.byref(self._h), self.A))
+
+
+class SparseExchangeField(FieldTerm):
+    """SparseExchangeField(A, mesh) with a scalar or cell-wise A
+    (sparse_exchange_field.cpp:8-18,25-330)."""
+
+    def __init__(self, A, mesh: Mesh, verbose=False):
+        _sparse_exchange(self, A, mesh, lib.maf_term_sparse_exchange_create, "SparseExchangeField")
+
+
+class ExchangeFieldPBC(FieldTerm):
+    """ExchangeFieldPBC(A, mesh): exchange with periodic boundaries in x, y and z
+    (exchange_field_pbc.cpp:9-225)."""
+
+    def __init__(self, A, mesh: Mesh, verbose=False):
+        _sparse_exchange(self, A, mesh, lib.maf_term_exchange_pbc_create, "ExchangeFieldPBC")
 
 
 class DmiField(FieldTerm):

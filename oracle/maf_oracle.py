@@ -645,6 +645,121 @@ class SpinTransferTorqueField(FieldTerm):
         return _replace_ms_zero(np.nan_to_num(h, nan=0.0, posinf=0.0, neginf=0.0), state)
 
 
+def exchange_matrix(mesh, A, A_field=None, periodic=False):
+    """One component block (N x N, cell index i0 + nx*(i1 + ny*i2)) of the 3N x 3N
+    exchange matrix of SparseExchangeField / ExchangeFieldPBC, assembled as COO
+    triplets and summed into CSR like the reference:
+      scalar A, open (sparse_exchange_field.cpp:25-101): neighbours inside the
+        mesh in the order +x,-x,+y,-y,+z,-z, value (2A)/mu0/d^2, no diagonal;
+      A field (sparse_exchange_field.cpp:289-330) or periodic
+        (exchange_field_pbc.cpp:126-163): value lapA(A_i, A_nb, d) =
+        2A_i/(mu0 d^2) * 2A_nb/(A_nb+A_i) (sparse_exchange_field.cpp:183-185),
+        periodic neighbours wrapped (i+n) % n, then the diagonal -sum; rows of
+        cells with A_i = 0 are left empty.
+    The three component blocks of the reference's matrix are identical."""
+    import scipy.sparse as sp
+
+    nx, ny, nz = mesh.nx, mesh.ny, mesh.nz
+    N = nx * ny * nz
+    i0, i1, i2 = np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing="ij")
+    row = (i0 + nx * (i1 + ny * i2)).reshape(-1, order="F")
+    Af = np.full((nx, ny, nz), float(A)) if A_field is None else np.asarray(A_field, dtype=np.float64)
+    Ai = Af.reshape(-1, order="F")
+    harmonic = periodic or A_field is not None
+    rows, cols, vals = [], [], []
+    m_self = np.zeros(N)
+    dirs = [(0, 1, mesh.dx), (0, -1, mesh.dx), (1, 1, mesh.dy), (1, -1, mesh.dy), (2, 1, mesh.dz), (2, -1, mesh.dz)]
+    for axis, s, d in dirs:
+        idx = [i0, i1, i2]
+        n = (nx, ny, nz)[axis]
+        j = idx[axis] + s
+        if periodic:
+            j = (j + n) % n
+            valid = np.ones_like(j, dtype=bool)
+        else:
+            valid = (j >= 0) & (j < n)
+        idx[axis] = np.where(valid, j, 0)
+        nb = (idx[0] + nx * (idx[1] + ny * idx[2])).reshape(-1, order="F")
+        valid = valid.reshape(-1, order="F")
+        if harmonic:
+            Anb = Ai[nb]
+            with np.errstate(divide="ignore", invalid="ignore"):
+                w = 2.0 * Ai / (mu0 * d ** 2) * 2.0 * Anb / (Anb + Ai)
+            keep = valid & (Ai != 0.0)
+            m_self[keep] -= w[keep]
+        else:
+            w = np.full(N, (2.0 * float(A)) / mu0 / d ** 2)
+            keep = valid
+        rows.append(row[keep])
+        cols.append(nb[keep])
+        vals.append(w[keep])
+    if harmonic:
+        keep = Ai != 0.0
+        rows.append(row[keep])
+        cols.append(row[keep])
+        vals.append(m_self[keep])
+    coo = sp.coo_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))), shape=(N, N))
+    return coo.tocsr()
+
+
+class SparseExchangeField(FieldTerm):
+    """sparse_exchange_field.cpp:8-18: H = matr * flat(m) / Ms, zero where
+    Ms_field == 0; default micro energy (micro_term.hpp:18)."""
+
+    periodic = False
+
+    def __init__(self, A, mesh):
+        if np.ndim(A) == 0:
+            self.matr = exchange_matrix(mesh, float(A), None, self.periodic)
+        else:
+            self.matr = exchange_matrix(mesh, 0.0, np.asarray(A, dtype=np.float64), self.periodic)
+
+    def H_in_Apm(self, state):
+        m = state.m
+        exch = np.stack([(self.matr @ m[..., c].reshape(-1, order="F")).reshape(m.shape[:3], order="F")
+                         for c in range(3)], axis=3)
+        with np.errstate(divide="ignore", invalid="ignore"):
+            h = exch * _inv_Ms(state)
+        return _replace_ms_zero(h, state)
+
+
+class ExchangeFieldPBC(SparseExchangeField):
+    """exchange_field_pbc.cpp:9-19: the harmonic-mean matrix with periodic
+    neighbours in x, y and z."""
+
+    periodic = True
+
+
+class DemagFieldPBC(FieldTerm):
+    """demag_field_pbc.cpp:10-71: periodic demag through the scalar potential on
+    the mesh's own grid.  R2C of Ms*m (x halved), K_a = 2 pi k_a / n_a,
+    div = sum_a (1 - exp(-i K_a)) M_a / d_a, u = -div / sum_a 4/d_a^2 sin^2(K_a/2)
+    with u(0,0,0) = 0, H_a = (1 - exp(i K_a)) u / d_a, then C2R with the 1/N
+    normalisation (the fftC2R default).  The C2R returns 2*(nx//2) columns
+    (is_odd = false), so only even nx gives the mesh's shape."""
+
+    def H_in_Apm(self, state):
+        mesh = state.mesh
+        nx, ny, nz = mesh.nx, mesh.ny, mesh.nz
+        if nx % 2:
+            raise ValueError("DemagFieldPBC: nx must be even")
+        ms = state.Ms if state.Ms_field is None else state.Ms_field[..., None]
+        M = np.fft.rfftn(ms * state.m, axes=(1, 2, 0))  # real transform along x
+        kx = (2.0 * math.pi * np.arange(nx // 2 + 1) / nx)[:, None, None]
+        ky = (2.0 * math.pi * np.arange(ny) / ny)[None, :, None]
+        kz = (2.0 * math.pi * np.arange(nz) / nz)[None, None, :]
+        div = ((1.0 - np.exp(-1j * kx)) * M[..., 0] / mesh.dx + (1.0 - np.exp(-1j * ky)) * M[..., 1] / mesh.dy
+               + (1.0 - np.exp(-1j * kz)) * M[..., 2] / mesh.dz)
+        den = (4.0 / mesh.dx ** 2 * np.sin(kx / 2.0) ** 2 + 4.0 / mesh.dy ** 2 * np.sin(ky / 2.0) ** 2
+               + 4.0 / mesh.dz ** 2 * np.sin(kz / 2.0) ** 2)
+        with np.errstate(divide="ignore", invalid="ignore"):
+            u = -div / den
+        u[0, 0, 0] = 0.0
+        h = np.stack([(1.0 - np.exp(1j * kx)) * u / mesh.dx, (1.0 - np.exp(1j * ky)) * u / mesh.dy,
+                      (1.0 - np.exp(1j * kz)) * u / mesh.dz], axis=3)
+        return np.fft.irfftn(h, s=(ny, nz, nx), axes=(1, 2, 0))
+
+
 def Heff_in_Apm(terms: Sequence[FieldTerm], state):
     """sequential_Heff_in_Apm, field_term.hpp:116-119."""
     h = terms[0].H_in_Apm(state)
