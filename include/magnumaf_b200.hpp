@@ -236,6 +236,64 @@ class ExternalField : public FieldTerm {
     }
 };
 
+// DemagFieldPBC() (demag_field_pbc.cpp): the mesh is the evaluated state's
+class DemagFieldPBC : public FieldTerm {
+  public:
+    DemagFieldPBC() {
+        maf_term t = nullptr;
+        maf_check(maf_term_demag_pbc_create(&t));
+        reset(t);
+    }
+};
+
+// SparseExchangeField(A, mesh) / (A_field, mesh) (sparse_exchange_field.cpp); A_field is [nz][ny][nx]
+class SparseExchangeField : public FieldTerm {
+  public:
+    SparseExchangeField(double A, Mesh mesh, bool /*verbose*/ = true) {
+        maf_term t = nullptr;
+        maf_check(maf_term_sparse_exchange_create(&t, (int)mesh.nx, (int)mesh.ny, (int)mesh.nz, nullptr, A));
+        reset(t);
+    }
+    SparseExchangeField(const HostArray& A_field, Mesh mesh, bool /*verbose*/ = true) {
+        if (A_field.size() != mesh.n())
+            throw std::invalid_argument("SparseExchangeField: size does not match the mesh");
+        maf_term t = nullptr;
+        maf_check(maf_term_sparse_exchange_create(&t, (int)mesh.nx, (int)mesh.ny, (int)mesh.nz, A_field.data(), 0.0));
+        reset(t);
+    }
+};
+
+// ExchangeFieldPBC(A, mesh) / (A_field, mesh) (exchange_field_pbc.cpp)
+class ExchangeFieldPBC : public FieldTerm {
+  public:
+    ExchangeFieldPBC(double A, Mesh mesh, bool /*verbose*/ = true) {
+        maf_term t = nullptr;
+        maf_check(maf_term_exchange_pbc_create(&t, (int)mesh.nx, (int)mesh.ny, (int)mesh.nz, nullptr, A));
+        reset(t);
+    }
+    ExchangeFieldPBC(const HostArray& A_field, Mesh mesh, bool /*verbose*/ = true) {
+        if (A_field.size() != mesh.n()) throw std::invalid_argument("ExchangeFieldPBC: size does not match the mesh");
+        maf_term t = nullptr;
+        maf_check(maf_term_exchange_pbc_create(&t, (int)mesh.nx, (int)mesh.ny, (int)mesh.nz, A_field.data(), 0.0));
+        reset(t);
+    }
+};
+
+// SpinTransferTorqueField(polarization, eta_damping, eta_field, j_e, fl_thickness)
+// (spin_transfer_torque_field.cpp); polarization is [3][nz][ny][nx]
+class SpinTransferTorqueField : public FieldTerm {
+  public:
+    SpinTransferTorqueField(const Mesh& mesh, const HostArray& polarization, double eta_damping, double eta_field,
+                            double j_e, double fl_thickness) {
+        if (polarization.size() != 3 * mesh.n())
+            throw std::invalid_argument("SpinTransferTorqueField: size does not match the mesh");
+        maf_term t = nullptr;
+        maf_check(maf_term_stt_create(&t, (int)mesh.nx, (int)mesh.ny, (int)mesh.nz, polarization.data(), eta_damping,
+                                      eta_field, j_e, fl_thickness));
+        reset(t);
+    }
+};
+
 using uptr_FieldTerm = std::unique_ptr<FieldTerm>;
 using vec_uptr_FieldTerm = std::vector<uptr_FieldTerm>;
 
