@@ -11,9 +11,13 @@ the unit sphere.  Inputs are synthetic and seeded.
 value      FP32-field form, H_eff evals/s with m resident in HBM (the field pipeline
            alone), summed over all ranks (independent replicas, "weak" scaling).
 e2e        the same metric through the public C ABI with host buffers: every step
-           copies m (FP64) host->device from pinned memory and H (FP32) back.
+           copies m (FP32; FP64 in fp64_m_value) host->device from pinned memory
+           and H (FP32) back.
 fp64_form  the FP64 form on the same mesh; rel_err_fp32_vs_fp64 checks the metric's
-           condition (FP32-field error <= 1e-5 relative to the FP64 form).
+           condition (FP32-field error <= 1e-5 relative to the FP64 form), also per
+           field term and for the component of H perpendicular to m.
+trajectory 5 ps of DP45 with dense output of <m> in both forms: simulated ns per
+           hour and the largest <m> difference between the forms.
 roofline   the dominant pass: algorithmic bytes per launch / its mean CUDA-event
            duration, against the measured HBM copy bandwidth.
 --impl reference  the FP64 CPU oracle (the reference algorithm restated in NumPy/SciPy)
@@ -42,6 +46,7 @@ DX = 3e-9
 MS = 8.6e5
 A_EX = 1.3e-11
 K1 = -1.0e4
+TRAJ_T = 5e-12  # simulated time of the reported trajectory
 SEED = 1234
 MU0 = 4e-7 * math.pi
 
@@ -309,6 +314,48 @@ def run_ours(args):
     rel_err = float(torch.linalg.vector_norm(d) / torch.linalg.vector_norm(H64))
     rel_max = float(d.abs().max() / H64.abs().max())
 
+    # the same error per field term (each term alone), and for the torque-relevant
+    # component of H perpendicular to m (the exchange self term, parallel to m,
+    # inflates |H| but exerts no torque)
+    per_term = {}
+    m3 = m64_dev.view(3, -1)
+    for name, term in zip(("demag", "exchange", "cubic", "zeeman"), terms):
+        one = M.LLGIntegrator(0.01, [term], "DP45")
+        with torch.cuda.stream(stream):
+            one.heff_device(s32, m32_dev.data_ptr(), H32.data_ptr())
+            one.heff_device(s64, m64_dev.data_ptr(), H64.data_ptr())
+        torch.cuda.synchronize()
+        h32, h64 = H32.double().view(3, -1), H64.view(3, -1)
+        p32 = h32 - (h32 * m3).sum(0, keepdim=True) * m3
+        p64 = h64 - (h64 * m3).sum(0, keepdim=True) * m3
+        nrm = float(torch.linalg.vector_norm(h64))
+        per_term[name] = {
+            "l2": float(torch.linalg.vector_norm(h32 - h64)) / nrm if nrm else 0.0,
+            "torque_l2": float(torch.linalg.vector_norm(p32 - p64) / torch.linalg.vector_norm(p64)),
+        }
+        del one
+
+    # a short trajectory in both forms: DP45 with dense output of <m> (RKF45
+    # back-steps), simulated ns per hour of wall time and the largest <m>
+    # difference between the forms over the samples
+    traj = {}
+    if not args.no_trajectory:
+        rows = {}
+        for prec in ("fp32_field", "fp64"):
+            st = M.State(mesh, MS, m, precision=prec)
+            st.set_stream(stream.cuda_stream)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            rows[prec] = llg.integrate_dense(st, TRAJ_T, TRAJ_T / 10)
+            wall = time.perf_counter() - t0
+            traj[prec] = {"sim_ns_per_hour": TRAJ_T * 1e9 / wall * 3600.0, "wall_s": wall, "steps": st.steps}
+            del st
+        n_rows = min(len(rows["fp32_field"]), len(rows["fp64"]))
+        traj["mean_m_max_abs_diff"] = float(np.abs(rows["fp32_field"][:n_rows, 1:]
+                                                   - rows["fp64"][:n_rows, 1:]).max())
+        traj["t_sim_s"] = TRAJ_T
+        traj["scheme"] = "DP45 (alpha 0.01, default controller), <m> sampled every %g s" % (TRAJ_T / 10)
+
     # per-pass timing (CUDA events between the pass kernels on the launching stream)
     passes = {}
     nprof = max(3, min(args.steps, 10))
@@ -338,23 +385,32 @@ def run_ours(args):
     ms_e2e_serial = timed(e2e_step, e2e_steps, max(1, min(args.warmup, 3)))
 
     # the same through the pipelined call: every step still copies its m in from
-    # pinned memory and its H out, overlapped with the neighbouring evaluations
-    m_bufs = [m_host, torch.from_numpy(m_norm.copy()).pin_memory()]
+    # pinned memory and its H out, overlapped with the neighbouring evaluations.
+    # The headline e2e passes m in FP32 (the field form's input precision; the
+    # reference's f32 State path), the FP64-input figure is reported beside it.
     H_bufs = [H_host, torch.empty(n3, dtype=torch.float32).pin_memory()]
+    m_bufs64 = [m_host, torch.from_numpy(m_norm.copy()).pin_memory()]
+    m_bufs32 = [torch.from_numpy(m_norm.astype(np.float32)).pin_memory() for _ in range(2)]
 
-    def pipe(n):
-        llg.heff_pipeline(s32, [m_bufs[i % 2].data_ptr() for i in range(n)],
-                          [H_bufs[i % 2].data_ptr() for i in range(n)])
+    def pipe(n, f32_in):
+        bufs = m_bufs32 if f32_in else m_bufs64
+        llg.heff_pipeline(s32, [bufs[i % 2].data_ptr() for i in range(n)],
+                          [H_bufs[i % 2].data_ptr() for i in range(n)], m_float32=f32_in)
 
-    pipe(2)  # allocates the double buffers
-    barrier()
-    t0 = time.perf_counter()
-    pipe(e2e_steps)
-    ms_e2e = (time.perf_counter() - t0) * 1e3
-    if dist:
-        t = torch.tensor([ms_e2e], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_e2e = float(t.item())
+    def timed_pipe(f32_in):
+        pipe(2, f32_in)  # allocates the double buffers
+        barrier()
+        t0 = time.perf_counter()
+        pipe(e2e_steps, f32_in)
+        ms = (time.perf_counter() - t0) * 1e3
+        if dist:
+            t = torch.tensor([ms], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms
+
+    ms_e2e = timed_pipe(True)
+    ms_e2e64 = timed_pipe(False)
 
     npass = len(pass_ms)
     value = world * args.steps / (ms32 * 1e-3)
@@ -378,15 +434,17 @@ def run_ours(args):
                    "tune": None if tune is None else {k: tune[k] for k in ("cols_wide", "convz_reg", "xinv_run")}},
         "fp64_form": {"value": world * args.steps / (ms64 * 1e-3), "ms_per_step": ms64 / args.steps,
                       "fp32_speedup": ms64 / ms32},
-        "rel_err_fp32_vs_fp64": {"l2": rel_err, "max": rel_max},
+        "rel_err_fp32_vs_fp64": {"l2": rel_err, "max": rel_max, "per_term": per_term},
+        "trajectory": traj,
         "passes_ms": pass_ms,
         "eval_roofline": {"bytes": eval_bytes, "achieved_gbs": eval_gbs, "frac": eval_gbs / peak},
         "roofline": {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
                      "algorithmic_bytes": bytes32[dominant]},
-        "e2e": {"value": world * e2e_steps / (ms_e2e * 1e-3), "unit": "evals/s", "h2d_bytes_per_step": n3 * 8,
+        "e2e": {"value": world * e2e_steps / (ms_e2e * 1e-3), "unit": "evals/s", "h2d_bytes_per_step": n3 * 4,
                 "d2h_bytes_per_step": n3 * 4,
-                "path": "LLGIntegrator.heff_pipeline over pinned host buffers (copies overlapped)",
+                "path": "LLGIntegrator.heff_pipeline(m_float32=True) over pinned host buffers (copies overlapped)",
+                "fp64_m_value": world * e2e_steps / (ms_e2e64 * 1e-3), "fp64_m_h2d_bytes_per_step": n3 * 8,
                 "serial_value": world * e2e_steps / (ms_e2e_serial * 1e-3)},
         "gpu_launches": npass * args.steps,
         "clocks": clocks,
@@ -411,6 +469,7 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--no-trajectory", action="store_true", help="skip the short DP45 trajectory")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default kernel variants")

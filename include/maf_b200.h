@@ -186,6 +186,10 @@ int maf_llg_heff_device(maf_llg l, maf_state s, const void* m_dev, void* H_dev);
  * pinned host memory for full link bandwidth).  The state keeps the last m.  No counterpart in the
  * reference beyond calling H_in_Apm n times. */
 int maf_llg_heff_pipeline(maf_llg l, maf_state s, const double* const* m_host, void* const* H_host, int n);
+/* maf_llg_heff_pipeline with FP32 host magnetisations (the reference's f32 State arrays; the field of an
+ * f32 m is the FP32 form's, demag_field.cpp:217-221): half the host->device bytes; each m is widened to
+ * FP64 on the device (exactly) before the same normalisation. */
+int maf_llg_heff_pipeline_m32(maf_llg l, maf_state s, const float* const* m_host, void* const* H_host, int n);
 /* Autotuner (no counterpart in the reference): the compile-time passes have two kernel variants each --
  * y-pass column tile (choices[0]: 0 default, 1 doubled), z convolution (choices[1]: 1 transforms in
  * registers, 0 shared-memory stages), x-inverse epilogue run length (choices[2]: 2 or 4 cells, 0 = the

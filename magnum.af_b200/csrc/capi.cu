@@ -183,7 +183,7 @@ int mafb::capi_run(const std::function<void()>& f) {
 // ---------------------------------------------------------------------------
 // Buffers and streams of the pipelined evaluation (maf_llg_heff_pipeline).
 struct HeffPipe {
-    DevBuf m[2], h[2], m32;
+    DevBuf m[2], h[2], m32, m_in32[2];  // m_in32: FP32 host inputs (maf_llg_heff_pipeline_m32)
     cudaStream_t up = nullptr, down = nullptr;
     cudaEvent_t up_done[2] = {}, comp_done[2] = {}, down_done[2] = {};
     ~HeffPipe() {
@@ -1412,8 +1412,10 @@ int maf_llg_heff_f32(maf_llg l, maf_state s, float* H) {
 // m[i+1] to the device, the evaluation of m[i] and the copy of H[i-1] to the
 // host run on three streams with double-buffered device buffers, so the host
 // link carries both directions while the field is computed.
-int maf_llg_heff_pipeline(maf_llg l, maf_state s, const double* const* m_host, void* const* H_host, int n) {
-    return guarded([&] {
+// m_host holds FP64 inputs, or FP32 inputs when m_f32 (widened on the device,
+// exactly, before the same normalisation).
+static void heff_pipeline(maf_llg l, maf_state s, const void* const* m_host, bool m_f32, void* const* H_host, int n) {
+    {
         check_llg_state(l, s);
         check(n >= 0 && (n == 0 || (m_host && H_host)), "maf_llg_heff_pipeline: bad argument");
         StateD& st = s->s;
@@ -1435,6 +1437,8 @@ int maf_llg_heff_pipeline(maf_llg l, maf_state s, const double* const* m_host, v
             s->pipe = std::move(p);
         }
         HeffPipe& p = *s->pipe;
+        if (m_f32)
+            for (int b = 0; b < 2; ++b) p.m_in32[b].ensure(sizeof(float) * n3);
         const auto terms = raw_terms(l->terms);
         MAF_CUDA(cudaStreamSynchronize(st.stream));
         for (int i = 0; i < n; ++i) {
@@ -1442,11 +1446,15 @@ int maf_llg_heff_pipeline(maf_llg l, maf_state s, const double* const* m_host, v
             check(m_host[i] && H_host[i], "maf_llg_heff_pipeline: NULL buffer");
             // host -> device, once the evaluation two steps back has released m[b]
             MAF_CUDA(cudaStreamWaitEvent(p.up, p.comp_done[b], 0));
-            MAF_CUDA(cudaMemcpyAsync(p.m[b].p, m_host[i], sizeof(double) * n3, cudaMemcpyHostToDevice, p.up));
+            if (m_f32)
+                MAF_CUDA(cudaMemcpyAsync(p.m_in32[b].p, m_host[i], sizeof(float) * n3, cudaMemcpyHostToDevice, p.up));
+            else
+                MAF_CUDA(cudaMemcpyAsync(p.m[b].p, m_host[i], sizeof(double) * n3, cudaMemcpyHostToDevice, p.up));
             MAF_CUDA(cudaEventRecord(p.up_done[b], p.up));
             // normalise (as maf_state_set_m) and evaluate once H[b] has gone to the host
             MAF_CUDA(cudaStreamWaitEvent(st.stream, p.up_done[b], 0));
             MAF_CUDA(cudaStreamWaitEvent(st.stream, p.down_done[b], 0));
+            if (m_f32) widen_m(p.m_in32[b].as<float>(), p.m[b].as<double>(), n3, st.stream);
             normalize_m(p.m[b].as<double>(), N, 2, nullptr, st.stream);
             EpilogueArgs ep;
             ep.kind = EPI_H;
@@ -1472,7 +1480,15 @@ int maf_llg_heff_pipeline(maf_llg l, maf_state s, const double* const* m_host, v
         MAF_CUDA(cudaStreamSynchronize(p.down));
         MAF_CUDA(cudaStreamSynchronize(p.up));
         MAF_CUDA(cudaStreamSynchronize(st.stream));
-    });
+    }
+}
+
+int maf_llg_heff_pipeline(maf_llg l, maf_state s, const double* const* m_host, void* const* H_host, int n) {
+    return guarded([&] { heff_pipeline(l, s, reinterpret_cast<const void* const*>(m_host), false, H_host, n); });
+}
+
+int maf_llg_heff_pipeline_m32(maf_llg l, maf_state s, const float* const* m_host, void* const* H_host, int n) {
+    return guarded([&] { heff_pipeline(l, s, reinterpret_cast<const void* const*>(m_host), true, H_host, n); });
 }
 
 int maf_llg_heff_device(maf_llg l, maf_state s, const void* m_dev, void* H_dev) {

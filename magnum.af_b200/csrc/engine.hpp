@@ -227,6 +227,7 @@ void eval_terms(const std::vector<Term*>& terms, const MeshDims& md, const R* m,
 
 // FP64 -> FP32 staging of m
 void stage_m32(const double* m64, float* m32, int64_t n, cudaStream_t st);
+void widen_m(const float* m32, double* m64, int64_t n, cudaStream_t st);  // FP32 -> FP64, exact
 
 // Newell tensor on the padded grid, one component [Pz][Py][Px] (newell.cu);
 // symmetric = true gives the parity-exact tensor the spectral pipeline uses.

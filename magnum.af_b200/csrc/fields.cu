@@ -405,6 +405,17 @@ __global__ void k_stage32(const double* __restrict__ a, float* __restrict__ b, i
         b[i] = (float)a[i];
 }
 
+__global__ void k_widen(const float* __restrict__ a, double* __restrict__ b, int64_t n) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        b[i] = (double)a[i];
+}
+
+void widen_m(const float* m32, double* m64, int64_t n, cudaStream_t st) {
+    const int64_t blocks = std::min<int64_t>(ceil_div(n, 256), 148LL * 16);
+    k_widen<<<(unsigned)blocks, 256, 0, st>>>(m32, m64, n);
+    MAF_LAUNCH_CHECK();
+}
+
 void stage_m32(const double* m64, float* m32, int64_t n, cudaStream_t st) {
     const int64_t blocks = std::min<int64_t>(ceil_div(n, 256), 148LL * 16);
     k_stage32<<<(unsigned)blocks, 256, 0, st>>>(m64, m32, n);

@@ -90,6 +90,7 @@ _SIGS = {
     "maf_llg_heff_f32": (_I, [_P, _P, _FP]),
     "maf_llg_heff_device": (_I, [_P, _P, _P, _P]),
     "maf_llg_heff_pipeline": (_I, [_P, _P, C.POINTER(_P), C.POINTER(_P), _I]),
+    "maf_llg_heff_pipeline_m32": (_I, [_P, _P, C.POINTER(_P), C.POINTER(_P), _I]),
     "maf_llg_autotune": (_I, [_P, _P, _I, C.POINTER(_I), _DP]),
     "maf_term_demag_get_tune": (_I, [_P, C.POINTER(_I)]),
     "maf_term_demag_set_tune": (_I, [_P, C.POINTER(_I)]),
@@ -758,16 +759,18 @@ class LLGIntegrator:
         return {"cols_wide": ch[0], "convz_reg": ch[1], "xinv_run": ch[2], "pass_ms_default": ms[:5].tolist(),
                 "pass_ms_alternative": ms[5:].tolist()}
 
-    def heff_pipeline(self, state: State, m_host_ptrs, H_host_ptrs):
+    def heff_pipeline(self, state: State, m_host_ptrs, H_host_ptrs, m_float32: bool = False):
         """Fields of several host magnetisations in a row, host copies overlapped
         with the evaluations (pass pinned buffers): m_host_ptrs[i] -> H_host_ptrs[i]
-        (addresses of double [3][N] inputs and of float/double [3][N] outputs)."""
+        (addresses of double [3][N] inputs -- float [3][N] with m_float32 -- and of
+        float/double [3][N] outputs)."""
         n = len(m_host_ptrs)
         if len(H_host_ptrs) != n:
             raise ValueError("as many outputs as inputs")
         mp = (_P * max(n, 1))(*[C.c_void_p(p) for p in m_host_ptrs])
         hp = (_P * max(n, 1))(*[C.c_void_p(p) for p in H_host_ptrs])
-        _ck(lib.maf_llg_heff_pipeline(self._h, state._h, mp, hp, n))
+        fn = lib.maf_llg_heff_pipeline_m32 if m_float32 else lib.maf_llg_heff_pipeline
+        _ck(fn(self._h, state._h, mp, hp, n))
 
     def heff_device_profile(self, state: State, m_dev_ptr: int, H_dev_ptr: int):
         """One field evaluation with per-pass CUDA-event timing: [(name, ms), ...]."""

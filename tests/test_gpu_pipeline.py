@@ -32,3 +32,24 @@ def test_pipeline_equals_single_calls(precision):
     for o, r in zip(outs, ref):
         assert np.array_equal(o, np.asarray(r).ravel(order="F"))
     np.testing.assert_array_equal(np.asarray(s.m), np.asarray(M.State(mesh, 8.6e5, ms[-1]).m))
+
+
+@pytest.mark.parametrize("precision", ["fp32_field", "fp64"])
+def test_pipeline_with_float32_inputs(precision):
+    """maf_llg_heff_pipeline_m32: FP32 host magnetisations give exactly the fields
+    of the same values passed in FP64 (the widening is exact)."""
+    shape = (32, 24, 4)
+    mesh = M.Mesh(*shape, 3e-9, 3e-9, 3e-9)
+    llg = M.LLGIntegrator(0.01, [M.DemagField(mesh), M.ExchangeField(1.3e-11)], "DP45")
+    ms = [random_m(shape, 60 + i).astype(np.float32) for i in range(3)]
+    s = M.State(mesh, 8.6e5, ms[0], precision=precision)
+    f32 = precision == "fp32_field"
+    ins32 = [np.asfortranarray(m).ravel(order="F").copy() for m in ms]
+    ins64 = [a.astype(np.float64) for a in ins32]
+    out_t = np.float32 if f32 else np.float64
+    outs32 = [np.empty(3 * np.prod(shape), dtype=out_t) for _ in ms]
+    outs64 = [np.empty(3 * np.prod(shape), dtype=out_t) for _ in ms]
+    llg.heff_pipeline(s, [a.ctypes.data for a in ins32], [o.ctypes.data for o in outs32], m_float32=True)
+    llg.heff_pipeline(s, [a.ctypes.data for a in ins64], [o.ctypes.data for o in outs64])
+    for a, b in zip(outs32, outs64):
+        assert np.array_equal(a, b)
