@@ -319,6 +319,9 @@ int maf_string_image(maf_string h, int i, maf_state* image);
 typedef struct maf_cnn_s* maf_cnn;
 int maf_cnn_create(maf_cnn* out, int cin, int width, int depth, unsigned long long seed);
 int maf_cnn_destroy(maf_cnn h);
+/* dilation of each layer's 3x3 kernel (n = depth values in 1..64; default 1): layer l reads its input at
+ * offsets -d_l, 0, +d_l, which widens the receptive field without pooling */
+int maf_cnn_set_dilation(maf_cnn h, const int* dilation, int n);
 int maf_cnn_n_params(maf_cnn h, long long* n);
 int maf_cnn_get_params(maf_cnn h, float* host);
 /* also resets the Adam moments */

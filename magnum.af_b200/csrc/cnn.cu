@@ -1,8 +1,9 @@
 // Learned warm start for the LBFGS minimiser: a small convolutional network
 // with hand-written training and inference kernels (FP32).
 //
-// Network: L layers of 3x3 convolutions (zero padding), ReLU after every layer
-// but the last; input x [B][cin][H][W] whose first three channels are the
+// Network: L layers of 3x3 convolutions (zero padding; layer l samples its
+// input at offsets -d_l, 0, +d_l, the dilation d_l, 1 by default), ReLU after
+// every layer but the last; input x [B][cin][H][W] whose first three channels are the
 // magnetisation m, the rest material/field parameter maps; output
 //     y = normalize(m + conv_L(...relu(conv_1(x))...))      [B][3][H][W],
 // a proposal for the relaxed magnetisation.  Loss: mean over cells of
@@ -26,11 +27,11 @@ namespace {
 constexpr int kMaxC = 32;      // channels per layer
 constexpr int kPixPerBlk = 256;
 
-// out[b][co][y][x] = bias[co] + sum_ci,dy,dx W[co][ci][dy][dx] in[b][ci][y+dy-1][x+dx-1]
+// out[b][co][y][x] = bias[co] + sum_ci,dy,dx W[co][ci][dy][dx] in[b][ci][y+(dy-1)d][x+(dx-1)d]
 // (relu on the output when RELU).  One thread per output pixel, all cout outputs.
 template <bool RELU>
 __global__ void k_conv_fwd(const float* __restrict__ in, const float* __restrict__ W, const float* __restrict__ bias,
-                           float* __restrict__ out, int B, int cin, int cout, int H, int Wd) {
+                           float* __restrict__ out, int B, int cin, int cout, int H, int Wd, int dil) {
     __shared__ float w[kMaxC * kMaxC * 9];
     for (int i = threadIdx.x; i < cout * cin * 9; i += blockDim.x) w[i] = W[i];
     __syncthreads();
@@ -47,7 +48,7 @@ __global__ void k_conv_fwd(const float* __restrict__ in, const float* __restrict
         float v[9];
 #pragma unroll
         for (int t = 0; t < 9; ++t) {
-            const int yy = y + t / 3 - 1, xx = x + t % 3 - 1;
+            const int yy = y + (t / 3 - 1) * dil, xx = x + (t % 3 - 1) * dil;
             v[t] = (yy >= 0 && yy < H && xx >= 0 && xx < Wd) ? src[yy * Wd + xx] : 0.f;
         }
         for (int co = 0; co < cout; ++co) {
@@ -64,11 +65,11 @@ __global__ void k_conv_fwd(const float* __restrict__ in, const float* __restrict
     }
 }
 
-// grad_in[b][ci][y][x] = sum_co,dy,dx W[co][ci][dy][dx] g[b][co][y-dy+1][x-dx+1],
+// grad_in[b][ci][y][x] = sum_co,dy,dx W[co][ci][dy][dx] g[b][co][y-(dy-1)d][x-(dx-1)d],
 // masked by relu'(in) when the input came out of a ReLU (in > 0).
 __global__ void k_conv_bwd_data(const float* __restrict__ g, const float* __restrict__ W,
                                 const float* __restrict__ act_in, float* __restrict__ gin, int B, int cin, int cout,
-                                int H, int Wd, int relu_mask) {
+                                int H, int Wd, int relu_mask, int dil) {
     __shared__ float w[kMaxC * kMaxC * 9];
     for (int i = threadIdx.x; i < cout * cin * 9; i += blockDim.x) w[i] = W[i];
     __syncthreads();
@@ -85,7 +86,7 @@ __global__ void k_conv_bwd_data(const float* __restrict__ g, const float* __rest
         float v[9];
 #pragma unroll
         for (int t = 0; t < 9; ++t) {
-            const int yy = y - (t / 3 - 1), xx = x - (t % 3 - 1);
+            const int yy = y - (t / 3 - 1) * dil, xx = x - (t % 3 - 1) * dil;
             v[t] = (yy >= 0 && yy < H && xx >= 0 && xx < Wd) ? src[yy * Wd + xx] : 0.f;
         }
         for (int ci = 0; ci < cin; ++ci) {
@@ -107,7 +108,7 @@ __global__ void k_conv_bwd_data(const float* __restrict__ g, const float* __rest
 // Partial weight/bias gradients: block (k, chunk) sums over the pixels of its
 // chunk for weight entry k = (co, ci, t) (or bias co when k >= cout*cin*9).
 __global__ void k_conv_bwd_w_part(const float* __restrict__ g, const float* __restrict__ in, float* __restrict__ part,
-                                  int B, int cin, int cout, int H, int Wd, int nchunk) {
+                                  int B, int cin, int cout, int H, int Wd, int nchunk, int dil) {
     const int nw = cout * cin * 9;
     const int k = blockIdx.x;
     const int chunk = blockIdx.y;
@@ -117,7 +118,7 @@ __global__ void k_conv_bwd_w_part(const float* __restrict__ g, const float* __re
     float acc = 0.f;
     if (k < nw) {
         const int co = k / (cin * 9), ci = (k / 9) % cin, t = k % 9;
-        const int dy = t / 3 - 1, dx = t % 3 - 1;
+        const int dy = (t / 3 - 1) * dil, dx = (t % 3 - 1) * dil;
         for (int64_t p = p0 + threadIdx.x; p < p1; p += blockDim.x) {
             const int b = (int)(p / HW);
             const int r = (int)(p - (int64_t)b * HW);
@@ -219,6 +220,7 @@ __global__ void k_adam(float* __restrict__ w, const float* __restrict__ g, float
 struct maf_cnn_s {
     int cin = 0, width = 0, depth = 0;
     std::vector<int> ch;        // channels: ch[0] = cin, ..., ch[depth] = 3
+    std::vector<int> dil;       // dilation per layer
     std::vector<int64_t> woff;  // offset of layer l's W in the flat buffer; b follows W
     int64_t nparams = 0;
     DevBuf params, grads, m1, m2, part;
@@ -260,10 +262,11 @@ void cnn_forward(maf_cnn_s* h, const float* x, int B, int H, int W) {
         const float* Wl = P + h->woff[l];
         const float* bl = Wl + (int64_t)h->ch[l + 1] * h->ch[l] * 9;
         float* out = h->act[l].as<float>();
+        const int d = h->dil[l];
         if (l + 1 < h->depth)
-            k_conv_fwd<true><<<blocks, 256, 0, h->stream>>>(in, Wl, bl, out, B, h->ch[l], h->ch[l + 1], H, W);
+            k_conv_fwd<true><<<blocks, 256, 0, h->stream>>>(in, Wl, bl, out, B, h->ch[l], h->ch[l + 1], H, W, d);
         else
-            k_conv_fwd<false><<<blocks, 256, 0, h->stream>>>(in, Wl, bl, out, B, h->ch[l], h->ch[l + 1], H, W);
+            k_conv_fwd<false><<<blocks, 256, 0, h->stream>>>(in, Wl, bl, out, B, h->ch[l], h->ch[l + 1], H, W, d);
         MAF_LAUNCH_CHECK();
         in = out;
     }
@@ -291,7 +294,7 @@ void cnn_loss_grad(maf_cnn_s* h, const float* x, const float* tgt, int B, int H,
         h->part.ensure(sizeof(float) * (size_t)nk * nchunk);
         k_conv_bwd_w_part<<<dim3(nk, nchunk), kPixPerBlk, 0, h->stream>>>(h->gact[l].as<float>(), in,
                                                                             h->part.as<float>(), B, ci, co, H, W,
-                                                                            nchunk);
+                                                                            nchunk, h->dil[l]);
         MAF_LAUNCH_CHECK();
         k_sum_chunks<<<(unsigned)ceil_div(nk, 256), 256, 0, h->stream>>>(h->part.as<float>(), G + h->woff[l], nk,
                                                                          nchunk);
@@ -299,7 +302,7 @@ void cnn_loss_grad(maf_cnn_s* h, const float* x, const float* tgt, int B, int H,
         if (l > 0) {
             k_conv_bwd_data<<<blocks, 256, 0, h->stream>>>(h->gact[l].as<float>(), P + h->woff[l],
                                                            h->act[l - 1].as<float>(), h->gact[l - 1].as<float>(), B,
-                                                           ci, co, H, W, 1);
+                                                           ci, co, H, W, 1, h->dil[l]);
             MAF_LAUNCH_CHECK();
         }
     }
@@ -320,6 +323,7 @@ int maf_cnn_create(maf_cnn* out, int cin, int width, int depth, unsigned long lo
         h->ch.push_back(cin);
         for (int l = 1; l < depth; ++l) h->ch.push_back(width);
         h->ch.push_back(3);
+        h->dil.assign(depth, 1);
         int64_t off = 0;
         for (int l = 0; l < depth; ++l) {
             h->woff.push_back(off);
@@ -354,6 +358,15 @@ int maf_cnn_destroy(maf_cnn h) {
         cudaStream_t s = h ? h->stream : nullptr;
         delete h;
         if (s) cudaStreamDestroy(s);
+    });
+}
+
+int maf_cnn_set_dilation(maf_cnn h, const int* dilation, int n) {
+    return capi_run([&] {
+        if (!h || !dilation || n != h->depth) throw Error(MAF_ERR_BADARG, "maf_cnn_set_dilation: one value per layer");
+        for (int l = 0; l < n; ++l)
+            if (dilation[l] < 1 || dilation[l] > 64) throw Error(MAF_ERR_BADARG, "maf_cnn_set_dilation: 1 <= d <= 64");
+        h->dil.assign(dilation, dilation + n);
     });
 }
 

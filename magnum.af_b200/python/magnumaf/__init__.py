@@ -120,6 +120,7 @@ _SIGS = {
     "maf_state_set_steps": (_I, [_P, C.c_ulonglong]),
     "maf_mean_m_noalloc": (_I, [_P, C.c_longlong, _DP, _P]),
     "maf_cnn_create": (_I, [C.POINTER(_P), _I, _I, _I, C.c_ulonglong]),
+    "maf_cnn_set_dilation": (_I, [_P, C.POINTER(_I), _I]),
     "maf_cnn_destroy": (_I, [_P]),
     "maf_cnn_n_params": (_I, [_P, C.POINTER(C.c_longlong)]),
     "maf_cnn_get_params": (_I, [_P, _FP]),
@@ -823,10 +824,15 @@ class ConvNet:
     Array arguments are device pointers (e.g. torch CUDA tensors' data_ptr()),
     NCHW float32: x [B][cin][H][W] with m in channels 0..2, y and targets [B][3][H][W]."""
 
-    def __init__(self, cin: int, width: int = 16, depth: int = 4, seed: int = 0):
+    def __init__(self, cin: int, width: int = 16, depth: int = 4, seed: int = 0, dilation=None):
         self.cin, self.width, self.depth = int(cin), int(width), int(depth)
         self._h = _P()
         _ck(lib.maf_cnn_create(C.byref(self._h), self.cin, self.width, self.depth, int(seed)))
+        self.dilation = [1] * self.depth
+        if dilation is not None:
+            d = [int(v) for v in dilation]
+            _ck(lib.maf_cnn_set_dilation(self._h, (_I * len(d))(*d), len(d)))
+            self.dilation = d
 
     def __del__(self):
         if getattr(self, "_h", None):

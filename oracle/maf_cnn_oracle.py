@@ -4,9 +4,10 @@ Only tests import this module.  It is pinned by central finite differences
 (tests/test_cnn_oracle.py), then used to check the device gradients.
 
 Network: y = normalize(m + conv_L(relu(... relu(conv_1(x))))), 3x3 convolutions
-with zero padding, x [B][cin][H][W] with m = x[:, :3]; loss = mean over the
-B*H*W cells of |y - target|^2.  Parameters: one flat vector, per layer
-W[cout][cin][3][3] then b[cout]."""
+with zero padding and dilation d_l per layer (taps at offsets -d, 0, +d; 1 by
+default), x [B][cin][H][W] with m = x[:, :3]; loss = mean over the B*H*W cells
+of |y - target|^2.  Parameters: one flat vector, per layer W[cout][cin][3][3]
+then b[cout]."""
 import numpy as np
 
 
@@ -30,24 +31,25 @@ def unpack(p, cin, width, depth):
     return out
 
 
-def conv(x, W, b):
-    """out[b,co,y,x] = b[co] + sum W[co,ci,dy,dx] x[b,ci,y+dy-1,x+dx-1] (zero outside)."""
+def conv(x, W, b, d=1):
+    """out[b,co,y,x] = b[co] + sum W[co,ci,dy,dx] x[b,ci,y+(dy-1)d,x+(dx-1)d] (zero outside)."""
     B, C, H, Wd = x.shape
-    xp = np.zeros((B, C, H + 2, Wd + 2))
-    xp[:, :, 1:-1, 1:-1] = x
+    xp = np.zeros((B, C, H + 2 * d, Wd + 2 * d))
+    xp[:, :, d:d + H, d:d + Wd] = x
     out = np.zeros((B, W.shape[0], H, Wd)) + b[None, :, None, None]
     for dy in range(3):
         for dx in range(3):
-            out += np.einsum("oc,bchw->bohw", W[:, :, dy, dx], xp[:, :, dy:dy + H, dx:dx + Wd])
+            out += np.einsum("oc,bchw->bohw", W[:, :, dy, dx], xp[:, :, dy * d:dy * d + H, dx * d:dx * d + Wd])
     return out
 
 
-def forward(p, x, cin, width, depth):
+def forward(p, x, cin, width, depth, dil=None):
     layers = unpack(p, cin, width, depth)
+    dil = dil or [1] * depth
     acts = []
     a = x
     for l, (W, b) in enumerate(layers):
-        z = conv(a, W, b)
+        z = conv(a, W, b, dil[l])
         a = np.maximum(z, 0.0) if l + 1 < depth else z
         acts.append(a)
     v = x[:, :3] + acts[-1]
@@ -56,16 +58,17 @@ def forward(p, x, cin, width, depth):
     return y, acts, v, n
 
 
-def loss(p, x, t, cin, width, depth):
-    y = forward(p, x, cin, width, depth)[0]
+def loss(p, x, t, cin, width, depth, dil=None):
+    y = forward(p, x, cin, width, depth, dil)[0]
     B, _, H, W = y.shape
     return float(np.sum((y - t) ** 2) / (B * H * W))
 
 
-def loss_grad(p, x, t, cin, width, depth):
+def loss_grad(p, x, t, cin, width, depth, dil=None):
     layers = unpack(p, cin, width, depth)
+    dil = dil or [1] * depth
     ch, offs, npar = layout(cin, width, depth)
-    y, acts, v, n = forward(p, x, cin, width, depth)
+    y, acts, v, n = forward(p, x, cin, width, depth, dil)
     B, _, H, Wd = y.shape
     cells = B * H * Wd
     L = float(np.sum((y - t) ** 2) / cells)
@@ -75,24 +78,25 @@ def loss_grad(p, x, t, cin, width, depth):
     grad = np.zeros(npar)
     for l in range(depth - 1, -1, -1):
         W, _ = layers[l]
+        d = dil[l]
         a_in = x if l == 0 else acts[l - 1]
-        ap = np.zeros((B, ch[l], H + 2, Wd + 2))
-        ap[:, :, 1:-1, 1:-1] = a_in
+        ap = np.zeros((B, ch[l], H + 2 * d, Wd + 2 * d))
+        ap[:, :, d:d + H, d:d + Wd] = a_in
         gW = np.zeros_like(W)
         for dy in range(3):
             for dx in range(3):
-                gW[:, :, dy, dx] = np.einsum("bohw,bchw->oc", g, ap[:, :, dy:dy + H, dx:dx + Wd])
+                gW[:, :, dy, dx] = np.einsum("bohw,bchw->oc", g, ap[:, :, dy * d:dy * d + H, dx * d:dx * d + Wd])
         nw = W.size
         grad[offs[l]:offs[l] + nw] = gW.ravel()
         grad[offs[l] + nw:offs[l] + nw + ch[l + 1]] = np.sum(g, axis=(0, 2, 3))
         if l > 0:
-            gp = np.zeros((B, W.shape[0], H + 2, Wd + 2))
-            gp[:, :, 1:-1, 1:-1] = g
+            gp = np.zeros((B, W.shape[0], H + 2 * d, Wd + 2 * d))
+            gp[:, :, d:d + H, d:d + Wd] = g
             gin = np.zeros((B, ch[l], H, Wd))
             for dy in range(3):
                 for dx in range(3):
-                    # input pixel (y, x) feeds output (y - dy + 1, x - dx + 1) through tap (dy, dx)
-                    gin += np.einsum("oc,bohw->bchw", W[:, :, dy, dx],
-                                     gp[:, :, 2 - dy:2 - dy + H, 2 - dx:2 - dx + Wd])
+                    # input pixel (y, x) feeds output (y - (dy-1)d, x - (dx-1)d) through tap (dy, dx)
+                    oy, ox = (2 - dy) * d, (2 - dx) * d
+                    gin += np.einsum("oc,bohw->bchw", W[:, :, dy, dx], gp[:, :, oy:oy + H, ox:ox + Wd])
             g = gin * (acts[l - 1] > 0)
     return L, grad

@@ -36,3 +36,23 @@ def test_untrained_last_layer_zero_returns_normalised_m():
     y = N.forward(p, x, *arch)[0]
     m = x[:, :3]
     np.testing.assert_allclose(y, m / np.linalg.norm(m, axis=1, keepdims=True), atol=1e-15)
+
+
+def test_dilated_gradient_matches_finite_differences():
+    """Dilated layers (taps at -d, 0, +d) with d larger than the image in one case."""
+    p, x, t, arch = _case(4, H=7, W=8)
+    dil = [1, 2, 9]
+    L, g = N.loss_grad(p, x, t, *arch, dil=dil)
+    assert abs(L - N.loss(p, x, t, *arch, dil=dil)) < 1e-14
+    eps = 1e-6
+    idx = np.random.default_rng(5).choice(p.size, 60, replace=False)
+    for i in idx:
+        pp, pm = p.copy(), p.copy()
+        pp[i] += eps
+        pm[i] -= eps
+        fd = (N.loss(pp, x, t, *arch, dil=dil) - N.loss(pm, x, t, *arch, dil=dil)) / (2 * eps)
+        assert abs(fd - g[i]) <= 1e-6 * max(1.0, abs(g[i])) + 1e-8, (i, fd, g[i])
+    # d = 1 everywhere is the undilated network
+    L1, g1 = N.loss_grad(p, x, t, *arch, dil=[1, 1, 1])
+    L0, g0 = N.loss_grad(p, x, t, *arch)
+    assert L1 == L0 and np.array_equal(g1, g0)

@@ -26,8 +26,9 @@ def _dev(a):
     return torch.from_numpy(np.ascontiguousarray(a, dtype=np.float32)).cuda()
 
 
-def test_gradients_match_oracle():
-    net = M.ConvNet(*ARCH, seed=3)
+@pytest.mark.parametrize("dil", [None, [1, 2, 4], [3, 1, 10]])
+def test_gradients_match_oracle(dil):
+    net = M.ConvNet(*ARCH, seed=3, dilation=dil)
     rng = np.random.default_rng(4)
     p = rng.normal(scale=0.4, size=net.n_params).astype(np.float32)
     net.set_params(p)
@@ -35,21 +36,22 @@ def test_gradients_match_oracle():
     xd, td = _dev(x), _dev(t)
     loss, g = net.loss_grad(xd.data_ptr(), td.data_ptr(), *x.shape[:1], x.shape[2], x.shape[3])
     x32, t32 = x.astype(np.float32).astype(np.float64), t.astype(np.float32).astype(np.float64)
-    L_ref, g_ref = N.loss_grad(p.astype(np.float64), x32, t32, *ARCH)
+    L_ref, g_ref = N.loss_grad(p.astype(np.float64), x32, t32, *ARCH, dil=dil)
     assert abs(loss - L_ref) <= 1e-5 * L_ref
     scale = np.abs(g_ref).max()
     np.testing.assert_allclose(g, g_ref, rtol=1e-3, atol=1e-5 * scale)
 
 
-def test_forward_matches_oracle():
-    net = M.ConvNet(*ARCH, seed=1)
+@pytest.mark.parametrize("dil", [None, [2, 3, 1]])
+def test_forward_matches_oracle(dil):
+    net = M.ConvNet(*ARCH, seed=1, dilation=dil)
     p = np.random.default_rng(6).normal(scale=0.4, size=net.n_params).astype(np.float32)
     net.set_params(p)
     x, _ = _data(7)
     xd = _dev(x)
     y = torch.empty((x.shape[0], 3, x.shape[2], x.shape[3]), dtype=torch.float32, device="cuda")
     net.forward(xd.data_ptr(), x.shape[0], x.shape[2], x.shape[3], y.data_ptr())
-    y_ref = N.forward(p.astype(np.float64), x.astype(np.float32).astype(np.float64), *ARCH)[0]
+    y_ref = N.forward(p.astype(np.float64), x.astype(np.float32).astype(np.float64), *ARCH, dil=dil)[0]
     np.testing.assert_allclose(y.cpu().numpy(), y_ref, atol=2e-5)
 
 
