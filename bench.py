@@ -18,6 +18,8 @@ fp64_form  the FP64 form on the same mesh; rel_err_fp32_vs_fp64 checks the metri
            field term and for the component of H perpendicular to m.
 trajectory 5 ps of DP45 with dense output of <m> in both forms: simulated ns per
            hour and the largest <m> difference between the forms.
+configs    simulated ns per hour of short runs of the strip (100x25x1) and skyrmion
+           film (512x512x4) configurations.
 roofline   the dominant pass: algorithmic bytes per launch / its mean CUDA-event
            duration, against the measured HBM copy bandwidth.
 --impl reference  the FP64 CPU oracle (the reference algorithm restated in NumPy/SciPy)
@@ -228,6 +230,59 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def other_configs(M, stream):
+    """Simulated ns per hour of wall time on the two other single-mesh
+    configurations (short runs, seeded inputs):
+    strip   100x25x1 cells of 5x5x3 nm, demag + exchange, Ms 8e5, A 1.3e-11,
+            m = x + U(-0.1, 0.1)^3 renormalised, alpha 1, DP45 (atol = rtol = 1e-6),
+            <m> sampled every 10 ps for 0.2 ns (FP64 form, the configuration's);
+    film    512x512x4 cells of 2x2x1 nm, demag + exchange (1.6e-11) + interface DMI
+            (3e-3) + uniaxial Ku 1e6 along z, Ms 1.1e6, alpha 0.1, m = +z with 20
+            reversed discs of radius 5-15 cells, RKF45, 200 steps in both forms."""
+    import torch
+
+    rng = np.random.default_rng(SEED + 1)
+    out = {}
+    mesh = M.Mesh(100, 25, 1, 5e-9, 5e-9, 3e-9)
+    m = np.zeros((100, 25, 1, 3))
+    m[..., 0] = 1.0
+    m += rng.uniform(-0.1, 0.1, size=m.shape)
+    st = M.State(mesh, 8e5, m)
+    st.set_stream(stream.cuda_stream)
+    llg = M.LLGIntegrator(1.0, [M.DemagField(mesh), M.ExchangeField(1.3e-11)], "DP45", atol=1e-6, rtol=1e-6)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    llg.integrate_dense(st, 2e-10, 1e-11)
+    wall = time.perf_counter() - t0
+    out["strip_100x25x1"] = {"sim_ns_per_hour": 0.2 / wall * 3600.0, "steps": st.steps, "wall_s": wall,
+                             "form": "fp64"}
+    del st, llg
+    n, nz = 512, 4
+    mesh = M.Mesh(n, n, nz, 2e-9, 2e-9, 1e-9)
+    m = np.zeros((n, n, nz, 3))
+    m[..., 2] = 1.0
+    yy, xx = np.meshgrid(np.arange(n), np.arange(n))
+    for _ in range(20):
+        r = rng.integers(5, 16)
+        cx, cy = rng.uniform(0, n, size=2)
+        m[(xx - cx) ** 2 + (yy - cy) ** 2 < r * r, :, 2] = -1.0
+    terms = [M.DemagField(mesh), M.ExchangeField(1.6e-11), M.DmiField(3e-3), M.UniaxialAnisotropyField(1e6)]
+    llg = M.LLGIntegrator(0.1, terms, "RKF45")
+    for prec in ("fp32_field", "fp64"):
+        st = M.State(mesh, 1.1e6, m, precision=prec)
+        st.set_stream(stream.cuda_stream)
+        llg.steps(st, 5)  # warm-up
+        torch.cuda.synchronize()
+        t_start = st.t
+        t0 = time.perf_counter()
+        llg.steps(st, 200)
+        wall = time.perf_counter() - t0
+        out["film_512x512x4_" + prec] = {"sim_ns_per_hour": (st.t - t_start) * 1e9 / wall * 3600.0,
+                                         "steps_per_s": 200 / wall, "sim_s": st.t - t_start}
+        del st
+    return out
+
+
 def run_ours(args):
     import ctypes as C
 
@@ -356,6 +411,9 @@ def run_ours(args):
         traj["t_sim_s"] = TRAJ_T
         traj["scheme"] = "DP45 (alpha 0.01, default controller), <m> sampled every %g s" % (TRAJ_T / 10)
 
+    # the other single-mesh configurations, short runs: simulated ns per hour
+    cfgs = {} if args.no_trajectory else other_configs(M, stream)
+
     # per-pass timing (CUDA events between the pass kernels on the launching stream)
     passes = {}
     nprof = max(3, min(args.steps, 10))
@@ -436,6 +494,7 @@ def run_ours(args):
                       "fp32_speedup": ms64 / ms32},
         "rel_err_fp32_vs_fp64": {"l2": rel_err, "max": rel_max, "per_term": per_term},
         "trajectory": traj,
+        "configs": cfgs,
         "passes_ms": pass_ms,
         "eval_roofline": {"bytes": eval_bytes, "achieved_gbs": eval_gbs, "frac": eval_gbs / peak},
         "roofline": {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak, "unit": "GB/s",
