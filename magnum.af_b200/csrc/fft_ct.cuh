@@ -49,6 +49,43 @@ template <int DIR, typename R> __host__ __device__ __forceinline__ void bfly16(c
     }
 }
 
+// 16-point DFT of v[0..7] with v[8..15] = 0, the zero-padded upper half of a
+// transform's input: the first radix-4 layer sees two nonzero inputs per group,
+// (a, b, 0, 0) -> (a + b, a + i b, a - b, a - i b) with i = W4^1 in the sign of DIR.
+template <int DIR, typename R> __host__ __device__ __forceinline__ void bfly16_half(cplx_t<R>* v) {
+    using C = cplx_t<R>;
+    const R c1 = (R)0.92387953251128675613, s1 = (R)0.38268343236508977173;  // cos, sin (pi/8)
+    const R h = (R)0.70710678118654752440;
+    C a[4][4];
+#pragma unroll
+    for (int n2 = 0; n2 < 4; ++n2) {
+        const C p = v[n2], q = v[4 + n2];
+        const C iq = cmul_i<DIR>(q);
+        a[n2][0] = cadd(p, q);
+        a[n2][1] = cadd(p, iq);
+        a[n2][2] = csub(p, q);
+        a[n2][3] = csub(p, iq);
+    }
+    const R sd = (R)DIR;
+    const C w1 = mk(c1, sd * s1), w2 = mk(h, sd * h), w3 = mk(s1, sd * c1);
+    a[1][1] = cmul(a[1][1], w1);
+    a[1][2] = cmul(a[1][2], w2);
+    a[1][3] = cmul(a[1][3], w3);
+    a[2][1] = cmul(a[2][1], w2);
+    a[2][2] = cmul_i<DIR>(a[2][2]);
+    a[2][3] = cmul(a[2][3], mk(-h, sd * h));  // W16^6
+    a[3][1] = cmul(a[3][1], w3);
+    a[3][2] = cmul(a[3][2], mk(-h, sd * h));  // W16^6
+    a[3][3] = cmul(a[3][3], mk(-c1, -sd * s1));  // W16^9 = -W16^1
+#pragma unroll
+    for (int k1 = 0; k1 < 4; ++k1) {
+        C t[4] = {a[0][k1], a[1][k1], a[2][k1], a[3][k1]};
+        bfly4<DIR>(t);
+#pragma unroll
+        for (int k2 = 0; k2 < 4; ++k2) v[k1 + 4 * k2] = t[k2];
+    }
+}
+
 template <int RAD, int DIR, typename R> __device__ __forceinline__ void bfly_ct(cplx_t<R>* v) {
     if constexpr (RAD == 2) {
         bfly2<DIR>(v[0], v[1]);
@@ -62,9 +99,11 @@ template <int RAD, int DIR, typename R> __device__ __forceinline__ void bfly_ct(
     }
 }
 
-// One stage over NB columns of length L with NT threads.
-template <typename R, int RAD, int DIR, bool BFAST, int L, int NS, int NB, int NT>
+// One stage over NB columns of length L with NT threads.  HOUT (last stage only):
+// just the outputs i < L/2 are written, the arithmetic only the others need is dropped.
+template <typename R, int RAD, int DIR, bool BFAST, int L, int NS, int NB, int NT, bool HOUT = false>
 __device__ __forceinline__ void ct_stage(cplx_t<R>* s, int sb, const cplx_t<R>* __restrict__ tw) {
+    static_assert(!HOUT || NS * RAD == L, "output pruning is for the last stage");
     using C = cplx_t<R>;
     constexpr int NBF = L / RAD;
     constexpr int TOTAL = NBF * NB;
@@ -102,6 +141,7 @@ __device__ __forceinline__ void ct_stage(cplx_t<R>* s, int sb, const cplx_t<R>* 
             const int d = (j - jm) * RAD + jm;
 #pragma unroll
             for (int r = 0; r < RAD; ++r) {
+                if (HOUT && r >= RAD / 2) continue;
                 const int i = d + r * NS;
                 s[BFAST ? spad(i) * NB + b : spad(i) + b * sb] = v[k][r];
             }
@@ -110,15 +150,19 @@ __device__ __forceinline__ void ct_stage(cplx_t<R>* s, int sb, const cplx_t<R>* 
     __syncthreads();
 }
 
-template <typename R, int DIR, bool BFAST, int L, int NS, int NB, int NT, int RAD, int... REST>
+template <typename R, int DIR, bool BFAST, int L, int NS, int NB, int NT, bool HOUT, int RAD, int... REST>
 __device__ __forceinline__ void ct_run(cplx_t<R>* s, int sb, const cplx_t<R>* __restrict__ tw) {
-    ct_stage<R, RAD, DIR, BFAST, L, NS, NB, NT>(s, sb, tw);
-    if constexpr (sizeof...(REST) > 0) ct_run<R, DIR, BFAST, L, NS * RAD, NB, NT, REST...>(s, sb, tw);
+    if constexpr (sizeof...(REST) > 0) {
+        ct_stage<R, RAD, DIR, BFAST, L, NS, NB, NT>(s, sb, tw);
+        ct_run<R, DIR, BFAST, L, NS * RAD, NB, NT, HOUT, REST...>(s, sb, tw);
+    } else {
+        ct_stage<R, RAD, DIR, BFAST, L, NS, NB, NT, HOUT>(s, sb, tw);
+    }
 }
 
 template <typename R, int DIR, bool BFAST, int L, int NB, int NT, int... RS>
 __device__ __forceinline__ void ct_fft(cplx_t<R>* s, int sb, const cplx_t<R>* __restrict__ tw, Radices<RS...>) {
-    ct_run<R, DIR, BFAST, L, 1, NB, NT, RS...>(s, sb, tw);
+    ct_run<R, DIR, BFAST, L, 1, NB, NT, false, RS...>(s, sb, tw);
 }
 
 // ----------------------------------------------------------------------------
@@ -136,12 +180,15 @@ template <bool BFAST, int NB, int NBF> __device__ __forceinline__ void ct_bj(int
 }
 
 // The caller synchronises before s is overwritten; ends with a barrier.
-template <typename R, int RAD, int DIR, bool BFAST, int L, int NB, int NT, typename LD>
+// HIN: the inputs i >= L/2 are zero (a zero-padded transform) -- with a radix-16
+// first stage they are neither loaded nor fed through the butterfly.
+template <typename R, int RAD, int DIR, bool BFAST, int L, int NB, int NT, bool HIN, typename LD>
 __device__ __forceinline__ void ct_stage_in(cplx_t<R>* s, int sb, LD&& ld) {
     using C = cplx_t<R>;
     constexpr int NBF = L / RAD;
     constexpr int TOTAL = NBF * NB;
     constexpr int BPT = (TOTAL + NT - 1) / NT;
+    constexpr bool HALF = HIN && RAD == 16;
     C v[BPT][RAD];
 #pragma unroll
     for (int k = 0; k < BPT; ++k) {
@@ -150,7 +197,7 @@ __device__ __forceinline__ void ct_stage_in(cplx_t<R>* s, int sb, LD&& ld) {
             int b, j;
             ct_bj<BFAST, NB, NBF>(q, b, j);
 #pragma unroll
-            for (int r = 0; r < RAD; ++r) v[k][r] = ld(b, j + r * NBF);
+            for (int r = 0; r < RAD; ++r) v[k][r] = (HALF && r >= RAD / 2) ? mk((R)0, (R)0) : ld(b, j + r * NBF);
         }
     }
 #pragma unroll
@@ -159,7 +206,10 @@ __device__ __forceinline__ void ct_stage_in(cplx_t<R>* s, int sb, LD&& ld) {
         if (TOTAL % NT == 0 || q < TOTAL) {
             int b, j;
             ct_bj<BFAST, NB, NBF>(q, b, j);
-            bfly_ct<RAD, DIR, R>(v[k]);
+            if constexpr (HALF)
+                bfly16_half<DIR, R>(v[k]);
+            else
+                bfly_ct<RAD, DIR, R>(v[k]);
 #pragma unroll
             for (int r = 0; r < RAD; ++r) {
                 const int i = j * RAD + r;
@@ -172,7 +222,9 @@ __device__ __forceinline__ void ct_stage_in(cplx_t<R>* s, int sb, LD&& ld) {
 
 // Reads s written by the previous stage (which ended with a barrier); no
 // barrier at the end: the caller synchronises before s is reused.
-template <typename R, int RAD, int DIR, bool BFAST, int L, int NB, int NT, typename ST>
+// HOUT: only the outputs i < L/2 are wanted (a truncated transform): the others
+// are not stored, and the arithmetic that only they need is dropped.
+template <typename R, int RAD, int DIR, bool BFAST, int L, int NB, int NT, bool HOUT, typename ST>
 __device__ __forceinline__ void ct_stage_out(const cplx_t<R>* s, int sb, const cplx_t<R>* __restrict__ tw, ST&& st) {
     using C = cplx_t<R>;
     constexpr int NBF = L / RAD;
@@ -198,39 +250,45 @@ __device__ __forceinline__ void ct_stage_out(const cplx_t<R>* s, int sb, const c
             }
             bfly_ct<RAD, DIR, R>(v);
 #pragma unroll
-            for (int r = 0; r < RAD; ++r) st(b, j + r * NS, v[r]);
+            for (int r = 0; r < RAD; ++r)
+                if (!HOUT || r < RAD / 2) st(b, j + r * NS, v[r]);
         }
     }
 }
 
-template <typename R, int DIR, bool BFAST, int L, int NS, int NB, int NT, typename ST, int RAD, int... REST>
+template <typename R, int DIR, bool BFAST, int L, int NS, int NB, int NT, bool HOUT, typename ST, int RAD,
+          int... REST>
 __device__ __forceinline__ void ct_run_out(cplx_t<R>* s, int sb, const cplx_t<R>* __restrict__ tw, ST&& st) {
     if constexpr (sizeof...(REST) == 0) {
         static_assert(NS * RAD == L, "radix sequence");
-        ct_stage_out<R, RAD, DIR, BFAST, L, NB, NT>(s, sb, tw, st);
+        ct_stage_out<R, RAD, DIR, BFAST, L, NB, NT, HOUT>(s, sb, tw, st);
     } else {
         ct_stage<R, RAD, DIR, BFAST, L, NS, NB, NT>(s, sb, tw);
-        ct_run_out<R, DIR, BFAST, L, NS * RAD, NB, NT, ST, REST...>(s, sb, tw, st);
+        ct_run_out<R, DIR, BFAST, L, NS * RAD, NB, NT, HOUT, ST, REST...>(s, sb, tw, st);
     }
 }
 
 // global -> first stage -> ... -> last stage, result in shared memory
-template <typename R, int DIR, bool BFAST, int L, int NB, int NT, typename LD, int R0, int... RS>
+// (HIN: the inputs i >= L/2 are zero; HOUT: only the outputs i < L/2 are written)
+template <typename R, int DIR, bool BFAST, int L, int NB, int NT, bool HIN = false, bool HOUT = false, typename LD,
+          int R0, int... RS>
 __device__ __forceinline__ void ct_fft_in(cplx_t<R>* s, int sb, const cplx_t<R>* __restrict__ tw, LD&& ld,
                                           Radices<R0, RS...>) {
-    ct_stage_in<R, R0, DIR, BFAST, L, NB, NT>(s, sb, ld);
-    if constexpr (sizeof...(RS) > 0) ct_run<R, DIR, BFAST, L, R0, NB, NT, RS...>(s, sb, tw);
+    static_assert(!HOUT || sizeof...(RS) > 0, "output pruning needs a separate last stage");
+    ct_stage_in<R, R0, DIR, BFAST, L, NB, NT, HIN>(s, sb, ld);
+    if constexpr (sizeof...(RS) > 0) ct_run<R, DIR, BFAST, L, R0, NB, NT, HOUT, RS...>(s, sb, tw);
 }
 
-// shared memory -> ... -> last stage -> global
-template <typename R, int DIR, bool BFAST, int L, int NB, int NT, typename ST, int... RS>
+// shared memory -> ... -> last stage -> global (HOUT: only outputs i < L/2 are stored)
+template <typename R, int DIR, bool BFAST, int L, int NB, int NT, bool HOUT = false, typename ST, int... RS>
 __device__ __forceinline__ void ct_fft_out(cplx_t<R>* s, int sb, const cplx_t<R>* __restrict__ tw, ST&& st,
                                            Radices<RS...>) {
-    ct_run_out<R, DIR, BFAST, L, 1, NB, NT, ST, RS...>(s, sb, tw, st);
+    ct_run_out<R, DIR, BFAST, L, 1, NB, NT, HOUT, ST, RS...>(s, sb, tw, st);
 }
 
 // global -> ... -> global; the caller synchronises before s is reused
-template <typename R, int DIR, bool BFAST, int L, int NB, int NT, typename LD, typename ST, int R0, int... RS>
+template <typename R, int DIR, bool BFAST, int L, int NB, int NT, bool HIN = false, bool HOUT = false, typename LD,
+          typename ST, int R0, int... RS>
 __device__ __forceinline__ void ct_fft_io(cplx_t<R>* s, int sb, const cplx_t<R>* __restrict__ tw, LD&& ld, ST&& st,
                                           Radices<R0, RS...>) {
     if constexpr (sizeof...(RS) == 0) {
@@ -238,21 +296,26 @@ __device__ __forceinline__ void ct_fft_io(cplx_t<R>* s, int sb, const cplx_t<R>*
         static_assert(R0 == L, "radix sequence");
         using C = cplx_t<R>;
         constexpr int BPT = (NB + NT - 1) / NT;
+        constexpr bool HALF = HIN && R0 == 16;
 #pragma unroll
         for (int k = 0; k < BPT; ++k) {
             const int q = threadIdx.x + k * NT;
             if (NB % NT == 0 || q < NB) {
                 C v[R0];
 #pragma unroll
-                for (int r = 0; r < R0; ++r) v[r] = ld(q, r);
-                bfly_ct<R0, DIR, R>(v);
+                for (int r = 0; r < R0; ++r) v[r] = (HALF && r >= R0 / 2) ? mk((R)0, (R)0) : ld(q, r);
+                if constexpr (HALF)
+                    bfly16_half<DIR, R>(v);
+                else
+                    bfly_ct<R0, DIR, R>(v);
 #pragma unroll
-                for (int r = 0; r < R0; ++r) st(q, r, v[r]);
+                for (int r = 0; r < R0; ++r)
+                    if (!HOUT || r < R0 / 2) st(q, r, v[r]);
             }
         }
     } else {
-        ct_stage_in<R, R0, DIR, BFAST, L, NB, NT>(s, sb, ld);
-        ct_run_out<R, DIR, BFAST, L, R0, NB, NT, ST, RS...>(s, sb, tw, st);
+        ct_stage_in<R, R0, DIR, BFAST, L, NB, NT, HIN>(s, sb, ld);
+        ct_run_out<R, DIR, BFAST, L, R0, NB, NT, HOUT, ST, RS...>(s, sb, tw, st);
     }
 }
 

@@ -31,7 +31,9 @@ static_assert(kRunCells == 2 || kRunCells == 4, "run length");
 #endif
 
 // ------------------------------------------------------------------ x forward
-template <typename R, int LC, int NB, int NT>
+// HIN: n_in <= LC, so the packed values k >= LC/2 are the zero padding (pruned
+// from the first stage)
+template <typename R, int LC, int NB, int NT, bool HIN>
 __global__ void __launch_bounds__(NT) k_xfwd_ct(const R* __restrict__ in, int n_in, int64_t rows, int64_t rows_pc,
                                                 const R* __restrict__ msf, R ms, cplx_t<R>* __restrict__ out,
                                                 int pitch, const cplx_t<R>* __restrict__ tw,
@@ -71,7 +73,7 @@ __global__ void __launch_bounds__(NT) k_xfwd_ct(const R* __restrict__ in, int n_
         }
         return mk(a, c);
     };
-    ct_fft_in<R, -1, false, LC, NB, NT>(s, SB, tw, ld, typename CtPlan<LC>::T());
+    ct_fft_in<R, -1, false, LC, NB, NT, HIN>(s, SB, tw, ld, typename CtPlan<LC>::T());
     // R2C post-processing by pairs: with E = (Z_k + Z*_{L-k})/2, O = -i (Z_k - Z*_{L-k})/2
     // and t = W_{2L}^k O, X[k] = E + t and X[L-k] = (E - t)*  (W_{2L}^{L-k} = -(W_{2L}^k)*),
     // so one pair of shared-memory reads and one twiddle give two outputs.
@@ -98,7 +100,9 @@ __global__ void __launch_bounds__(NT) k_xfwd_ct(const R* __restrict__ in, int n_
 // inputs straight from global memory (rows >= n_in are the zero padding and
 // are not read), the last stage stores straight to global memory (rows >=
 // n_out are truncated and not written).
-template <typename R, int DIR, int L, int NB, int NT>
+// HIN: n_in <= L/2 (zero-padded input), HOUT: n_out <= L/2 (truncated output);
+// both prune the transform at compile time
+template <typename R, int DIR, int L, int NB, int NT, bool HIN, bool HOUT>
 __global__ void __launch_bounds__(NT, (kMinBlocks<R, NT, 1024, 512>)) k_cols_ct(const cplx_t<R>* in, cplx_t<R>* out, int n_in, int n_out, int ncols,
                                                 int64_t in_si, int64_t out_si, int64_t in_sbat, int64_t out_sbat,
                                                 const cplx_t<R>* __restrict__ tw) {
@@ -113,7 +117,7 @@ __global__ void __launch_bounds__(NT, (kMinBlocks<R, NT, 1024, 512>)) k_cols_ct(
     auto st = [&](int b, int i, C v) {
         if (i < n_out && b < ncv) ob[i * out_si + b] = v;
     };
-    ct_fft_io<R, DIR, true, L, NB, NT>(s, 0, tw, ld, st, typename CtPlan<L>::T());
+    ct_fft_io<R, DIR, true, L, NB, NT, HIN, HOUT>(s, 0, tw, ld, st, typename CtPlan<L>::T());
 }
 
 // -------------------------------------------------- z convolution (3-D meshes)
@@ -149,7 +153,8 @@ __global__ void __launch_bounds__(NT, (kMinBlocks<R, NT, 768, 512>)) k_convz_ct(
         const int64_t o = at(col, i, ok);
         return ok ? S[o] : mk((R)0, (R)0);
     };
-    ct_fft_in<R, -1, true, L, NC, NT>(s, 0, tw, ld, typename CtPlan<L>::T());
+    // L = 2 nz: the upper half of the input is the padding, of the output the truncation
+    ct_fft_in<R, -1, true, L, NC, NT, true>(s, 0, tw, ld, typename CtPlan<L>::T());
     const int Pz = 2 * nz;
     const int64_t tcs = (int64_t)(nz + 1) * (ny + 1) * nxh;
     for (int idx = threadIdx.x; idx < L * NB; idx += NT) {
@@ -179,7 +184,7 @@ __global__ void __launch_bounds__(NT, (kMinBlocks<R, NT, 768, 512>)) k_convz_ct(
         const int64_t o = at(col, i, ok);
         if (ok) S[o] = v;
     };
-    ct_fft_out<R, 1, true, L, NC, NT>(s, 0, tw, st, typename CtPlan<L>::T());
+    ct_fft_out<R, 1, true, L, NC, NT, true>(s, 0, tw, st, typename CtPlan<L>::T());
 }
 
 // ------------------------------ z convolution, transforms in registers (nz <= 16)
@@ -288,7 +293,8 @@ __global__ void __launch_bounds__(NT) k_convy_ct(cplx_t<R>* S, const R* __restri
         const int comp = col / NB, b = col % NB;
         return (i < ny && b < ncv) ? S[comp * cs + (int64_t)i * pitch + c0 + b] : mk((R)0, (R)0);
     };
-    ct_fft_in<R, -1, true, L, NC, NT>(s, 0, tw, ld, typename CtPlan<L>::T());
+    // L = 2 ny: zero-padded input, truncated output
+    ct_fft_in<R, -1, true, L, NC, NT, true>(s, 0, tw, ld, typename CtPlan<L>::T());
     const int64_t tcs = (int64_t)(ny + 1) * nxh;
     for (int idx = threadIdx.x; idx < L * NB; idx += NT) {
         const int ky = idx / NB;
@@ -309,7 +315,7 @@ __global__ void __launch_bounds__(NT) k_convy_ct(cplx_t<R>* S, const R* __restri
         const int comp = col / NB, b = col % NB;
         if (i < ny && b < ncv) S[comp * cs + (int64_t)i * pitch + c0 + b] = v;
     };
-    ct_fft_out<R, 1, true, L, NC, NT>(s, 0, tw, st, typename CtPlan<L>::T());
+    ct_fft_out<R, 1, true, L, NC, NT, true>(s, 0, tw, st, typename CtPlan<L>::T());
 }
 
 // --------------------------------------------------- x inverse + epilogue
@@ -339,7 +345,11 @@ __global__ void __launch_bounds__(NT, (kMinBlocks<R, NT, (RN == 2 ? MAF_XINV_THR
         const C O = cmulc(csub(Xk, cconj(Xm)), twP[k]);
         return cadd(E_, cmul_i<1>(O));
     };
-    ct_fft_in<R, 1, false, LC, NC, NT>(s, SB, tw, ld, typename CtPlan<LC>::T());
+    // only the first nx of the 2 LC real outputs (packed values k < LC/2) are kept
+    if constexpr (LC >= 32)
+        ct_fft_in<R, 1, false, LC, NC, NT, false, true>(s, SB, tw, ld, typename CtPlan<LC>::T());
+    else
+        ct_fft_in<R, 1, false, LC, NC, NT>(s, SB, tw, ld, typename CtPlan<LC>::T());
     if constexpr (EPI == EPI_H || EPI == EPI_LLG) {
         if (run4) {
             const int runs = g.nx / RN;
@@ -465,7 +475,7 @@ constexpr int pow2floor(int x) {
     return p;
 }
 
-template <typename R, int LC>
+template <typename R, int LC, bool HIN>
 static void xfwd_L(const R* in, int n_in, int64_t rows, int64_t rows_pc, const R* msf, R ms, cplx_t<R>* out, int pitch,
                    const void* tw, const void* twP, cudaStream_t st) {
     constexpr int NB = pow2floor(cmax(1, kTileX<R> / LC));
@@ -473,7 +483,7 @@ static void xfwd_L(const R* in, int n_in, int64_t rows, int64_t rows_pc, const R
     static_assert(NT <= kMaxFftThreads, "CTA size");
     constexpr int SB = (LC - 1) + ((LC - 1) >> 4) + 1;
     const size_t smem = sizeof(cplx_t<R>) * (size_t)NB * SB;
-    auto k = k_xfwd_ct<R, LC, NB, NT>;
+    auto k = k_xfwd_ct<R, LC, NB, NT, HIN>;
     ct_smem(k, smem);
     k<<<(unsigned)ceil_div(rows, NB), NT, smem, st>>>(in, n_in, rows, rows_pc, msf, ms, out, pitch,
                                                        static_cast<const cplx_t<R>*>(tw),
@@ -481,14 +491,14 @@ static void xfwd_L(const R* in, int n_in, int64_t rows, int64_t rows_pc, const R
     MAF_LAUNCH_CHECK();
 }
 
-template <typename R, int DIR, int L, int TILE>
+template <typename R, int DIR, int L, int TILE, bool HIN, bool HOUT>
 static void cols_L(const cplx_t<R>* in, cplx_t<R>* out, int n_in, int n_out, int ncols, int64_t in_si, int64_t out_si,
                    int64_t in_sbat, int64_t out_sbat, int nbat, const void* tw, cudaStream_t st) {
     constexpr int NB = pow2floor(cmin(32, cmax(1, TILE / L)));
     constexpr int NT = L * NB / kE;
     static_assert(NT <= 1024, "CTA size");
     const size_t smem = sizeof(cplx_t<R>) * (size_t)NB * ((L - 1) + ((L - 1) >> 4) + 1);
-    auto k = k_cols_ct<R, DIR, L, NB, NT>;
+    auto k = k_cols_ct<R, DIR, L, NB, NT, HIN, HOUT>;
     ct_smem(k, smem);
     dim3 grid((unsigned)ceil_div(ncols, NB), (unsigned)nbat);
     k<<<grid, NT, smem, st>>>(in, out, n_in, n_out, ncols, in_si, out_si, in_sbat, out_sbat,
@@ -598,7 +608,17 @@ bool ct_xfwd(const R* in, int n_in, int64_t rows, int64_t rows_pc, const R* msf,
              int Px, Twiddles& tw, cudaStream_t st) {
     const int LC = Px / 2;
     const bool f64 = sizeof(R) == 8;
-#define X(N) xfwd_L<R, N>(in, n_in, rows, rows_pc, msf, ms, out, pitch, tw.get(N, f64), tw.get(Px, f64), st)
+    // a zero-padded input (n_in <= LC: the magnetisation) runs the pruned first stage;
+    // a full input (the tensor, assembled in FP64) the complete one
+    const bool half = n_in <= LC;
+    if (!half && !f64) return false;
+#define X(N)                                                                                                   \
+    do {                                                                                                       \
+        if (half)                                                                                              \
+            xfwd_L<R, N, true>(in, n_in, rows, rows_pc, msf, ms, out, pitch, tw.get(N, f64), tw.get(Px, f64), st); \
+        else if constexpr (sizeof(R) == 8)                                                                     \
+            xfwd_L<R, N, false>(in, n_in, rows, rows_pc, msf, ms, out, pitch, tw.get(N, f64), tw.get(Px, f64), st); \
+    } while (0)
     MAF_CT_SWITCH(LC, X)
 #undef X
 }
@@ -607,17 +627,33 @@ template <typename R, int DIR>
 bool ct_cols(const cplx_t<R>* in, cplx_t<R>* out, int L, int n_in, int n_out, int ncols, int64_t in_si, int64_t out_si,
              int64_t in_sbat, int64_t out_sbat, int nbat, Twiddles& tw, const TuneChoice& tc, cudaStream_t st) {
     const bool f64 = sizeof(R) == 8;
-#define X(N)                                                                                                    \
-    do {                                                                                                        \
-        if (tc.cols_wide)                                                                                       \
-            cols_L<R, DIR, N, 2 * kTileCols<R>>(in, out, n_in, n_out, ncols, in_si, out_si, in_sbat, out_sbat,   \
-                                                nbat, tw.get(N, f64), st);                                      \
-        else                                                                                                    \
-            cols_L<R, DIR, N, kTileCols<R>>(in, out, n_in, n_out, ncols, in_si, out_si, in_sbat, out_sbat, nbat, \
-                                            tw.get(N, f64), st);                                                \
+    // pruned variants: the forward y pass (zero-padded input), the inverse y pass
+    // (truncated output); the tensor's full transforms (FP64) run unpruned
+    const bool hin = 2 * n_in <= L, hout = 2 * n_out <= L;
+    if (hin && hout) return false;
+    if (!hin && !hout && !f64) return false;
+#define C2(N, T, HI, HO) \
+    cols_L<R, DIR, N, T, HI, HO>(in, out, n_in, n_out, ncols, in_si, out_si, in_sbat, out_sbat, nbat, tw.get(N, f64), st)
+#define C1(N, T)                                                \
+    do {                                                        \
+        if (hin)                                                \
+            C2(N, T, true, false);                              \
+        else if (hout)                                          \
+            C2(N, T, false, true);                              \
+        else if constexpr (sizeof(R) == 8)                      \
+            C2(N, T, false, false);                             \
+    } while (0)
+#define X(N)                                                    \
+    do {                                                        \
+        if (tc.cols_wide)                                       \
+            C1(N, 2 * kTileCols<R>);                            \
+        else                                                    \
+            C1(N, kTileCols<R>);                                \
     } while (0)
     MAF_CT_SWITCH(L, X)
 #undef X
+#undef C1
+#undef C2
 }
 
 template <typename R>
