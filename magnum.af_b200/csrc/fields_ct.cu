@@ -202,8 +202,10 @@ __global__ void __launch_bounds__(6 * NB, (kMinBlocks<R, 6 * NB, 576, 288>))
     using C = cplx_t<R>;
     constexpr int L = 2 * NZ;
     constexpr int NC = 6 * NB;  // columns (row, comp, b) = threads
+    constexpr int NT6 = 6 * (NZ + 1) * NB;  // tensor slice: [6][NZ+1][NB]
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C* s = reinterpret_cast<C*>(smem_raw);  // [L][NC]
+    R* tsl = reinterpret_cast<R*>(s + L * NC);
     const int Py = 2 * ny;
     const int ky = blockIdx.y;
     const bool two = ky != 0 && ky != ny;
@@ -212,6 +214,23 @@ __global__ void __launch_bounds__(6 * NB, (kMinBlocks<R, 6 * NB, 576, 288>))
     const int64_t si = (int64_t)Py * pitch;       // z stride
     const int64_t cs = (int64_t)NZ * Py * pitch;  // component stride
     const int col = threadIdx.x;
+    const int64_t tcs = (int64_t)(NZ + 1) * (ny + 1) * nxh;
+    // the tensor rows of this tile go to shared memory asynchronously, under the
+    // spectrum loads and the forward transforms (columns b >= ncv are not read)
+    for (int i = col; i < NT6; i += NC) {
+        const int b = i % NB;
+        const int kz = (i / NB) % (NZ + 1);
+        const int c = i / (NB * (NZ + 1));
+        if (b < ncv) {
+            const R* src = Nred + c * tcs + ((int64_t)kz * (ny + 1) + ky) * nxh + c0 + b;
+            const unsigned dst = (unsigned)__cvta_generic_to_shared(tsl + i);
+            if constexpr (sizeof(R) == 4)
+                asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(dst), "l"(src));
+            else
+                asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(dst), "l"(src));
+        }
+    }
+    asm volatile("cp.async.commit_group;\n" ::);
     {
         const int row = col / (3 * NB);
         const int comp = (col / NB) % 3;
@@ -231,17 +250,18 @@ __global__ void __launch_bounds__(6 * NB, (kMinBlocks<R, 6 * NB, 576, 288>))
             s[(2 * k + 1) * NC + col] = o[k];
         }
     }
+    asm volatile("cp.async.wait_all;\n" ::);
     __syncthreads();
-    const int64_t tcs = (int64_t)(NZ + 1) * (ny + 1) * nxh;
     for (int idx = threadIdx.x; idx < L * NB; idx += NC) {
         const int kz = idx / NB;
         const int b = idx % NB;
         if (b >= ncv) continue;
         const int kzr = kz <= NZ ? kz : L - kz;
         const R sz = kz <= NZ ? (R)1 : (R)-1;
-        const int64_t o = ((int64_t)kzr * (ny + 1) + ky) * nxh + c0 + b;
-        const R Nxx = Nred[o], Nxy = Nred[tcs + o], Nxz = sz * Nred[2 * tcs + o];
-        const R Nyy = Nred[3 * tcs + o], Nyz = sz * Nred[4 * tcs + o], Nzz = Nred[5 * tcs + o];
+        const R* tp = tsl + kzr * NB + b;
+        constexpr int TC = (NZ + 1) * NB;  // component stride of the slice
+        const R Nxx = tp[0], Nxy = tp[TC], Nxz = sz * tp[2 * TC];
+        const R Nyy = tp[3 * TC], Nyz = sz * tp[4 * TC], Nzz = tp[5 * TC];
 #pragma unroll
         for (int row = 0; row < 2; ++row) {
             if (row == 1 && !two) break;
@@ -515,7 +535,8 @@ static void convz_L(cplx_t<R>* S, const R* Nred, int nz, int ny, int nxh, int pi
     if constexpr (L <= 32 && REG) {
         // transforms in registers: one thread per column, NB columns of kx
         constexpr int NBR = sizeof(R) == 4 ? 32 : 16;
-        constexpr size_t smem_r = sizeof(cplx_t<R>) * (size_t)L * 6 * NBR;
+        // spectra [L][6 NBR] plus the tensor slice [6][L/2 + 1][NBR]
+        constexpr size_t smem_r = sizeof(cplx_t<R>) * (size_t)L * 6 * NBR + sizeof(R) * (size_t)6 * (L / 2 + 1) * NBR;
         auto kr = k_convz_reg<R, L / 2, NBR>;
         ct_smem(kr, smem_r);
         dim3 grid((unsigned)ceil_div(nxh, NBR), (unsigned)(ny + 1));
