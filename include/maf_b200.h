@@ -292,6 +292,14 @@ typedef struct maf_string_s* maf_string;
 int maf_string_create(maf_string* out, maf_state state, const maf_state* inputimages, int n_inputimages, int n_interp,
                       double dt, maf_llg llg);
 int maf_string_destroy(maf_string h);
+/* Batched integration (no counterpart in the reference, whose integrate() steps the images one after the
+ * other with the shared adaptive integrator, string_method.cpp:108-121): with substeps > 0 every image
+ * advances its dt by `substeps` fixed RK4 steps of dt/substeps (the deterministic RK4 of
+ * stochastic_integrator.cpp:34-40, the llg's alpha and terms, its own demag buffers and CUDA stream), and
+ * all images are advanced together by one CUDA graph of the ensemble batch (maf_stoch_batch_*); the arc
+ * lengths, re-interpolation and energies stay the reference's.  substeps = 0 returns to the reference's
+ * integration.  Needs a scalar alpha and a scalar Ms. */
+int maf_string_set_batched(maf_string h, int substeps);
 /* StringMethod::step (string_method.cpp:128-132): every image integrated for dt,
  * arc lengths x (FrobeniusNorm of image differences), linear re-interpolation */
 int maf_string_step(maf_string h);

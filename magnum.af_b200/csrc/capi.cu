@@ -1911,8 +1911,28 @@ struct maf_string_s {
     std::vector<double> x, x_interp, E;
     DevBuf tmp;      // [n_interp][3N] copy of the images for the re-interpolation
     DevBuf scratch;  // reduction partials
+    // batched integration (maf_string_set_batched): per image a fixed-step RK4
+    // integrator with its own demag buffers and its own stream; every image is
+    // advanced by one CUDA graph of the ensemble batch
+    int substeps = 0;
+    std::vector<std::unique_ptr<maf_stoch_s>> bits;
+    std::vector<cudaStream_t> bstreams;
+    maf_stoch_batch_s* batch = nullptr;
+    void drop_batch() {
+        if (batch) maf_stoch_batch_destroy(batch);
+        batch = nullptr;
+        for (auto& img : images) img->s.stream = stream;
+        for (auto st : bstreams) {
+            cudaStreamSynchronize(st);
+            cudaStreamDestroy(st);
+        }
+        bstreams.clear();
+        bits.clear();
+        substeps = 0;
+    }
     ~maf_string_s() {
         if (stream) cudaStreamSynchronize(stream);
+        drop_batch();
         images.clear();
         tmp.release();
         scratch.release();
@@ -1978,8 +1998,15 @@ void string_normalize(maf_string_s* h) {
     }
 }
 
-// StringMethod::integrate (string_method.cpp:108-121)
+// StringMethod::integrate (string_method.cpp:108-121); in batched mode every image
+// takes `substeps` RK4 steps of dt/substeps, all images in the ensemble graph
 void string_integrate(maf_string_s* h) {
+    if (h->batch) {
+        MAF_CUDA(cudaStreamSynchronize(h->stream));  // the re-interpolation has written the images
+        const int rc = maf_stoch_batch_steps(h->batch, h->substeps);
+        if (rc != MAF_OK) throw Error(rc, maf_last_error());
+        return;
+    }
     for (auto& img : h->images) {
         const double t0 = img->s.t;
         while (img->s.t < t0 + h->dt) llg_step(h->llg, img.get());
@@ -2014,6 +2041,7 @@ void string_lin_interpolate(maf_string_s* h) {
         }
     }
     string_normalize(h);
+    if (h->batch) MAF_CUDA(cudaStreamSynchronize(h->stream));  // images are read next on their own streams
 }
 
 std::vector<const double*> image_ms(const maf_string_s* h) {
@@ -2189,6 +2217,68 @@ int maf_string_create(maf_string* out, maf_state state, const maf_state* inputim
 
 int maf_string_destroy(maf_string h) {
     return guarded([&] { delete h; });
+}
+
+int maf_string_set_batched(maf_string h, int substeps) {
+    return guarded([&] {
+        check(h && substeps >= 0, "maf_string_set_batched: bad argument");
+        MAF_CUDA(cudaStreamSynchronize(h->stream));
+        h->drop_batch();
+        if (substeps == 0) return;
+        maf_llg_s* l = h->llg;
+        check(!l->has_alpha_field, "StringMethod batched: needs a scalar alpha");
+        const StateD& s0 = h->images[0]->s;
+        check(!s0.has_Ms_field, "StringMethod batched: needs a scalar Ms");
+        try {
+            // demag terms get a copy per image (their spectral buffers are per plan);
+            // the local terms hold no mutable state and are shared
+            std::vector<double> tensor;
+            for (int i = 0; i < h->n_interp; ++i) {
+                cudaStream_t st;
+                MAF_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+                h->bstreams.push_back(st);
+                auto it = std::make_unique<maf_stoch_s>();
+                it->alpha = l->alpha;
+                it->T = 0.0;
+                it->dt = h->dt / substeps;
+                it->mode = 2;  // deterministic RK4 (stochastic_integrator.cpp:34-40)
+                it->member = (unsigned)i;
+                for (auto& t : l->terms) {
+                    if (t->kind != TK_DEMAG) {
+                        it->terms.push_back(t);
+                        continue;
+                    }
+                    auto c = std::make_shared<Term>();
+                    c->kind = TK_DEMAG;
+                    c->p[0] = t->p[0];
+                    if (!t->demag_pbc()) {
+                        if (tensor.empty()) {
+                            tensor.resize(t->demag->tensor_elems());
+                            t->demag->download_tensor(tensor.data(), 0);
+                        }
+                        c->demag_mesh = t->demag_mesh;
+                        c->demag = std::make_unique<Demag>(t->demag_mesh, st, tensor.data());
+                        c->demag->tune = t->demag->tune;
+                    }
+                    it->terms.push_back(c);
+                }
+                h->images[i]->s.stream = st;
+                h->bits.push_back(std::move(it));
+            }
+            std::vector<maf_stoch> its;
+            std::vector<maf_state> sts;
+            for (int i = 0; i < h->n_interp; ++i) {
+                its.push_back(h->bits[i].get());
+                sts.push_back(h->images[i].get());
+            }
+            const int rc = maf_stoch_batch_create(&h->batch, its.data(), sts.data(), h->n_interp);
+            if (rc != MAF_OK) throw Error(rc, maf_last_error());
+            h->substeps = substeps;
+        } catch (...) {
+            h->drop_batch();
+            throw;
+        }
+    });
 }
 
 int maf_string_step(maf_string h) {

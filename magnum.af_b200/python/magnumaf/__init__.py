@@ -134,6 +134,7 @@ _SIGS = {
     "maf_string_create": (_I, [C.POINTER(_P), _P, C.POINTER(_P), _I, _I, _D, _P]),
     "maf_string_destroy": (_I, [_P]),
     "maf_string_step": (_I, [_P]),
+    "maf_string_set_batched": (_I, [_P, _I]),
     "maf_string_calc_E": (_I, [_P, _DP]),
     "maf_string_run": (_I, [_P, C.c_char_p, _D, _D, _I, _I, _I, _DP, C.POINTER(_I)]),
     "maf_string_n_images": (_I, [_P, C.POINTER(_I)]),
@@ -935,6 +936,13 @@ class StringMethod:
 
     def step(self):
         _ck(lib.maf_string_step(self._h))
+
+    def set_batched(self, substeps: int):
+        """Advance all images together in one CUDA graph: each image integrates its
+        dt with `substeps` fixed RK4 steps (its own demag buffers and stream).
+        Not the reference's integration (one adaptive integrator stepping the images
+        one after the other); substeps=0 returns to it."""
+        _ck(lib.maf_string_set_batched(self._h, int(substeps)))
 
     def calc_E(self) -> np.ndarray:
         out = np.empty(self.n_interp)

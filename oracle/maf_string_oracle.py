@@ -80,7 +80,17 @@ class StringMethod:
         for img in self.images:
             img.m = O.normalize(img.m)
 
+    rk4_substeps = 0  # > 0: the batched integration of the device string (maf_string_set_batched)
+
     def integrate(self):
+        if self.rk4_substeps:
+            # every image: rk4_substeps deterministic RK4 steps of dt / rk4_substeps
+            # (stochastic_integrator.cpp:34-40) with the llg's alpha and terms
+            h = self.dt / self.rk4_substeps
+            for img in self.images:
+                for _ in range(self.rk4_substeps):
+                    O.det_rk4_step(img, self.llg.terms, self.llg.alpha, h)
+            return
         for i, img in enumerate(self.images):
             llg = self.llgs[i] if self.per_image else self.llg
             t0 = img.t

@@ -99,3 +99,34 @@ def test_rejects_single_image():
     llg = M.LLGIntegrator(1.0, [M.ExchangeField(1e-11)])
     with pytest.raises(RuntimeError):
         M.StringMethod(M.State(gm, MS, a), [a], 3, 1e-13, llg)
+
+
+@pytest.mark.parametrize("substeps", [1, 4, 5])
+def test_batched_string_matches_oracle(substeps):
+    """maf_string_set_batched: every image advances its dt with `substeps` fixed
+    RK4 steps, all images in one CUDA graph; images, arc lengths and energies
+    after two string steps against the oracle's string with the same integration."""
+    g, o = _setup(6, 6e-14)
+    g.set_batched(substeps)
+    o.rk4_substeps = substeps
+    for _ in range(2):
+        g.step()
+        o.step()
+    for gi, oi in zip(g.images, o.images):
+        assert np.abs(np.asarray(gi.m) - oi.m).max() < 1e-12
+        assert gi.t == pytest.approx(oi.t, rel=1e-14)
+    x, xi = g.x()
+    np.testing.assert_allclose(x, o.x, rtol=1e-11, atol=1e-15)
+    np.testing.assert_allclose(g.calc_E(), o.calc_E(), rtol=1e-11)
+
+
+def test_batched_string_run_and_back_to_reference_mode(tmp_path):
+    g, _ = _setup(5, 5e-14, reverse=True)
+    g.set_batched(2)
+    dE = g.run(str(tmp_path) + os.sep, string_steps=30, verbose=False)
+    assert np.isfinite(dE) and dE > 0
+    assert os.path.exists(tmp_path / "E_barrier.dat")
+    g.set_batched(0)  # the reference's sequential adaptive integration again
+    g.step()
+    with pytest.raises(M.MafError):
+        g.set_batched(-1)
