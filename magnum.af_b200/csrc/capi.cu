@@ -2437,6 +2437,11 @@ int maf_stoch_batch_create(maf_stoch_batch* out, const maf_stoch* integrators, c
                 check(integrators[j] != integrators[i], "maf_stoch_batch_create: an integrator appears twice");
                 check(states[j]->s.stream != states[i]->s.stream,
                       "maf_stoch_batch_create: members must run on distinct streams");
+                // members run concurrently: a demag plan's spectral buffers cannot be shared
+                for (auto& ti : integrators[i]->terms)
+                    for (auto& tj : integrators[j]->terms)
+                        check(ti->kind != TK_DEMAG || ti.get() != tj.get(),
+                              "maf_stoch_batch_create: members share a DemagField; give each member its own");
             }
             b->its.push_back(integrators[i]);
             b->sts.push_back(states[i]);

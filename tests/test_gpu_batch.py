@@ -59,3 +59,17 @@ def test_batch_rejects_shared_state():
     it2, _, _ = _member(1, SPECS[0])
     with pytest.raises(M.MafError):
         M.StochasticBatch([(it, st), (it2, st)])
+
+
+def test_batch_rejects_a_shared_demag_plan():
+    """Members run concurrently, so one DemagField (one set of spectral buffers)
+    cannot serve two of them."""
+    mesh = M.Mesh(16, 16, 1, 2e-9, 2e-9, 2e-9)
+    d = M.DemagField(mesh)
+    members = []
+    for i in range(2):
+        st = M.State(mesh, 8e5, random_m((16, 16, 1), 40 + i))
+        members.append((M.Stochastic_LLG(0.2, 300.0, 2e-14, st, [d, M.ExchangeField(1.3e-11)], seed=5, member=i),
+                        st))
+    with pytest.raises(M.MafError):
+        M.StochasticBatch(members)
