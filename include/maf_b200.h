@@ -86,7 +86,9 @@ int maf_state_precision(maf_state s, int* precision);
  * H_in_Apm(const State&) and Energy_in_J(const State&). */
 
 /* DemagField(Mesh mesh, ...) (magnumaf/src/field_terms/micro/demag_field.cpp:211-213):
- * the Newell tensor is computed on the GPU in FP64 and transformed once. */
+ * the Newell tensor is computed on the GPU in FP64 and transformed once.  The term holds one set of
+ * spectral work buffers: evaluations of it on different streams must not overlap in time (synchronous
+ * calls never do; concurrent ensembles need one DemagField per member). */
 int maf_term_demag_create(maf_term* out, int nx, int ny, int nz, double dx, double dy, double dz);
 /* DemagField from a reduced spectral tensor saved earlier with maf_term_demag_tensor (the disk cache of
  * get_Nfft(mesh, verbose, caching=true), demag_field.cpp:185-199, and util/cache_manager.cpp:49-116). */
