@@ -217,17 +217,21 @@ __global__ void __launch_bounds__(6 * NB, (kMinBlocks<R, 6 * NB, 576, 288>))
     const int64_t tcs = (int64_t)(NZ + 1) * (ny + 1) * nxh;
     // the tensor rows of this tile go to shared memory asynchronously, under the
     // spectrum loads and the forward transforms (columns b >= ncv are not read)
-    for (int i = col; i < NT6; i += NC) {
-        const int b = i % NB;
-        const int kz = (i / NB) % (NZ + 1);
-        const int c = i / (NB * (NZ + 1));
+    // (thread col = (component c, column b): one pointer step per kz row)
+    static_assert(NT6 == NC * (NZ + 1), "one slice column per thread");
+    {
+        const int c = col / NB, b = col % NB;
         if (b < ncv) {
-            const R* src = Nred + c * tcs + ((int64_t)kz * (ny + 1) + ky) * nxh + c0 + b;
-            const unsigned dst = (unsigned)__cvta_generic_to_shared(tsl + i);
-            if constexpr (sizeof(R) == 4)
-                asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(dst), "l"(src));
-            else
-                asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(dst), "l"(src));
+            const R* src = Nred + c * tcs + (int64_t)ky * nxh + c0 + b;
+            const int64_t sstep = (int64_t)(ny + 1) * nxh;
+            unsigned dst = (unsigned)__cvta_generic_to_shared(tsl + c * (NZ + 1) * NB + b);
+#pragma unroll 1
+            for (int kz = 0; kz <= NZ; ++kz, src += sstep, dst += NB * sizeof(R)) {
+                if constexpr (sizeof(R) == 4)
+                    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(dst), "l"(src));
+                else
+                    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(dst), "l"(src));
+            }
         }
     }
     asm volatile("cp.async.commit_group;\n" ::);
