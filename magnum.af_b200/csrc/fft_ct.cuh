@@ -279,6 +279,18 @@ __device__ __forceinline__ void ct_fft_in(cplx_t<R>* s, int sb, const cplx_t<R>*
     if constexpr (sizeof...(RS) > 0) ct_run<R, DIR, BFAST, L, R0, NB, NT, HOUT, RS...>(s, sb, tw);
 }
 
+// ct_fft_in with a hook between the first stage and the others: the first stage
+// ends with a barrier, so when mid() runs no thread reads the load source any more
+// (a pipelined kernel refills it there).
+template <typename R, int DIR, bool BFAST, int L, int NB, int NT, bool HIN, typename LD, typename MID, int R0,
+          int... RS>
+__device__ __forceinline__ void ct_fft_in_hook(cplx_t<R>* s, int sb, const cplx_t<R>* __restrict__ tw, LD&& ld,
+                                               MID&& mid, Radices<R0, RS...>) {
+    ct_stage_in<R, R0, DIR, BFAST, L, NB, NT, HIN>(s, sb, ld);
+    mid();
+    if constexpr (sizeof...(RS) > 0) ct_run<R, DIR, BFAST, L, R0, NB, NT, false, RS...>(s, sb, tw);
+}
+
 // shared memory -> ... -> last stage -> global (HOUT: only outputs i < L/2 are stored)
 template <typename R, int DIR, bool BFAST, int L, int NB, int NT, bool HOUT = false, typename ST, int... RS>
 __device__ __forceinline__ void ct_fft_out(cplx_t<R>* s, int sb, const cplx_t<R>* __restrict__ tw, ST&& st,

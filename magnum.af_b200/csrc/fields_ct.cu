@@ -30,6 +30,16 @@ static_assert(kRunCells == 2 || kRunCells == 4, "run length");
 #define MAF_XINV_THREADS 576
 #endif
 
+// Byte offset of the staging buffer behind the transform tile of k_xfwd_pipe
+// (16-byte aligned), and that kernel's shared memory.
+template <typename R, int LC, int NB> constexpr size_t xfwd_stage_offset() {
+    constexpr size_t SB = (LC - 1) + ((LC - 1) >> 4) + 1;
+    return (sizeof(cplx_t<R>) * NB * SB + 15) / 16 * 16;
+}
+template <typename R, int LC, int NB> constexpr size_t xfwd_pipe_smem() {
+    return xfwd_stage_offset<R, LC, NB>() + sizeof(R) * NB * LC;
+}
+
 // ------------------------------------------------------------------ x forward
 // HIN: n_in <= LC, so the packed values k >= LC/2 are the zero padding (pruned
 // from the first stage)
@@ -92,6 +102,69 @@ __global__ void __launch_bounds__(NT) k_xfwd_ct(const R* __restrict__ in, int n_
         C* o = out + row * pitch;
         o[k] = cadd(E_, t);
         if (k < LC / 2) o[LC - k] = cconj(csub(E_, t));
+    }
+}
+
+// x forward, persistent and pipelined: each CTA walks tiles of NB rows; the m rows
+// of the next tile are copied into a shared-memory staging buffer with cp.async
+// while the current tile's transform runs (issued right after the first stage,
+// the staging buffer's only reader).  For a scalar Ms, n_in <= LC (zero-padded
+// half pruned) and rows of whole 16-byte chunks; the same arithmetic as k_xfwd_ct.
+template <typename R, int LC, int NB, int NT>
+__global__ void __launch_bounds__(NT, 4) k_xfwd_pipe(const R* __restrict__ in, int n_in, int64_t rows, R ms,
+                                                  cplx_t<R>* __restrict__ out, int pitch,
+                                                  const cplx_t<R>* __restrict__ tw,
+                                                  const cplx_t<R>* __restrict__ twP) {
+    using C = cplx_t<R>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C* s = reinterpret_cast<C*>(smem_raw);
+    constexpr int SB = (LC - 1) + ((LC - 1) >> 4) + 1;
+    R* stage = reinterpret_cast<R*>(smem_raw + xfwd_stage_offset<R, LC, NB>());
+    constexpr int E16 = 16 / (int)sizeof(R);
+    const int64_t ntiles = (rows + NB - 1) / NB;
+    auto prefetch = [&](int64_t tile) {
+        const int64_t r0 = tile * NB;
+        const int nrow = (int)min((int64_t)NB, rows - r0);
+        const int nchunk = nrow * n_in / E16;
+        const R* src = in + r0 * n_in + threadIdx.x * E16;
+        unsigned dst = (unsigned)__cvta_generic_to_shared(stage + threadIdx.x * E16);
+#pragma unroll 1
+        for (int q = threadIdx.x; q < nchunk; q += NT, src += NT * E16, dst += NT * 16)
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(src));
+        asm volatile("cp.async.commit_group;\n" ::);
+    };
+    int64_t tile = blockIdx.x;
+    if (tile < ntiles) prefetch(tile);
+    for (; tile < ntiles; tile += gridDim.x) {
+        const int64_t r0 = tile * NB;
+        asm volatile("cp.async.wait_all;\n" ::);
+        __syncthreads();
+        auto ld = [&](int b, int k) -> C {
+            const int x0 = 2 * k;
+            if (r0 + b >= rows || x0 >= n_in) return mk((R)0, (R)0);
+            const C v = *reinterpret_cast<const C*>(stage + b * n_in + x0);
+            return mk(v.x * ms, v.y * ms);
+        };
+        const int64_t next = tile + gridDim.x;
+        ct_fft_in_hook<R, -1, false, LC, NB, NT, true>(
+            s, SB, tw, ld, [&] { if (next < ntiles) prefetch(next); }, typename CtPlan<LC>::T());
+        const R half = (R)0.5;
+        constexpr int KH = LC / 2 + 1;
+        for (int idx = threadIdx.x; idx < NB * KH; idx += NT) {
+            const int b = idx / KH;
+            const int k = idx - b * KH;
+            const int64_t row = r0 + b;
+            if (row >= rows) continue;
+            const C Zk = s[spad(k) + b * SB];
+            const C Zm = s[spad(k == 0 ? 0 : LC - k) + b * SB];
+            const C E_ = cscale(cadd(Zk, cconj(Zm)), half);
+            const C O = cscale(cmul_i<-1>(csub(Zk, cconj(Zm))), half);
+            const C t = cmul(twP[k], O);
+            C* o = out + row * pitch;
+            o[k] = cadd(E_, t);
+            if (k < LC / 2) o[LC - k] = cconj(csub(E_, t));
+        }
+        __syncthreads();  // s is rewritten by the next tile's first stage
     }
 }
 
@@ -507,6 +580,30 @@ static void xfwd_L(const R* in, int n_in, int64_t rows, int64_t rows_pc, const R
     static_assert(NT <= kMaxFftThreads, "CTA size");
     constexpr int SB = (LC - 1) + ((LC - 1) >> 4) + 1;
     const size_t smem = sizeof(cplx_t<R>) * (size_t)NB * SB;
+    if constexpr (HIN) {
+        // the pipelined persistent kernel: scalar Ms, rows of whole 16-byte chunks
+        constexpr int E16 = 16 / (int)sizeof(R);
+        if (!msf && n_in % E16 == 0 && (uintptr_t)in % 16 == 0) {
+            auto kp = k_xfwd_pipe<R, LC, NB, NT>;
+            const size_t smem_p = xfwd_pipe_smem<R, LC, NB>();
+            ct_smem(kp, smem_p);
+            static int per_sm[2] = {0, 0}, sms = 0;  // per precision, measured once per process
+            int& ps = per_sm[sizeof(R) == 8];
+            if (!ps) {
+                MAF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ps, kp, NT, smem_p));
+                int dev = 0;
+                MAF_CUDA(cudaGetDevice(&dev));
+                MAF_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+                if (ps < 1) ps = 1;
+            }
+            const int64_t ntiles = ceil_div(rows, NB);
+            const unsigned grid = (unsigned)std::min<int64_t>(ntiles, (int64_t)ps * sms);
+            kp<<<grid, NT, smem_p, st>>>(in, n_in, rows, ms, out, pitch, static_cast<const cplx_t<R>*>(tw),
+                                         static_cast<const cplx_t<R>*>(twP));
+            MAF_LAUNCH_CHECK();
+            return;
+        }
+    }
     auto k = k_xfwd_ct<R, LC, NB, NT, HIN>;
     ct_smem(k, smem);
     k<<<(unsigned)ceil_div(rows, NB), NT, smem, st>>>(in, n_in, rows, rows_pc, msf, ms, out, pitch,
