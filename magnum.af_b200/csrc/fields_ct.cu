@@ -176,7 +176,7 @@ __global__ void __launch_bounds__(NT, 4) k_xfwd_pipe(const R* __restrict__ in, i
 // HIN: n_in <= L/2 (zero-padded input), HOUT: n_out <= L/2 (truncated output);
 // both prune the transform at compile time
 template <typename R, int DIR, int L, int NB, int NT, bool HIN, bool HOUT>
-__global__ void __launch_bounds__(NT, (kMinBlocks<R, NT, 1024, 512>)) k_cols_ct(const cplx_t<R>* in, cplx_t<R>* out, int n_in, int n_out, int ncols,
+__global__ void __launch_bounds__(NT, (kMinBlocks<R, NT * (L * NB / kE > NT ? L * NB / kE / NT : 1), 1024, 512>)) k_cols_ct(const cplx_t<R>* in, cplx_t<R>* out, int n_in, int n_out, int ncols,
                                                 int64_t in_si, int64_t out_si, int64_t in_sbat, int64_t out_sbat,
                                                 const cplx_t<R>* __restrict__ tw) {
     using C = cplx_t<R>;
@@ -564,6 +564,14 @@ template <typename R> constexpr int kTileC = sizeof(R) == 4 ? 8192 : 4096;
 #define MAF_COLS_TILE_F32 8192
 #endif
 template <typename R> constexpr int kTileCols = sizeof(R) == 4 ? MAF_COLS_TILE_F32 : 4096;
+// radix-16 butterflies per thread and stage in the FP32 y passes (1 or 2; a build
+// option): two halve the CTA to 256 threads at 128 registers, two CTAs per SM as
+// with one, and each thread keeps twice the loads in flight
+#ifndef MAF_COLS_BPT_F32
+#define MAF_COLS_BPT_F32 2
+#endif
+template <typename R> constexpr int kColsBpt = sizeof(R) == 4 ? MAF_COLS_BPT_F32 : 1;
+static_assert(MAF_COLS_BPT_F32 == 1 || MAF_COLS_BPT_F32 == 2, "butterflies per thread");
 constexpr int cmax(int a, int b) { return a > b ? a : b; }
 constexpr int cmin(int a, int b) { return a < b ? a : b; }
 constexpr int pow2floor(int x) {
@@ -616,7 +624,7 @@ template <typename R, int DIR, int L, int TILE, bool HIN, bool HOUT>
 static void cols_L(const cplx_t<R>* in, cplx_t<R>* out, int n_in, int n_out, int ncols, int64_t in_si, int64_t out_si,
                    int64_t in_sbat, int64_t out_sbat, int nbat, const void* tw, cudaStream_t st) {
     constexpr int NB = pow2floor(cmin(32, cmax(1, TILE / L)));
-    constexpr int NT = L * NB / kE;
+    constexpr int NT = L * NB / (kE * kColsBpt<R>) > 0 ? L * NB / (kE * kColsBpt<R>) : 1;
     static_assert(NT <= 1024, "CTA size");
     const size_t smem = sizeof(cplx_t<R>) * (size_t)NB * ((L - 1) + ((L - 1) >> 4) + 1);
     auto k = k_cols_ct<R, DIR, L, NB, NT, HIN, HOUT>;
