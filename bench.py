@@ -85,6 +85,32 @@ def pass_bytes(r, nx=None, ny=None, nz=None):
     }
 
 
+def interval_bytes(name, r, nx=None, ny=None, nz=None):
+    """Algorithmic bytes of one interval of a Runge-Kutta attempt profile
+    (LLGIntegrator.attempt_profile): the field passes (the x inverse with the LLG
+    epilogue: spectrum + m for the stencils + the FP64 m of the cross product, k
+    written in FP64), the FP32 copy of m, the stage combine m + sum a_j k_j over
+    N FP64 k buffers (FP64 staged m written, plus its FP32 copy in the FP32-field
+    form) and the finalize (m and N k's read, the candidate written)."""
+    nx, ny, nz = (NX if nx is None else nx), (NY if ny is None else ny), (NZ if nz is None else nz)
+    N = nx * ny * nz
+    pb = pass_bytes(r, nx, ny, nz)
+    if name in ("x_fwd", "y_fwd", "z_conv", "y_inv"):
+        return pb[name]
+    if name == "x_inv_local":  # LLG epilogue
+        spec = 3 * (nx + 1) * ny * nz * 2 * r
+        return spec + (3 * N * 4 + 3 * N * 8 if r == 4 else 3 * N * 8) + 3 * N * 8
+    if name == "stage_m32":
+        return 3 * N * 8 + 3 * N * 4
+    if name.startswith("rk_combine_k"):
+        k = int(name[len("rk_combine_k"):])
+        return (k + 1) * 3 * N * 8 + 3 * N * 8 + (3 * N * 4 if r == 4 else 0)
+    if name.startswith("rk_finalize_k"):
+        k = int(name[len("rk_finalize_k"):])
+        return (k + 1) * 3 * N * 8 + 3 * N * 8
+    return None
+
+
 def peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -96,7 +122,8 @@ def peaks():
 
 
 def ncu_traffic():
-    """Per-launch DRAM bytes of the dominant pass from the committed ncu summary."""
+    """Per-launch DRAM bytes of the dominant pass from the committed ncu summary
+    (a 512x512x16 capture scaled to the full launch by the tiles processed)."""
     p = os.path.join(ROOT, "profiles", "traffic_1024x1024x16.txt")
     out = {}
     try:
@@ -228,6 +255,96 @@ def run_reference(args):
         "e2e": {"value": value, "unit": "evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+def oracle_parity_slab(M, terms_of, stream, nz_slab=2):
+    """The device's H_eff against the FP64 oracle on a 1024 x 1024 x nz_slab slab of
+    the workload (x rows of 1024 cells and 2048-point padded y columns: the same x
+    and y kernels as the full mesh), the oracle fed the device's own tensor (parity
+    on identical inputs; the oracle's own Newell sums differ at their rounding
+    noise).  Returns relative L2 / max errors of the FP64 and FP32-field forms."""
+    import maf_oracle as O
+    import torch
+
+    threads = os.cpu_count() or 1
+    O.FFT_WORKERS = threads
+    mesh = M.Mesh(NX, NY, nz_slab, DX, DX, DX)
+    om = O.Mesh(NX, NY, nz_slab, DX, DX, DX)
+    m, h_ext = workload(nz=nz_slab)
+    d = M.DemagField(mesh)
+    gterms = terms_of(d, h_ext)
+    llg = M.LLGIntegrator(0.01, gterms, "DP45")
+    s64 = M.State(mesh, MS, m)
+    s32 = M.State(mesh, MS, m, precision="fp32_field")
+    s64.set_stream(stream.cuda_stream)
+    s32.set_stream(stream.cuda_stream)
+    h64 = llg.H_in_Apm(s64)
+    h32 = np.asarray(llg.H_in_Apm_f32(s32), dtype=np.float64)
+    torch.cuda.synchronize()
+    oterms = [O.DemagField(om, N_real=d.get_N(symmetric=True)), O.ExchangeField(A_EX), O.CubicAnisotropyField(K1),
+              O.ExternalField(h_ext)]
+    ref = O.Heff_in_Apm(oterms, O.State(om, MS, m))
+
+    def errs(h):
+        dd = h - ref
+        return {"l2": float(np.linalg.norm(dd) / np.linalg.norm(ref)), "max": float(np.abs(dd).max() / np.abs(ref).max())}
+
+    return {"mesh": "%dx%dx%d slab of the workload" % (NX, NY, nz_slab), "tensor": "device tensor fed to the oracle",
+            "fp64": errs(h64), "fp32_field": errs(h32), "tolerance": {"fp64": 1e-12, "fp32_field": 1e-5}}
+
+
+def rk_step_figures(M, mesh, m, terms, stream, steps, peak):
+    """DP45 on the full mesh in both forms: one Runge-Kutta attempt timed kernel by
+    kernel (CUDA events, mean of 3 attempts at the step size the controller has
+    reached), with each kernel's algorithmic bytes / time against the HBM peak, and
+    a plain LLGIntegrator.step loop (no dense output): steps/s, attempts and
+    simulated ns per hour of wall time."""
+    import torch
+
+    out = {}
+    for prec in ("fp32_field", "fp64"):
+        r = 4 if prec == "fp32_field" else 8
+        llg = M.LLGIntegrator(0.01, terms, "DP45")
+        st = M.State(mesh, MS, m, precision=prec)
+        st.set_stream(stream.cuda_stream)
+        llg.steps(st, 3)  # warm-up; grows the first step from hmin
+        torch.cuda.synchronize()
+        c0 = llg.counters()
+        t_sim0 = st.t
+        t0 = time.perf_counter()
+        llg.steps(st, steps)
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+        c1 = llg.counters()
+        reps = 3
+        agg = {}
+        for _ in range(reps):
+            for name, ms in llg.attempt_profile(st, llg.h):
+                if name in ("start", "attempt"):
+                    continue
+                a = agg.setdefault(name, [0.0, 0])
+                a[0] += ms
+                a[1] += 1
+        kernels = {}
+        attempt_ms = 0.0
+        for name, (ms, cnt) in agg.items():
+            per_attempt_ms = ms / reps
+            attempt_ms += per_attempt_ms
+            b = interval_bytes(name, r)
+            gbs = b * cnt / (ms * 1e-3) / 1e9 if b else None
+            kernels[name] = {"launches_per_attempt": cnt // reps, "ms_per_attempt": per_attempt_ms,
+                             "gbs": gbs, "frac": gbs / peak if gbs else None}
+        rk_only = sum(v["ms_per_attempt"] for k, v in kernels.items() if k.startswith("rk_") or k == "stage_m32")
+        out[prec] = {
+            "steps": steps, "attempts": int((c1["accepted"] + c1["rejected"]) - (c0["accepted"] + c0["rejected"])),
+            "wall_s": wall, "steps_per_s": steps / wall,
+            "sim_ns_per_hour": (st.t - t_sim0) * 1e9 / wall * 3600.0, "sim_s": st.t - t_sim0,
+            "attempt_ms_profiled": attempt_ms, "rk_kernels_share": rk_only / attempt_ms if attempt_ms else None,
+            "kernels": kernels,
+        }
+        del st, llg
+    out["scheme"] = "DP45, alpha 0.01, default controller (atol = rtol = 1e-6), from the random initial m"
+    return out
 
 
 def other_configs(M, stream):
@@ -421,6 +538,20 @@ def run_ours(args):
         for name, ms in llg.heff_device_profile(s32, m32_dev.data_ptr(), H32.data_ptr()):
             passes.setdefault(name, []).append(ms)
     pass_ms = {k: float(np.mean(v)) for k, v in passes.items()}
+    passes64 = {}
+    for _ in range(nprof):
+        for name, ms in llg.heff_device_profile(s64, m64_dev.data_ptr(), H64.data_ptr()):
+            passes64.setdefault(name, []).append(ms)
+    pass_ms64 = {k: float(np.mean(v)) for k, v in passes64.items()}
+    # the local terms alone (exchange, cubic, Zeeman: the k_local_epi kernel, no demag)
+    loc = M.LLGIntegrator(0.01, terms[1:], "DP45")
+    loc_ms = {}
+    for prec_name, st_, mp_, hp_ in (("fp32_field", s32, m32_dev, H32), ("fp64", s64, m64_dev, H64)):
+        v = []
+        for _ in range(nprof):
+            v += [ms for _, ms in loc.heff_device_profile(st_, mp_.data_ptr(), hp_.data_ptr())]
+        loc_ms[prec_name] = float(np.mean(v))
+    del loc
     bytes32 = pass_bytes(4)
     dominant = max(pass_ms, key=pass_ms.get)
     peak, peak_kind = peaks()
@@ -428,6 +559,29 @@ def run_ours(args):
     traffic = ncu_traffic().get(dominant)
     eval_bytes = sum(bytes32.values())
     eval_gbs = eval_bytes / (ms32 / args.steps * 1e-3) / 1e9
+    # every kernel of the field path: algorithmic bytes / CUDA-event time against the peak
+    bytes64 = pass_bytes(8)
+    N = NX * NY * NZ
+    kernels = {}
+    for form, pm, by, r in (("fp32_field", pass_ms, bytes32, 4), ("fp64", pass_ms64, bytes64, 8)):
+        for name, ms in pm.items():
+            gbs = by[name] / (ms * 1e-3) / 1e9
+            kernels["%s/%s" % (form, name)] = {"ms": ms, "bytes": by[name], "gbs": gbs, "frac": gbs / peak}
+        lb = 2 * 3 * N * r  # m read, H written (neighbours from cache)
+        gbs = lb / (loc_ms[form] * 1e-3) / 1e9
+        kernels["%s/local_terms" % form] = {"ms": loc_ms[form], "bytes": lb, "gbs": gbs, "frac": gbs / peak}
+
+    # the device's field against the FP64 oracle on a slab with the full mesh's x and y lengths
+    parity = None
+    if not args.no_oracle_parity:
+        parity = oracle_parity_slab(
+            M, lambda d, hx: [d, M.ExchangeField(A_EX), M.CubicAnisotropyField(K1), M.ExternalField.uniform(*hx)],
+            stream)
+
+    # the time step: DP45 attempt split by kernel, and a plain step loop in both forms
+    rk = None
+    if not args.no_trajectory and args.rk_steps > 0:
+        rk = rk_step_figures(M, mesh, m, terms, stream, args.rk_steps, peak)
 
     # end to end through the C ABI with pinned host buffers
     m_host = torch.from_numpy(m_norm.copy()).pin_memory()
@@ -496,9 +650,15 @@ def run_ours(args):
         "trajectory": traj,
         "configs": cfgs,
         "passes_ms": pass_ms,
+        "passes_ms_fp64": pass_ms64,
+        "kernels": kernels,
+        "rel_err_vs_oracle": parity,
+        "rk_step": rk,
         "eval_roofline": {"bytes": eval_bytes, "achieved_gbs": eval_gbs, "frac": eval_gbs / peak},
         "roofline": {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
+                     "traffic_source": "profiles/traffic_1024x1024x16.txt: ncu dram bytes of a 512x512x16 launch "
+                                       "of the same kernel, scaled by the tiles processed (not measured in this run)",
                      "algorithmic_bytes": bytes32[dominant]},
         "e2e": {"value": world * e2e_steps / (ms_e2e * 1e-3), "unit": "evals/s", "h2d_bytes_per_step": n3 * 4,
                 "d2h_bytes_per_step": n3 * 4,
@@ -532,6 +692,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default kernel variants")
+    ap.add_argument("--no-oracle-parity", action="store_true", help="skip the slab comparison with the FP64 oracle")
+    ap.add_argument("--rk-steps", type=int, default=300, help="DP45 steps of the plain step loop per form")
     ap.add_argument("--mesh", type=int, nargs=3, default=None, metavar=("NX", "NY", "NZ"),
                     help="smaller mesh for profiling captures (the reported metric is defined at 1024 1024 16)")
     args = ap.parse_args()

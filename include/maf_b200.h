@@ -210,6 +210,15 @@ int maf_term_demag_set_tune(maf_term t, const int choices[3]);
 int maf_llg_heff_device_profile(maf_llg l, maf_state s, const void* m_dev, void* H_dev, double* pass_ms,
                                 int max_passes, int* npasses);
 int maf_llg_pass_name(maf_llg l, maf_state s, int index, char* buf, int buflen);
+/* One Runge-Kutta attempt of the integrator's scheme with step dt from the state's m
+ * (AdaptiveRungeKutta's stage loop, adaptive_runge_kutta.cpp:113-173; the state is not
+ * changed) with a CUDA event after every kernel: synchronises and returns the duration in
+ * ms of each interval -- the FP32 copy of m ("stage_m32"), every stage's combine
+ * ("rk_combine_kN": N = FP64 k buffers read) and field passes, and the finalize
+ * ("rk_finalize_kN": sumbk, error norm and candidate from N distinct k buffers).  Names
+ * come from maf_llg_profile_name (valid until the next profile on this integrator). */
+int maf_llg_attempt_profile(maf_llg l, maf_state s, double dt, double* ms_out, int max_entries, int* n_entries);
+int maf_llg_profile_name(maf_llg l, int index, char* buf, int buflen);
 /* dm/dt = LLGIntegrator::f(state) (llg_integrator.cpp:18-38) */
 int maf_llg_dmdt(maf_llg l, maf_state s, double* dmdt_host);
 /* LLGIntegrator::integrate_dense (llg_integrator.cpp:68-104): rows of (t, <mx>, <my>, <mz>),
@@ -352,12 +361,19 @@ int maf_cnn_train_step(maf_cnn h, const float* x_dev, const float* target_dev, i
  * between steps while other streams run (cudaMalloc can synchronise the
  * device), or an application that has reserved all free device memory.
  * Its scratch is a fixed 128 KiB static device array per device, which limits
- * ncells to 33554432 (2^25); larger ncells return MAF_ERR_BADARG.  The first
- * call on a device looks up that array's address.  Work is queued on
- * cuda_stream (NULL: the legacy default stream) and the call returns after that
- * stream has finished it.  Calls that overlap on one device (other streams or
- * host threads, unordered) share the scratch and race: both results are then
- * undefined. */
+ * ncells to 33554432 (2^25); larger ncells return MAF_ERR_BADARG.
+ * CUDA loads the code and that array lazily, on first use in a device's
+ * context, and the load allocates device memory and may synchronise the
+ * device.  maf_state_create performs that load, so once a state exists on the
+ * device no call allocates.  A caller that passes a field it did not get from
+ * a state should make one warm-up call before it reserves device memory or
+ * starts concurrent streams.  Work is queued on cuda_stream (NULL: the legacy
+ * default stream) and the call returns after that stream has finished it.  A
+ * state's own stream is non-blocking, so a field of a state must be read on the
+ * state's stream (the one given to maf_state_set_stream) or after that stream
+ * has been synchronised; otherwise <m> may be taken from a half-updated field.
+ * Calls that overlap on one device (other streams or host threads, unordered)
+ * share the scratch and race: both results are then undefined. */
 int maf_mean_m_noalloc(const double* m_dev, long long ncells, double out[3], void* cuda_stream);
 
 #ifdef __cplusplus

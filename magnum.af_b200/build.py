@@ -25,15 +25,21 @@ INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
           "--expt-relaxed-constexpr", "-I" + CSRC, "-I" + INCLUDE]
+# object name -> (source, extra nvcc options); fields_ct.cu is compiled once per
+# group of its template instantiations (see the end of that file) so that the
+# groups build in parallel
 SOURCES = {
-    "fields.cu": [],
-    "fields_ct.cu": [],
-    "llg.cu": [],
-    "newell.cu": ["-fmad=false"],
-    "capi.cu": [],
-    "noalloc.cu": [],
-    "cnn.cu": [],
+    "fields.o": ("fields.cu", []),
+    "llg.o": ("llg.cu", []),
+    "newell.o": ("newell.cu", ["-fmad=false"]),
+    "capi.o": ("capi.cu", []),
+    "noalloc.o": ("noalloc.cu", []),
+    "cnn.o": ("cnn.cu", []),
 }
+for _part in (1, 2, 3):
+    for _real in (4, 8):
+        SOURCES["fields_ct_%d_%d.o" % (_part, _real)] = (
+            "fields_ct.cu", ["-DMAF_CT_PART=%d" % _part, "-DMAF_CT_REAL=%d" % _real])
 
 
 def nvcc() -> str:
@@ -51,19 +57,35 @@ def _deps_mtime() -> float:
     return max(mt, os.path.getmtime(__file__))
 
 
+def _headers_mtime() -> float:
+    """Newest header (csrc/*.cuh, *.hpp, include/*) or this script."""
+    mt = os.path.getmtime(__file__)
+    for d in (CSRC, INCLUDE):
+        for f in os.listdir(d):
+            if not f.endswith(".cu"):
+                mt = max(mt, os.path.getmtime(os.path.join(d, f)))
+    return mt
+
+
 def build(force: bool = False, verbose: bool = False) -> str:
     os.makedirs(LIBDIR, exist_ok=True)
     os.makedirs(OBJDIR, exist_ok=True)
     if not force and os.path.exists(LIB) and os.path.getmtime(LIB) >= _deps_mtime():
         return LIB
     nv = nvcc()
+    hdr = _headers_mtime()
+    user = os.environ.get("MAF_NVCC_EXTRA", "")
 
     def compile_one(item):
-        src, extra = item
-        obj = os.path.join(OBJDIR, src.replace(".cu", ".o"))
+        objname, (src, extra) = item
+        obj = os.path.join(OBJDIR, objname)
+        # an object is rebuilt when its source, a header or this script is newer
+        # (always with --force or extra user options)
+        if (not force and not user and os.path.exists(obj)
+                and os.path.getmtime(obj) >= max(hdr, os.path.getmtime(os.path.join(CSRC, src)))):
+            return obj
         # MAF_NVCC_EXTRA: additional nvcc options, e.g. -DMAF_COLS_TILE_F32=16384 (tile sizes)
-        user = os.environ.get("MAF_NVCC_EXTRA", "").split()
-        cmd = [nv, *COMMON, *ARCH, *extra, *user, "-c", os.path.join(CSRC, src), "-o", obj]
+        cmd = [nv, *COMMON, *ARCH, *extra, *user.split(), "-c", os.path.join(CSRC, src), "-o", obj]
         if verbose:
             print(" ".join(cmd), flush=True)
         r = subprocess.run(cmd, capture_output=True, text=True)
@@ -71,7 +93,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
             raise RuntimeError(f"nvcc failed for {src}:\n{r.stdout}\n{r.stderr}")
         return obj
 
-    with ThreadPoolExecutor(max_workers=min(4, os.cpu_count() or 1)) as ex:
+    with ThreadPoolExecutor(max_workers=min(12, os.cpu_count() or 1)) as ex:
         objs = list(ex.map(compile_one, SOURCES.items()))
     tmp = LIB + ".tmp"
     cmd = [nv, *ARCH, "-shared", "-Xcompiler", "-fPIC", "-cudart", "static", *objs, "-o", tmp]

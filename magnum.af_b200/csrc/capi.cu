@@ -227,6 +227,7 @@ struct maf_llg_s {
     DevBuf k[8];
     DevBuf mstage64, mstage32, mcand, partials, errbuf, h32out;
     unsigned long long accumulated_steps = 0;
+    std::vector<std::string> prof_names;  // interval names of the last maf_llg_attempt_profile
 };
 
 namespace {
@@ -249,16 +250,24 @@ std::vector<Term*> raw_terms(const std::vector<std::shared_ptr<Term>>& v) {
 
 // Field of `terms` on the state's current m with the given epilogue.
 void eval_on_state(maf_state_s* st, const std::vector<Term*>& terms, EpilogueArgs ep, double* energy = nullptr,
-                   const double* m64_for_llg = nullptr) {
+                   const double* m64_for_llg = nullptr, PassMarks* marks = nullptr) {
     StateD& s = st->s;
     if (ep.kind == EPI_LLG && !ep.llg.m64) ep.llg.m64 = m64_for_llg ? m64_for_llg : s.m64.as<double>();
     if (s.precision == PREC_FP32_FIELD) {
         ensure_m32(st);
-        eval_terms<float>(terms, s.md, s.m32.as<float>(), s.msinfo(), ep, s.stream, st->scratch, energy);
+        eval_terms<float>(terms, s.md, s.m32.as<float>(), s.msinfo(), ep, s.stream, st->scratch, energy, marks);
     } else {
-        eval_terms<double>(terms, s.md, s.m64.as<double>(), s.msinfo(), ep, s.stream, st->scratch, energy);
+        eval_terms<double>(terms, s.md, s.m64.as<double>(), s.msinfo(), ep, s.stream, st->scratch, energy, marks);
     }
 }
+
+// interval names of the attempt profile that carry the number of FP64 k
+// buffers a Runge-Kutta kernel reads (its algorithmic bytes depend on it)
+const char* const kCombineNames[8] = {"rk_combine_k0", "rk_combine_k1", "rk_combine_k2", "rk_combine_k3",
+                                      "rk_combine_k4", "rk_combine_k5", "rk_combine_k6", "rk_combine_k7"};
+const char* const kFinalizeNames[9] = {"rk_finalize_k0", "rk_finalize_k1", "rk_finalize_k2",
+                                       "rk_finalize_k3", "rk_finalize_k4", "rk_finalize_k5",
+                                       "rk_finalize_k6", "rk_finalize_k7", "rk_finalize_k8"};
 
 LLGParams llg_params(const maf_llg_s* l, double scale) {
     LLGParams p;
@@ -273,7 +282,8 @@ LLGParams llg_params(const maf_llg_s* l, double scale) {
 
 // One RK attempt of `sch` with step dt; leaves m + sumbk (normalised per
 // norm_mode) in l->mcand and returns the error norm.
-double rk_attempt(maf_llg_s* l, maf_state_s* st, const Scheme& sch, double dt, int norm_mode) {
+double rk_attempt(maf_llg_s* l, maf_state_s* st, const Scheme& sch, double dt, int norm_mode,
+                  PassMarks* marks = nullptr) {
     StateD& s = st->s;
     const int64_t N = s.md.N();
     const int64_t n3 = 3 * N;
@@ -282,7 +292,7 @@ double rk_attempt(maf_llg_s* l, maf_state_s* st, const Scheme& sch, double dt, i
     l->mstage64.ensure(sizeof(double) * n3);
     if (f32) l->mstage32.ensure(sizeof(float) * n3);
     l->mcand.ensure(sizeof(double) * n3);
-    l->partials.ensure(sizeof(double) * 148 * 8 + 64);
+    l->partials.ensure(sizeof(double) * sm_count() * 8 + 64);
     l->errbuf.ensure(sizeof(double) * 4);
     auto terms = raw_terms(l->terms);
     const double kscale = sch.dt_in_k ? dt : 1.0;
@@ -294,7 +304,12 @@ double rk_attempt(maf_llg_s* l, maf_state_s* st, const Scheme& sch, double dt, i
         ep.llg = llg_params(l, kscale);
         if (stg == 0) {
             ep.llg.m64 = s.m64.as<double>();
-            eval_on_state(st, terms, ep);
+            if (marks) {
+                marks->mark(s.stream, "attempt");
+                ensure_m32(st);
+                marks->mark(s.stream, "stage_m32");
+            }
+            eval_on_state(st, terms, ep, nullptr, nullptr, marks);
         } else {
             KList kl;
             for (int j = 0; j < stg; ++j) {
@@ -305,12 +320,14 @@ double rk_attempt(maf_llg_s* l, maf_state_s* st, const Scheme& sch, double dt, i
             }
             rk_combine(s.m64.as<double>(), kl, l->mstage64.as<double>(), f32 ? l->mstage32.as<float>() : nullptr, n3,
                        s.stream);
+            if (marks) marks->mark(s.stream, kCombineNames[kl.n]);
             ep.llg.m64 = l->mstage64.as<double>();
             if (f32)
-                eval_terms<float>(terms, s.md, l->mstage32.as<float>(), s.msinfo(), ep, s.stream, st->scratch, nullptr);
+                eval_terms<float>(terms, s.md, l->mstage32.as<float>(), s.msinfo(), ep, s.stream, st->scratch, nullptr,
+                                  marks);
             else
                 eval_terms<double>(terms, s.md, l->mstage64.as<double>(), s.msinfo(), ep, s.stream, st->scratch,
-                                   nullptr);
+                                   nullptr, marks);
         }
     }
     KList kb, ke;
@@ -328,6 +345,13 @@ double rk_attempt(maf_llg_s* l, maf_state_s* st, const Scheme& sch, double dt, i
     }
     rk_finalize(s.m64.as<double>(), kb, ke, sch.form, l->ctrl.atol, l->ctrl.rtol, l->mcand.as<double>(), norm_mode, N,
                 l->partials.as<double>(), l->errbuf.as<double>(), s.stream);
+    if (marks) {
+        std::vector<const double*> uniq;
+        for (int j = 0; j < kb.n; ++j) uniq.push_back(kb.k[j]);
+        for (int j = 0; j < ke.n; ++j)
+            if (std::find(uniq.begin(), uniq.end(), ke.k[j]) == uniq.end()) uniq.push_back(ke.k[j]);
+        marks->mark(s.stream, kFinalizeNames[std::min<size_t>(uniq.size(), 8)]);
+    }
     double err = 0;
     MAF_CUDA(cudaMemcpyAsync(&err, l->errbuf.p, sizeof(double), cudaMemcpyDeviceToHost, s.stream));
     MAF_CUDA(cudaStreamSynchronize(s.stream));
@@ -357,10 +381,11 @@ void llg_step(maf_llg_s* l, maf_state_s* st) {
 
 void mean_m_host(maf_state_s* st, const double* m64, double out[3]) {
     StateD& s = st->s;
-    st->scratch.ensure(sizeof(double) * (4 * 148 * 2 + 8));
+    const int nres = 4 * mean_m_blocks();
+    st->scratch.ensure(sizeof(double) * (nres + 8));
     double* scr = st->scratch.as<double>();
-    mean_m(m64, s.md.N(), scr, scr + 4 * 148 * 2, s.stream);
-    MAF_CUDA(cudaMemcpyAsync(out, scr + 4 * 148 * 2, 3 * sizeof(double), cudaMemcpyDeviceToHost, s.stream));
+    mean_m(m64, s.md.N(), scr, scr + nres, s.stream);
+    MAF_CUDA(cudaMemcpyAsync(out, scr + nres, 3 * sizeof(double), cudaMemcpyDeviceToHost, s.stream));
     MAF_CUDA(cudaStreamSynchronize(s.stream));
 }
 
@@ -487,7 +512,7 @@ void stoch_step(maf_stoch_s* h, maf_state_s* st, unsigned long long* q_dev = nul
     h->mstage64.ensure(sizeof(double) * n3);
     if (f32) h->mstage32.ensure(sizeof(float) * n3);
     h->mcand.ensure(sizeof(double) * n3);
-    h->partials.ensure(sizeof(double) * 148 * 8 + 64);
+    h->partials.ensure(sizeof(double) * sm_count() * 8 + 64);
     h->errbuf.ensure(sizeof(double) * 4);
     std::vector<Term*> terms;
     for (auto& t : h->terms) terms.push_back(t.get());
@@ -766,7 +791,7 @@ double lbfgs_minimize(maf_lbfgs_s* h, maf_state_s* st) {
         h->sV[i].ensure(sizeof(double) * n3);
         h->yV[i].ensure(sizeof(double) * n3);
     }
-    h->red.ensure(sizeof(double) * (2 * 148 + 8));
+    h->red.ensure(sizeof(double) * (red_blocks() + 8));
     LbfgsCtx c{h, st, n3, S.md.N(), S.stream};
     const double eps = 2.22e-16, eps2 = std::sqrt(eps), epsr = std::pow(eps, 0.9);
     const double tolf2 = std::sqrt(h->tolerance), tolf3 = std::pow(h->tolerance, 0.3333333333333333333333333);
@@ -878,6 +903,7 @@ int maf_state_create(maf_state* out, int nx, int ny, int nz, double dx, double d
         check(nx > 0 && ny > 0 && nz > 0, "maf_state_create: mesh sizes must be positive");
         check(precision == MAF_FP64 || precision == MAF_FP32_FIELD, "maf_state_create: bad precision");
         require_device();
+        noalloc_prepare_current_device();
         auto h = std::make_unique<maf_state_s>();
         StateD& s = h->s;
         s.md = MeshDims{nx, ny, nz, dx, dy, dz};
@@ -1622,6 +1648,39 @@ int maf_term_demag_set_tune(maf_term t, const int choices[3]) {
     });
 }
 
+// One Runge-Kutta attempt of the integrator's scheme with step dt on the state's
+// m (the state is not changed), with CUDA events between its kernels: the
+// conversion of m to FP32 (FP32-field form), each stage's combine and field
+// passes, and the finalize (sumbk, error norm, candidate).
+int maf_llg_attempt_profile(maf_llg l, maf_state s, double dt, double* ms_out, int max_entries, int* n_entries) {
+    return guarded([&] {
+        check_llg_state(l, s);
+        check(ms_out && n_entries && max_entries > 0 && dt > 0, "maf_llg_attempt_profile: bad argument");
+        const int norm_mode = s->s.has_Ms_field ? 2 : 1;
+        s->m32_valid = false;  // a step starts from a new m: time its FP32 copy too
+        PassMarks marks;
+        rk_attempt(l, s, l->scheme, dt, norm_mode, &marks);
+        MAF_CUDA(cudaStreamSynchronize(s->s.stream));
+        l->prof_names.clear();
+        int n = 0;
+        for (size_t i = 1; i < marks.ev.size() && n < max_entries; ++i, ++n) {
+            float ms = 0;
+            MAF_CUDA(cudaEventElapsedTime(&ms, marks.ev[i - 1], marks.ev[i]));
+            ms_out[n] = ms;
+            l->prof_names.emplace_back(marks.names[i]);
+        }
+        *n_entries = n;
+    });
+}
+
+int maf_llg_profile_name(maf_llg l, int index, char* buf, int buflen) {
+    return guarded([&] {
+        check(l && buf && buflen > 0, "NULL argument");
+        check(index >= 0 && index < (int)l->prof_names.size(), "profile index out of range");
+        std::snprintf(buf, (size_t)buflen, "%s", l->prof_names[(size_t)index].c_str());
+    });
+}
+
 int maf_llg_pass_name(maf_llg l, maf_state s, int index, char* buf, int buflen) {
     return guarded([&] {
         check_llg_state(l, s);
@@ -1968,7 +2027,7 @@ std::unique_ptr<maf_state_s> make_image(const maf_state_s& tmpl, cudaStream_t st
 
 // FrobeniusNorm(a - b) = sqrt(mean((a - b)^2)) over all 3N values (util.cpp:53-55)
 double frob_diff(maf_string_s* h, const double* a, const double* b, int64_t n3) {
-    h->scratch.ensure(sizeof(double) * (2 * 148 + 2));
+    h->scratch.ensure(sizeof(double) * (red_blocks() + 2));
     return std::sqrt(sqdiff_host(a, b, n3, h->scratch.as<double>(), h->stream) / (double)n3);
 }
 

@@ -63,4 +63,20 @@ template <int DIR, typename C> __host__ __device__ __forceinline__ C cmul_i(C a)
 
 __host__ __device__ __forceinline__ int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
 
+// Streaming multiprocessors of the current device, queried once per device
+// ordinal (grid sizes of the grid-stride kernels and the reduction partial
+// buffers sized from them).
+inline int sm_count() {
+    constexpr int kMaxOrdinals = 64;
+    static int cache[kMaxOrdinals] = {};
+    int dev = 0;
+    MAF_CUDA(cudaGetDevice(&dev));
+    int v = (dev >= 0 && dev < kMaxOrdinals) ? __atomic_load_n(&cache[dev], __ATOMIC_RELAXED) : 0;
+    if (v <= 0) {
+        MAF_CUDA(cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev));
+        if (dev >= 0 && dev < kMaxOrdinals) __atomic_store_n(&cache[dev], v, __ATOMIC_RELAXED);
+    }
+    return v;
+}
+
 }  // namespace mafb

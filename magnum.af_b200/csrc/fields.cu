@@ -411,13 +411,13 @@ __global__ void k_widen(const float* __restrict__ a, double* __restrict__ b, int
 }
 
 void widen_m(const float* m32, double* m64, int64_t n, cudaStream_t st) {
-    const int64_t blocks = std::min<int64_t>(ceil_div(n, 256), 148LL * 16);
+    const int64_t blocks = std::min<int64_t>(ceil_div(n, 256), (int64_t)sm_count() * 16);
     k_widen<<<(unsigned)blocks, 256, 0, st>>>(m32, m64, n);
     MAF_LAUNCH_CHECK();
 }
 
 void stage_m32(const double* m64, float* m32, int64_t n, cudaStream_t st) {
-    const int64_t blocks = std::min<int64_t>(ceil_div(n, 256), 148LL * 16);
+    const int64_t blocks = std::min<int64_t>(ceil_div(n, 256), (int64_t)sm_count() * 16);
     k_stage32<<<(unsigned)blocks, 256, 0, st>>>(m64, m32, n);
     MAF_LAUNCH_CHECK();
 }
@@ -567,7 +567,7 @@ void Demag::build_tensor(cudaStream_t st) {
                                     (int64_t)Py_ * pitch_, (int64_t)Py_ * pitch_, pitch_, pitch_, Py_, tw_, tune,
                                     st);
         const int64_t total = cstride;
-        const int64_t blocks = std::min<int64_t>(ceil_div(total, 256), 148LL * 16);
+        const int64_t blocks = std::min<int64_t>(ceil_div(total, 256), (int64_t)sm_count() * 16);
         k_reduce_tensor<<<(unsigned)blocks, 256, 0, st>>>(spec.as<double2>(), Nred64_.as<double>() + ci * cstride,
                                                            nxh(), pitch_, Py_, Kz, Ky);
         MAF_LAUNCH_CHECK();
@@ -595,7 +595,7 @@ template <> const float* Demag::tensor<float>() {
     if (!Nred32_.p) {
         const int64_t n = (int64_t)tensor_elems();
         Nred32_.alloc(sizeof(float) * n);
-        k_d2f<<<(unsigned)std::min<int64_t>(ceil_div(n, 256), 148LL * 16), 256>>>(Nred64_.as<double>(),
+        k_d2f<<<(unsigned)std::min<int64_t>(ceil_div(n, 256), (int64_t)sm_count() * 16), 256>>>(Nred64_.as<double>(),
                                                                                    Nred32_.as<float>(), n);
         MAF_LAUNCH_CHECK();
         MAF_CUDA(cudaDeviceSynchronize());
@@ -804,7 +804,7 @@ void eval_terms(const std::vector<Term*>& terms, const MeshDims& md, const R* m,
     int nblocks = 0;
     if (ep.kind == EPI_EDENS || ep.kind == EPI_EGRAD) {
         // upper bound of CTAs for the partial sums
-        const int64_t maxb = std::max<int64_t>(md.N(), 148 * 8) + 1;
+        const int64_t maxb = std::max<int64_t>(md.N(), (int64_t)sm_count() * 8) + 1;
         scratch.ensure(sizeof(double) * (maxb + 1));
         ep.partials = scratch.as<double>();
     }
@@ -814,7 +814,7 @@ void eval_terms(const std::vector<Term*>& terms, const MeshDims& md, const R* m,
         demag->inverse_x_epilogue<R>(m, ms, tl, ep, st, &nblocks, marks);
     } else {
         const int threads = 256;
-        const int64_t blocks = std::min<int64_t>(ceil_div(md.N(), threads), 148LL * 8);
+        const int64_t blocks = std::min<int64_t>(ceil_div(md.N(), threads), (int64_t)sm_count() * 8);
         nblocks = (int)blocks;
         const Geom g = md.geom();
         if (marks) marks->mark(st, "start");

@@ -855,19 +855,42 @@ bool ct_xinv(const cplx_t<R>* S1, int pitch, int Px, Twiddles& tw, const Geom& g
 #undef X
 }
 
-#define MAF_INST(R)                                                                                                   \
+// The instantiations are split over several compilations of this file
+// (MAF_CT_PART = 1: x forward and convolutions, 2: y passes, 3: x inverse;
+// MAF_CT_REAL = 4 or 8 selects FP32 or FP64), so that the build compiles them
+// in parallel; without the macros every instantiation is made here.
+#if !defined(MAF_CT_PART) || MAF_CT_PART == 1
+#define MAF_INST1(R)                                                                                                  \
     template bool ct_xfwd<R>(const R*, int, int64_t, int64_t, const R*, R, cplx_t<R>*, int, int, Twiddles&,          \
                              cudaStream_t);                                                                          \
+    template bool ct_convz<R>(cplx_t<R>*, const R*, int, int, int, int, Twiddles&, const TuneChoice&,                \
+                              cudaStream_t);                                                                         \
+    template bool ct_convy<R>(cplx_t<R>*, const R*, int, int, int, Twiddles&, cudaStream_t);
+#else
+#define MAF_INST1(R)
+#endif
+#if !defined(MAF_CT_PART) || MAF_CT_PART == 2
+#define MAF_INST2(R)                                                                                                  \
     template bool ct_cols<R, -1>(const cplx_t<R>*, cplx_t<R>*, int, int, int, int, int64_t, int64_t, int64_t,        \
                                  int64_t, int, Twiddles&, const TuneChoice&, cudaStream_t);                          \
     template bool ct_cols<R, 1>(const cplx_t<R>*, cplx_t<R>*, int, int, int, int, int64_t, int64_t, int64_t, int64_t, \
-                                int, Twiddles&, const TuneChoice&, cudaStream_t);                                    \
-    template bool ct_convz<R>(cplx_t<R>*, const R*, int, int, int, int, Twiddles&, const TuneChoice&,                \
-                              cudaStream_t);                                                                         \
-    template bool ct_convy<R>(cplx_t<R>*, const R*, int, int, int, Twiddles&, cudaStream_t);                         \
+                                int, Twiddles&, const TuneChoice&, cudaStream_t);
+#else
+#define MAF_INST2(R)
+#endif
+#if !defined(MAF_CT_PART) || MAF_CT_PART == 3
+#define MAF_INST3(R)                                                                                                  \
     template bool ct_xinv<R>(const cplx_t<R>*, int, int, Twiddles&, const Geom&, R, const R*, const MsInfo&,          \
                              const TermList&, const EpilogueArgs&, const TuneChoice&, cudaStream_t, int*);
+#else
+#define MAF_INST3(R)
+#endif
+#define MAF_INST(R) MAF_INST1(R) MAF_INST2(R) MAF_INST3(R)
+#if !defined(MAF_CT_REAL) || MAF_CT_REAL == 4
 MAF_INST(float)
+#endif
+#if !defined(MAF_CT_REAL) || MAF_CT_REAL == 8
 MAF_INST(double)
+#endif
 
 }  // namespace mafb

@@ -23,8 +23,52 @@ __global__ void k_combine(const double* __restrict__ m, KList kl, double* __rest
     }
 }
 
+// The same combine with the number of k's a compile-time constant and two
+// values per thread through 16-byte loads: each thread issues its NK + 1
+// independent loads before the first use (the generic loop above issues them
+// one trip at a time).  Same arithmetic and summation order, so bit-identical.
+// Needs n even and 16-byte aligned buffers.
+template <int NK>
+__global__ void __launch_bounds__(256) k_combine_v(const double* __restrict__ m, KList kl, double* __restrict__ out64,
+                                                   float* __restrict__ out32, int64_t n2) {
+    const double2* m2 = reinterpret_cast<const double2*>(m);
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n2; i += (int64_t)gridDim.x * blockDim.x) {
+        double2 kv[NK];
+#pragma unroll
+        for (int j = 0; j < NK; ++j) kv[j] = reinterpret_cast<const double2*>(kl.k[j])[i];
+        double2 acc = m2[i];
+#pragma unroll
+        for (int j = 0; j < NK; ++j) {
+            acc.x = acc.x + kl.c[j] * kv[j].x;
+            acc.y = acc.y + kl.c[j] * kv[j].y;
+        }
+        reinterpret_cast<double2*>(out64)[i] = acc;
+        if (out32) reinterpret_cast<float2*>(out32)[i] = make_float2((float)acc.x, (float)acc.y);
+    }
+}
+
+static bool aligned16(const void* p) { return ((uintptr_t)p & 15) == 0; }
+
 void rk_combine(const double* m, const KList& kl, double* out64, float* out32, int64_t n, cudaStream_t st) {
-    const int64_t blocks = std::min<int64_t>(ceil_div(n, 256), 148LL * 16);
+    bool vec = n % 2 == 0 && kl.n >= 1 && kl.n <= 7 && aligned16(m) && aligned16(out64) &&
+               (!out32 || ((uintptr_t)out32 & 7) == 0);
+    for (int j = 0; j < kl.n; ++j) vec = vec && aligned16(kl.k[j]);
+    if (vec) {
+        const int64_t n2 = n / 2;
+        const unsigned blocks = (unsigned)std::min<int64_t>(ceil_div(n2, 256), (int64_t)sm_count() * 16);
+        switch (kl.n) {
+            case 1: k_combine_v<1><<<blocks, 256, 0, st>>>(m, kl, out64, out32, n2); break;
+            case 2: k_combine_v<2><<<blocks, 256, 0, st>>>(m, kl, out64, out32, n2); break;
+            case 3: k_combine_v<3><<<blocks, 256, 0, st>>>(m, kl, out64, out32, n2); break;
+            case 4: k_combine_v<4><<<blocks, 256, 0, st>>>(m, kl, out64, out32, n2); break;
+            case 5: k_combine_v<5><<<blocks, 256, 0, st>>>(m, kl, out64, out32, n2); break;
+            case 6: k_combine_v<6><<<blocks, 256, 0, st>>>(m, kl, out64, out32, n2); break;
+            default: k_combine_v<7><<<blocks, 256, 0, st>>>(m, kl, out64, out32, n2); break;
+        }
+        MAF_LAUNCH_CHECK();
+        return;
+    }
+    const int64_t blocks = std::min<int64_t>(ceil_div(n, 256), (int64_t)sm_count() * 16);
     k_combine<<<(unsigned)blocks, 256, 0, st>>>(m, kl, out64, out32, n);
     MAF_LAUNCH_CHECK();
 }
@@ -101,11 +145,127 @@ __global__ void k_max_partials(const double* __restrict__ p, int n, double* out)
     }
 }
 
+// The union of the b- and e-lists' k buffers, each loaded once: k[j] enters
+// sumbk with cb[j] and the error sum with ce[j] (a zero coefficient: not in
+// that list).  The lists' own orders are kept (checked by the caller), so the
+// sums are formed in the same order as in k_finalize.
+struct KUnion {
+    const double* k[8] = {};
+    double cb[8] = {};
+    double ce[8] = {};
+    int n = 0;
+};
+
+__device__ __forceinline__ double fin_one(double sumbk, double e, int form, double mi, double atol, double rtol,
+                                          double& vmax) {
+    const double err = form == 0 ? e : sumbk - e;
+    const double mn = mi + sumbk;
+    const double mx = mi > mn ? mi : mn;  // af::max(m, m + sumbk)
+    const double sc = atol + rtol * fabs(mx);
+    vmax = nanmax(vmax, fabs(err / sc));
+    return mn;
+}
+
+__device__ __forceinline__ void fin_norm(double* o, int norm_mode) {
+    if (norm_mode == 1) {
+        const double nrm = sqrt(o[0] * o[0] + o[1] * o[1] + o[2] * o[2]);
+        o[0] /= nrm; o[1] /= nrm; o[2] /= nrm;
+    } else if (norm_mode == 2) {
+        const double nrm = sqrt(o[0] * o[0] + o[1] * o[1] + o[2] * o[2]);
+        if (nrm != 0) { o[0] /= nrm; o[1] /= nrm; o[2] /= nrm; }
+        else { o[0] = 0; o[1] = 0; o[2] = 0; }
+    }
+}
+
+// k_finalize with NU union buffers known at compile time and two cells per
+// thread through 16-byte loads (N even, 16-byte aligned buffers); same
+// arithmetic as k_finalize, bit-identical results.
+template <int NU>
+__global__ void __launch_bounds__(256) k_finalize_v(const double* __restrict__ m, KUnion ku, int form, double atol,
+                                                    double rtol, double* __restrict__ mcand, int norm_mode, int64_t N,
+                                                    double* __restrict__ partials) {
+    const int64_t N2 = N / 2;
+    double vmax = 0.0;
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < N2; p += (int64_t)gridDim.x * blockDim.x) {
+        double o0[3], o1[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const int64_t i = c * N2 + p;
+            double2 kv[NU];
+#pragma unroll
+            for (int j = 0; j < NU; ++j) kv[j] = reinterpret_cast<const double2*>(ku.k[j])[i];
+            const double2 mi = reinterpret_cast<const double2*>(m)[i];
+            double b0 = 0.0, b1 = 0.0, e0 = 0.0, e1 = 0.0;
+#pragma unroll
+            for (int j = 0; j < NU; ++j) {
+                if (ku.cb[j] != 0.0) {
+                    b0 = b0 + ku.cb[j] * kv[j].x;
+                    b1 = b1 + ku.cb[j] * kv[j].y;
+                }
+                if (ku.ce[j] != 0.0) {
+                    e0 = e0 + ku.ce[j] * kv[j].x;
+                    e1 = e1 + ku.ce[j] * kv[j].y;
+                }
+            }
+            o0[c] = fin_one(b0, e0, form, mi.x, atol, rtol, vmax);
+            o1[c] = fin_one(b1, e1, form, mi.y, atol, rtol, vmax);
+        }
+        fin_norm(o0, norm_mode);
+        fin_norm(o1, norm_mode);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) reinterpret_cast<double2*>(mcand)[c * N2 + p] = make_double2(o0[c], o1[c]);
+    }
+    block_max_store(vmax, partials);
+}
+
+// Union of the two lists with each list's order preserved, or false.
+static bool make_union(const KList& kb, const KList& ke, KUnion& u) {
+    for (int j = 0; j < kb.n; ++j) {
+        if (kb.c[j] == 0.0) return false;
+        u.k[u.n] = kb.k[j];
+        u.cb[u.n] = kb.c[j];
+        ++u.n;
+    }
+    int last = -1;
+    for (int j = 0; j < ke.n; ++j) {
+        if (ke.c[j] == 0.0) continue;  // adds nothing to the error sum
+        int at = -1;
+        for (int q = 0; q < u.n; ++q)
+            if (u.k[q] == ke.k[j]) at = q;
+        if (at < 0) {
+            if (u.n == 8) return false;
+            at = u.n++;
+            u.k[at] = ke.k[j];
+        }
+        if (at <= last) return false;  // the e-list's order would change
+        u.ce[at] = ke.c[j];
+        last = at;
+    }
+    return u.n >= 1 && u.n <= 7;
+}
+
 int rk_finalize(const double* m, const KList& kb, const KList& ke, int form, double atol, double rtol, double* mcand,
                 int norm_mode, int64_t N, double* partials, double* err_dev, cudaStream_t st) {
     const int threads = 256;
-    const int blocks = (int)std::min<int64_t>(ceil_div(N, threads), 148LL * 8);
-    k_finalize<<<blocks, threads, 0, st>>>(m, kb, ke, form, atol, rtol, mcand, norm_mode, N, partials);
+    KUnion u;
+    bool vec = N % 2 == 0 && aligned16(m) && aligned16(mcand) && make_union(kb, ke, u);
+    for (int j = 0; vec && j < u.n; ++j) vec = aligned16(u.k[j]);
+    int blocks;
+    if (vec) {
+        blocks = (int)std::min<int64_t>(ceil_div(N / 2, threads), (int64_t)sm_count() * 8);
+        switch (u.n) {
+            case 1: k_finalize_v<1><<<blocks, threads, 0, st>>>(m, u, form, atol, rtol, mcand, norm_mode, N, partials); break;
+            case 2: k_finalize_v<2><<<blocks, threads, 0, st>>>(m, u, form, atol, rtol, mcand, norm_mode, N, partials); break;
+            case 3: k_finalize_v<3><<<blocks, threads, 0, st>>>(m, u, form, atol, rtol, mcand, norm_mode, N, partials); break;
+            case 4: k_finalize_v<4><<<blocks, threads, 0, st>>>(m, u, form, atol, rtol, mcand, norm_mode, N, partials); break;
+            case 5: k_finalize_v<5><<<blocks, threads, 0, st>>>(m, u, form, atol, rtol, mcand, norm_mode, N, partials); break;
+            case 6: k_finalize_v<6><<<blocks, threads, 0, st>>>(m, u, form, atol, rtol, mcand, norm_mode, N, partials); break;
+            default: k_finalize_v<7><<<blocks, threads, 0, st>>>(m, u, form, atol, rtol, mcand, norm_mode, N, partials); break;
+        }
+    } else {
+        blocks = (int)std::min<int64_t>(ceil_div(N, threads), (int64_t)sm_count() * 8);
+        k_finalize<<<blocks, threads, 0, st>>>(m, kb, ke, form, atol, rtol, mcand, norm_mode, N, partials);
+    }
     MAF_LAUNCH_CHECK();
     k_max_partials<<<1, 256, 0, st>>>(partials, blocks, err_dev);
     MAF_LAUNCH_CHECK();
@@ -135,7 +295,7 @@ __global__ void k_normalize(double* __restrict__ m, int64_t N, int mode, unsigne
 }
 
 void normalize_m(double* m, int64_t N, int mode, unsigned long long* zero_count_dev, cudaStream_t st) {
-    const int64_t blocks = std::min<int64_t>(ceil_div(N, 256), 148LL * 8);
+    const int64_t blocks = std::min<int64_t>(ceil_div(N, 256), (int64_t)sm_count() * 8);
     k_normalize<<<(unsigned)blocks, 256, 0, st>>>(m, N, mode, zero_count_dev);
     MAF_LAUNCH_CHECK();
 }
@@ -153,7 +313,7 @@ __global__ void k_ms_from_m(const double* __restrict__ m, double Ms, double* __r
 }
 
 void ms_field_from_m(const double* m, double Ms, double* msf, float* msf32, int64_t N, cudaStream_t st) {
-    const int64_t blocks = std::min<int64_t>(ceil_div(N, 256), 148LL * 8);
+    const int64_t blocks = std::min<int64_t>(ceil_div(N, 256), (int64_t)sm_count() * 8);
     k_ms_from_m<<<(unsigned)blocks, 256, 0, st>>>(m, Ms, msf, msf32, N);
     MAF_LAUNCH_CHECK();
 }
@@ -201,8 +361,10 @@ __global__ void k_mean_final(const double* __restrict__ part, int nb, double* __
     }
 }
 
+int mean_m_blocks() { return 2 * sm_count(); }
+
 void mean_m(const double* m, int64_t N, double* scratch, double* out_dev, cudaStream_t st) {
-    const int blocks = (int)std::min<int64_t>(ceil_div(N, 256), 148LL * 2);
+    const int blocks = (int)std::min<int64_t>(ceil_div(N, 256), mean_m_blocks());
     k_mean_partials<<<blocks, 256, 0, st>>>(m, N, scratch);
     MAF_LAUNCH_CHECK();
     k_mean_final<<<1, 32, 0, st>>>(scratch, blocks, out_dev);
@@ -216,7 +378,7 @@ __global__ void k_f2d(const float* __restrict__ a, double* __restrict__ b, int64
 }
 
 void f32_to_f64(const float* a, double* b, int64_t n, cudaStream_t st) {
-    const int64_t blocks = std::min<int64_t>(ceil_div(n, 256), 148LL * 16);
+    const int64_t blocks = std::min<int64_t>(ceil_div(n, 256), (int64_t)sm_count() * 16);
     k_f2d<<<(unsigned)blocks, 256, 0, st>>>(a, b, n);
     MAF_LAUNCH_CHECK();
 }
@@ -224,7 +386,9 @@ void f32_to_f64(const float* a, double* b, int64_t n, cudaStream_t st) {
 // ---------------------------------------------------------------------------
 // vector operations of the LBFGS minimiser (lbfgs_minimizer.cpp:44-46, 96-177)
 // ---------------------------------------------------------------------------
-constexpr int kRedBlocks = 148 * 2;
+// reduction blocks of the LBFGS vector operations (partials at scratch[0, n),
+// the result at scratch[n])
+int red_blocks() { return 2 * sm_count(); }
 
 // per-block partials: mode 0 sum a*b, mode 1 max |a| (NaN-propagating),
 // mode 2 sum (a-b)^2 (the string method's Frobenius norm of image differences)
@@ -269,13 +433,14 @@ __global__ void k_red_final(const double* __restrict__ part, int nb, int mode, d
 }
 
 double reduce_host(const double* a, const double* b, int64_t n, int mode, double* scratch, cudaStream_t st) {
-    const int blocks = (int)std::min<int64_t>(ceil_div(n, 256), kRedBlocks);
+    const int nred = red_blocks();
+    const int blocks = (int)std::min<int64_t>(ceil_div(n, 256), nred);
     k_red_partials<<<blocks, 256, 0, st>>>(a, b, n, mode, scratch);
     MAF_LAUNCH_CHECK();
-    k_red_final<<<1, 32, 0, st>>>(scratch, blocks, mode, scratch + kRedBlocks);
+    k_red_final<<<1, 32, 0, st>>>(scratch, blocks, mode, scratch + nred);
     MAF_LAUNCH_CHECK();
     double v = 0;
-    MAF_CUDA(cudaMemcpyAsync(&v, scratch + kRedBlocks, sizeof(double), cudaMemcpyDeviceToHost, st));
+    MAF_CUDA(cudaMemcpyAsync(&v, scratch + nred, sizeof(double), cudaMemcpyDeviceToHost, st));
     MAF_CUDA(cudaStreamSynchronize(st));
     return v;
 }
@@ -301,7 +466,7 @@ __global__ void k_lerp(double* __restrict__ out, const double* __restrict__ a, c
 }
 
 void lerp(double* out, const double* a, const double* b, double c1, double c2, int64_t n, cudaStream_t st) {
-    const int64_t blocks = std::min<int64_t>(ceil_div(n, 256), 148LL * 16);
+    const int64_t blocks = std::min<int64_t>(ceil_div(n, 256), (int64_t)sm_count() * 16);
     k_lerp<<<(unsigned)blocks, 256, 0, st>>>(out, a, b, c1, c2, n);
     MAF_LAUNCH_CHECK();
 }
@@ -323,7 +488,7 @@ __global__ void k_axpby(double* out, double a, const double* x, double b, const 
 }
 
 void axpby(double* out, double a, const double* x, double b, const double* y, int64_t n, cudaStream_t st) {
-    const int64_t blocks = std::min<int64_t>(ceil_div(n, 256), 148LL * 16);
+    const int64_t blocks = std::min<int64_t>(ceil_div(n, 256), (int64_t)sm_count() * 16);
     k_axpby<<<(unsigned)blocks, 256, 0, st>>>(out, a, x, b, y, n);
     MAF_LAUNCH_CHECK();
 }
@@ -343,7 +508,7 @@ __global__ void k_normalize_combine(double* __restrict__ m, const double* __rest
 }
 
 void normalize_combine(double* m, const double* wa, double stp, const double* s, int64_t N, cudaStream_t st) {
-    const int64_t blocks = std::min<int64_t>(ceil_div(N, 256), 148LL * 8);
+    const int64_t blocks = std::min<int64_t>(ceil_div(N, 256), (int64_t)sm_count() * 8);
     k_normalize_combine<<<(unsigned)blocks, 256, 0, st>>>(m, wa, stp, s, N);
     MAF_LAUNCH_CHECK();
 }
@@ -364,7 +529,7 @@ __global__ void k_noise(double* __restrict__ out, int64_t N, double sigma, unsig
 
 void thermal_field(double* out, int64_t N, double sigma, unsigned long long seed, unsigned member,
                    unsigned long long index, cudaStream_t st) {
-    const int64_t blocks = std::min<int64_t>(ceil_div(N, 256), 148LL * 8);
+    const int64_t blocks = std::min<int64_t>(ceil_div(N, 256), (int64_t)sm_count() * 8);
     k_noise<<<(unsigned)blocks, 256, 0, st>>>(out, N, sigma, seed, member, index);
     MAF_LAUNCH_CHECK();
 }

@@ -117,7 +117,7 @@ void newell_component(double* out, int comp, const MeshDims& md, int Px, int Py,
                       cudaStream_t st) {
     const int64_t total = (int64_t)Px * Py * Pz;
     const int threads = 128;
-    const int64_t blocks = std::min<int64_t>(ceil_div(total, threads), 148LL * 64);
+    const int64_t blocks = std::min<int64_t>(ceil_div(total, threads), (int64_t)sm_count() * 64);
     k_newell<<<(unsigned)blocks, threads, 0, st>>>(out, comp, Px, Py, Pz, md.dx, md.dy, md.dz, symmetric ? 1 : 0);
     MAF_LAUNCH_CHECK();
 }

@@ -22,7 +22,6 @@
 // threads on the same device, without ordering between them) share this one
 // scratch array and race: their partial sums overwrite each other and both
 // results are undefined.  Calls on the same stream are ordered and safe.
-#include <mutex>
 #include <string>
 
 #include "../../include/maf_b200.h"
@@ -39,7 +38,6 @@ constexpr long long kCellsPerBlock = (long long)kThreads * kCellsPerThread;  // 
 constexpr int kMaxBlocks = 4096;
 constexpr long long kMaxCells = kCellsPerBlock * kMaxBlocks;  // 33,554,432 cells
 constexpr int kResult = 4 * kMaxBlocks;
-constexpr int kMaxDevices = 64;
 
 __device__ __align__(256) double g_noalloc_scratch[4 * kMaxBlocks + 4];
 
@@ -106,27 +104,30 @@ __global__ void __launch_bounds__(1024) k_mean_combine(const double* __restrict_
     }
 }
 
-std::mutex g_mu;
-double* g_scratch_ptr[kMaxDevices] = {};
-
-// Address of this device's copy of g_noalloc_scratch, looked up once per device
-// with that device current (the first call on a device does the lookup).
-double* scratch_for_current_device() {
-    int dev = 0;
-    MAF_CUDA(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= kMaxDevices)
-        throw Error(MAF_ERR_UNSUPPORTED, "maf_mean_m_noalloc: device ordinal " + std::to_string(dev) +
-                                             " is beyond the " + std::to_string(kMaxDevices) + " supported");
-    std::lock_guard<std::mutex> lock(g_mu);
-    if (!g_scratch_ptr[dev]) {
-        void* p = nullptr;
-        MAF_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
-        g_scratch_ptr[dev] = static_cast<double*>(p);
-    }
-    return g_scratch_ptr[dev];
+// Address of the current device's copy of g_noalloc_scratch.  The lookup is
+// repeated on every call instead of being cached: a symbol address belongs to
+// the current CUDA context, and a cached one would dangle after
+// cudaDeviceReset or under another context.  Once this file's module is
+// loaded in the context the lookup allocates nothing.
+double* scratch_for_current_context() {
+    void* p = nullptr;
+    MAF_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+    return static_cast<double*>(p);
 }
 
 }  // namespace
+
+// CUDA loads the module of this file (its code and the static scratch array)
+// lazily, on the first use in a context, and that load allocates device memory
+// and may synchronise the device.  maf_state_create calls this, so the load
+// happens when the first state is created on a device -- a call that allocates
+// anyway -- and maf_mean_m_noalloc's own calls then allocate nothing.
+void mafb::noalloc_prepare_current_device() {
+    (void)scratch_for_current_context();
+    cudaFuncAttributes attr;
+    MAF_CUDA(cudaFuncGetAttributes(&attr, k_mean_chunks));
+    MAF_CUDA(cudaFuncGetAttributes(&attr, k_mean_combine));
+}
 
 extern "C" int maf_mean_m_noalloc(const double* m_dev, long long ncells, double out[3], void* cuda_stream) {
     return capi_run([&] {
@@ -136,7 +137,7 @@ extern "C" int maf_mean_m_noalloc(const double* m_dev, long long ncells, double 
             throw Error(MAF_ERR_BADARG, "maf_mean_m_noalloc: ncells = " + std::to_string(ncells) +
                                             " exceeds the fixed scratch limit of " + std::to_string(kMaxCells) +
                                             " cells; use maf_state_mean_m for larger meshes");
-        double* scr = scratch_for_current_device();
+        double* scr = scratch_for_current_context();
         cudaStream_t st = static_cast<cudaStream_t>(cuda_stream);
         const int nb = (int)((ncells + kCellsPerBlock - 1) / kCellsPerBlock);
         k_mean_chunks<<<nb, kThreads, 0, st>>>(m_dev, ncells, scr);

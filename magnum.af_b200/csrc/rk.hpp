@@ -16,11 +16,14 @@ int rk_finalize(const double* m, const KList& kb, const KList& ke, int form, dou
                 int norm_mode, int64_t N, double* partials, double* err_dev, cudaStream_t st);
 void normalize_m(double* m, int64_t N, int mode, unsigned long long* zero_count_dev, cudaStream_t st);
 void ms_field_from_m(const double* m, double Ms, double* msf, float* msf32, int64_t N, cudaStream_t st);
+// partial-sum blocks of mean_m (its scratch needs 4 per block; out_dev may sit behind them)
+int mean_m_blocks();
 void mean_m(const double* m, int64_t N, double* scratch, double* out_dev, cudaStream_t st);
 void f32_to_f64(const float* a, double* b, int64_t n, cudaStream_t st);
 void thermal_field(double* out, int64_t N, double sigma, unsigned long long seed, unsigned member,
                    unsigned long long index, cudaStream_t st);
-// LBFGS vector operations; scratch needs 2*148+1 doubles; the reductions synchronise
+// LBFGS vector operations; scratch needs red_blocks() + 1 doubles; the reductions synchronise
+int red_blocks();
 double dot_host(const double* a, const double* b, int64_t n, double* scratch, cudaStream_t st);
 double maxabs_host(const double* a, int64_t n, double* scratch, cudaStream_t st);
 void axpby(double* out, double a, const double* x, double b, const double* y, int64_t n, cudaStream_t st);

@@ -96,6 +96,8 @@ _SIGS = {
     "maf_term_demag_set_tune": (_I, [_P, C.POINTER(_I)]),
     "maf_llg_heff_device_profile": (_I, [_P, _P, _P, _P, _DP, _I, C.POINTER(_I)]),
     "maf_llg_pass_name": (_I, [_P, _P, _I, C.c_char_p, _I]),
+    "maf_llg_attempt_profile": (_I, [_P, _P, C.c_double, _DP, _I, C.POINTER(_I)]),
+    "maf_llg_profile_name": (_I, [_P, _I, C.c_char_p, _I]),
     "maf_llg_dmdt": (_I, [_P, _P, _DP]),
     "maf_llg_integrate_dense": (_I, [_P, _P, _D, _D, _DP, _I, C.POINTER(_I)]),
     "maf_llg_rk_attempt": (_I, [_P, _P, C.c_char_p, _D, _DP, _DP]),
@@ -784,6 +786,21 @@ class LLGIntegrator:
         buf = C.create_string_buffer(64)
         for i in range(n.value):
             _ck(lib.maf_llg_pass_name(self._h, state._h, i, buf, 64))
+            out.append((buf.value.decode(), float(ms[i])))
+        return out
+
+
+    def attempt_profile(self, state: State, dt: float):
+        """One Runge-Kutta attempt of this integrator's scheme with step dt (the state
+        is not changed), with CUDA events between its kernels: [(name, ms), ...]."""
+        cap = 256
+        ms = np.zeros(cap)
+        n = C.c_int()
+        _ck(lib.maf_llg_attempt_profile(self._h, state._h, float(dt), _dptr(ms), cap, C.byref(n)))
+        out = []
+        buf = C.create_string_buffer(64)
+        for i in range(n.value):
+            _ck(lib.maf_llg_profile_name(self._h, i, buf, 64))
             out.append((buf.value.decode(), float(ms[i])))
         return out
 
