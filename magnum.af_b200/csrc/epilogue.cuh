@@ -355,6 +355,61 @@ __device__ __forceinline__ void runN_epilogue(const TermList& tl, const Geom& g,
     }
 }
 
+// ---------------------------------------------------------------------------
+// Host side of the run epilogue: eligibility and per-launch term constants.
+// ---------------------------------------------------------------------------
+// The 4-cell epilogue (epilogue.cuh) needs nx % 4 == 0, 16-byte aligned m and
+// output, a scalar Ms and only terms with scalar parameters.
+template <typename R>
+inline bool run4_eligible(const Geom& g, const R* m, const MsInfo& ms, const TermList& tl, const EpilogueArgs& ep) {
+    if (g.nx % 4 != 0 || ms.field64) return false;
+    if (ep.kind != EPI_H && ep.kind != EPI_LLG) return false;
+    if (((uintptr_t)m | (uintptr_t)ep.out) % 16 != 0) return false;
+    if (ep.kind == EPI_LLG && ((uintptr_t)ep.llg.m64 % 16 != 0)) return false;
+    for (int i = 0; i < tl.n; ++i) {
+        const TermDesc& t = tl.t[i];
+        switch (t.kind) {
+            case TK_DEMAG: case TK_EXCHANGE: case TK_CUBIC: break;
+            case TK_DMI: case TK_UNIAXIAL: case TK_ZEEMAN:
+                if (t.f0 || t.f1) return false;
+                break;
+            default: return false;
+        }
+    }
+    return true;
+}
+
+// Per-launch constants of the 4-cell epilogue (TermDesc::q); the scalar Ms is
+// known because run4 excludes an Ms_field.
+inline void prepare_run4(TermList& tl, const Geom& g, double Ms) {
+    const double mu0Ms = kMu0 * Ms;
+    for (int i = 0; i < tl.n; ++i) {
+        TermDesc& t = tl.t[i];
+        switch (t.kind) {
+            case TK_EXCHANGE: {
+                const double c = 2.0 * t.p[0] / mu0Ms;
+                t.q[0] = c / (g.dx * g.dx);
+                t.q[1] = c / (g.dy * g.dy);
+                t.q[2] = c / (g.dz * g.dz);
+                break;
+            }
+            case TK_DMI:
+                t.q[0] = 2.0 * t.p[0] / mu0Ms;
+                t.q[1] = 0.5 / g.dx;
+                t.q[2] = 0.5 / g.dy;
+                t.q[3] = 0.5 / g.dz;
+                break;
+            case TK_UNIAXIAL: t.q[0] = 2.0 * t.p[0] / mu0Ms; break;
+            case TK_CUBIC:
+                t.q[0] = -2.0 * t.p[0] / mu0Ms;
+                t.q[1] = -2.0 * t.p[1] / mu0Ms;
+                t.q[2] = -4.0 * t.p[2] / mu0Ms;
+                break;
+            default: break;
+        }
+    }
+}
+
 __device__ __forceinline__ void block_sum_store(double v, double* partials) {
     __shared__ double red[32];
     for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);

@@ -449,15 +449,22 @@ __global__ void __launch_bounds__(NT, (kMinBlocks<R, NT, (RN == 2 ? MAF_XINV_THR
         ct_fft_in<R, 1, false, LC, NC, NT>(s, SB, tw, ld, typename CtPlan<LC>::T());
     if constexpr (EPI == EPI_H || EPI == EPI_LLG) {
         if (run4) {
-            const int runs = g.nx / RN;
+            // the rows are nx = LC cells long (the x padding doubles nx), so the run
+            // index arithmetic is compile-time; (y, z) of the CTA's first row once
+            constexpr int runs = LC / RN;
+            const int z0 = ry0 / g.ny;
+            const int y0 = ry0 - z0 * g.ny;
             for (int idx = threadIdx.x; idx < NBR * runs; idx += NT) {
                 const int b = idx / runs;
                 const int x0 = (idx - b * runs) * RN;
                 const int ry = ry0 + b;
                 if (ry >= rows_pc) continue;
-                const int z = ry / g.ny;
-                const int y = ry - z * g.ny;
-                const int64_t cell0 = (int64_t)ry * g.nx + x0;
+                int y = y0 + b, z = z0;
+                while (y >= g.ny) {
+                    y -= g.ny;
+                    ++z;
+                }
+                const int64_t cell0 = (int64_t)ry * LC + x0;
                 RunN<R, RN> r;
                 runN_load<R, RN>(m, g, x0, y, z, cell0, r);
                 R hd[RN][3];
@@ -494,59 +501,6 @@ __global__ void __launch_bounds__(NT, (kMinBlocks<R, NT, (RN == 2 ? MAF_XINV_THR
         epilogue_cell<R, EPI>(g, x, y, z, cell, m, ms, tl, ep, hd, eacc);
     }
     if constexpr (EPI == EPI_EDENS || EPI == EPI_EGRAD) block_sum_store(eacc, ep.partials);
-}
-
-// ------------------------------------------------------------------ dispatch
-// The 4-cell epilogue (epilogue.cuh) needs nx % 4 == 0, 16-byte aligned m and
-// output, a scalar Ms and only terms with scalar parameters.
-template <typename R>
-static bool run4_eligible(const Geom& g, const R* m, const MsInfo& ms, const TermList& tl, const EpilogueArgs& ep) {
-    if (g.nx % 4 != 0 || ms.field64) return false;
-    if (ep.kind != EPI_H && ep.kind != EPI_LLG) return false;
-    if (((uintptr_t)m | (uintptr_t)ep.out) % 16 != 0) return false;
-    if (ep.kind == EPI_LLG && ((uintptr_t)ep.llg.m64 % 16 != 0)) return false;
-    for (int i = 0; i < tl.n; ++i) {
-        const TermDesc& t = tl.t[i];
-        switch (t.kind) {
-            case TK_DEMAG: case TK_EXCHANGE: case TK_CUBIC: break;
-            case TK_DMI: case TK_UNIAXIAL: case TK_ZEEMAN:
-                if (t.f0 || t.f1) return false;
-                break;
-            default: return false;
-        }
-    }
-    return true;
-}
-
-// Per-launch constants of the 4-cell epilogue (TermDesc::q); the scalar Ms is
-// known because run4 excludes an Ms_field.
-static void prepare_run4(TermList& tl, const Geom& g, double Ms) {
-    const double mu0Ms = kMu0 * Ms;
-    for (int i = 0; i < tl.n; ++i) {
-        TermDesc& t = tl.t[i];
-        switch (t.kind) {
-            case TK_EXCHANGE: {
-                const double c = 2.0 * t.p[0] / mu0Ms;
-                t.q[0] = c / (g.dx * g.dx);
-                t.q[1] = c / (g.dy * g.dy);
-                t.q[2] = c / (g.dz * g.dz);
-                break;
-            }
-            case TK_DMI:
-                t.q[0] = 2.0 * t.p[0] / mu0Ms;
-                t.q[1] = 0.5 / g.dx;
-                t.q[2] = 0.5 / g.dy;
-                t.q[3] = 0.5 / g.dz;
-                break;
-            case TK_UNIAXIAL: t.q[0] = 2.0 * t.p[0] / mu0Ms; break;
-            case TK_CUBIC:
-                t.q[0] = -2.0 * t.p[0] / mu0Ms;
-                t.q[1] = -2.0 * t.p[1] / mu0Ms;
-                t.q[2] = -4.0 * t.p[2] / mu0Ms;
-                break;
-            default: break;
-        }
-    }
 }
 
 // ------------------------------------------------------------------ launches
@@ -832,6 +786,7 @@ bool ct_xinv(const cplx_t<R>* S1, int pitch, int Px, Twiddles& tw, const Geom& g
              const MsInfo& ms, const TermList& tl, const EpilogueArgs& ep, const TuneChoice& tc, cudaStream_t st,
              int* nblocks) {
     const int LC = Px / 2;
+    if (g.nx != LC) return false;  // the kernels take the row length from LC
     const bool f64 = sizeof(R) == 8;
     const int run = tc.xinv_run ? tc.xinv_run : kRunCells;
 #define X(N)                                                                                                    \
