@@ -336,6 +336,75 @@ def rk_step_figures(M, mesh, m, terms, stream, steps, peak):
     return out
 
 
+def heun_ensemble(M, steps, fused_only=False, shapes=None):
+    """The batched Langevin ensemble: 64 stochastic-Heun members at T = 300 K on
+    2-D meshes whose two sides are drawn (seeded) from {64, 96, 128, 192, 256, 384,
+    512} cells of 2 x 2 x 1 nm; demag + exchange (1.6e-11 J/m) + interface DMI
+    (3e-3 J/m^2) + uniaxial Ku 1e6 J/m^3 along z, Ms 1.1e6 A/m, alpha 0.1, dt 5 fs,
+    FP32 field / FP64 state, each member with its own noise stream.  Timed on the
+    host around StochasticBatch.steps (each call synchronises): the batched passes
+    (one launch per pass for all members, one CUDA graph per two steps), the
+    per-member graph on forked streams, and (a few steps) the members stepped one
+    after another."""
+    import torch
+
+    rng = np.random.default_rng(SEED + 7)
+    sides = [64, 96, 128, 192, 256, 384, 512]
+    if shapes is None:
+        shapes = [(int(rng.choice(sides)), int(rng.choice(sides))) for _ in range(64)]
+
+    def build():
+        out = []
+        for i, (nx, ny) in enumerate(shapes):
+            mesh = M.Mesh(nx, ny, 1, 2e-9, 2e-9, 1e-9)
+            terms = [M.DemagField(mesh), M.ExchangeField(1.6e-11), M.DmiField(3e-3), M.UniaxialAnisotropyField(1e6)]
+            m = np.zeros((nx, ny, 1, 3))
+            m[..., 2] = 1.0
+            st = M.State(mesh, 1.1e6, m, precision="fp32_field")
+            it = M.Stochastic_LLG(0.1, 300.0, 5e-15, st, terms, "Heun", seed=SEED, member=i)
+            out.append((it, st, terms))
+        return out
+
+    def run(batch, n):
+        batch.steps(3)  # the eager step, then a capture
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        batch.steps(n)
+        torch.cuda.synchronize()
+        return time.perf_counter() - t0
+
+    cells = sum(nx * ny for nx, ny in shapes)
+    res = {"members": len(shapes), "cells": cells, "steps": steps,
+           "config": "%d stochastic-Heun members, sides %s (2-D), T 300 K, FP32 field / FP64 state" % (
+               len(shapes), "from {64..512}" if len(set(shapes)) > 1 else "%dx%d" % shapes[0])}
+    mem = build()
+    fb = M.StochasticBatch([(it, st) for it, st, _ in mem], fused=True)
+    t = run(fb, steps)
+    res["fused"] = {"active": fb.fused_active, "s": t, "ensemble_steps_per_s": steps / t,
+                    "member_steps_per_s": len(shapes) * steps / t, "cell_steps_per_s": cells * steps / t}
+    del fb, mem
+    if not fused_only:
+        mem = build()
+        gb = M.StochasticBatch([(it, st) for it, st, _ in mem], fused=False)
+        t = run(gb, steps)
+        res["graph_of_streams"] = {"s": t, "ensemble_steps_per_s": steps / t}
+        del gb
+        nser = max(2, min(steps, 20))
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for it, st, _ in mem:
+            it.steps(st, nser)
+        torch.cuda.synchronize()
+        t = time.perf_counter() - t0
+        res["one_after_another"] = {"s": t, "steps": nser, "ensemble_steps_per_s": nser / t}
+        res["fused_speedup_vs_serial"] = res["fused"]["ensemble_steps_per_s"] / res["one_after_another"][
+            "ensemble_steps_per_s"]
+        res["fused_speedup_vs_streams"] = res["fused"]["ensemble_steps_per_s"] / res["graph_of_streams"][
+            "ensemble_steps_per_s"]
+        del mem
+    return res
+
+
 def other_configs(M, stream):
     """Simulated ns per hour of wall time on the two other single-mesh
     configurations (short runs, seeded inputs):
@@ -519,6 +588,10 @@ def run_ours(args):
 
     # the other single-mesh configurations, short runs: simulated ns per hour
     cfgs = {} if args.no_trajectory else other_configs(M, stream)
+    if not args.no_trajectory and args.heun_steps > 0:
+        cfgs["heun_ensemble_64"] = heun_ensemble(M, args.heun_steps)
+        # the same with 64 small members (64 x 64): launch-bound, where one launch per pass pays
+        cfgs["heun_ensemble_64_small"] = heun_ensemble(M, args.heun_steps, shapes=[(64, 64)] * 64)
 
     # per-pass timing (CUDA events between the pass kernels on the launching stream)
     passes = {}
@@ -701,6 +774,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default kernel variants")
     ap.add_argument("--rk-steps", type=int, default=300, help="DP45 steps of the plain step loop per form")
+    ap.add_argument("--heun-steps", type=int, default=1000, help="steps of the 64-member Heun ensemble")
     ap.add_argument("--mesh", type=int, nargs=3, default=None, metavar=("NX", "NY", "NZ"),
                     help="smaller mesh for profiling captures (the reported metric is defined at 1024 1024 16)")
     args = ap.parse_args()

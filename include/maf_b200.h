@@ -203,6 +203,10 @@ int maf_llg_heff_pipeline_m32(maf_llg l, maf_state s, const float* const* m_host
 int maf_llg_autotune(maf_llg l, maf_state s, int reps, int choices[3], double* pass_ms);
 int maf_term_demag_get_tune(maf_term t, int choices[3]);
 int maf_term_demag_set_tune(maf_term t, const int choices[3]);
+/* Runs every pass of this DemagField with the run-time-plan kernels (the ones the batched passes of
+ * maf_stoch_batch_set_fused use) instead of the compile-time ones; on = 0 restores the default.  Both
+ * compute the same field up to rounding (no counterpart in the reference). */
+int maf_term_demag_set_generic(maf_term t, int on);
 /* maf_llg_heff_device with a CUDA event after every pass kernel: synchronises and
  * returns each pass's duration in ms (the instrumentation LLGIntegrator::time_heff,
  * llg_integrator.cpp:11-16, and the per-term timers of field_term.hpp:49-86 provide,
@@ -266,6 +270,15 @@ typedef struct maf_stoch_batch_s* maf_stoch_batch;
 int maf_stoch_batch_create(maf_stoch_batch* out, const maf_stoch* integrators, const maf_state* states, int n);
 int maf_stoch_batch_destroy(maf_stoch_batch b);
 int maf_stoch_batch_steps(maf_stoch_batch b, int nsteps);
+/* Batched passes (no counterpart in the reference): with on = 1 the next capture records every pass of
+ * a step as ONE launch for all members -- each CTA takes a (member, tile) pair from a device work table
+ * and runs that tile of the member's run-time-plan kernel -- instead of one launch per member and pass.
+ * Members must be 2-D meshes with one non-periodic DemagField, scalar parameters, one scheme, dt and
+ * precision; a batch that does not qualify keeps the per-member graph.  A member's trajectory equals
+ * the one its own integrator computes with maf_term_demag_set_generic(demag, 1), bit for bit.
+ * maf_stoch_batch_is_fused reports whether the current graph runs the batched passes. */
+int maf_stoch_batch_set_fused(maf_stoch_batch b, int on);
+int maf_stoch_batch_is_fused(maf_stoch_batch b, int* active);
 
 /* ------------------------------------------------------------- LBFGS ---
  * LBFGS_Minimizer(terms, tolerance = 1e-6, maxIter = 230)

@@ -35,6 +35,7 @@ SOURCES = {
     "capi.o": ("capi.cu", []),
     "noalloc.o": ("noalloc.cu", []),
     "cnn.o": ("cnn.cu", []),
+    "batch.o": ("batch.cu", []),
 }
 for _part in (1, 2, 3):
     for _real in (4, 8):

@@ -12,6 +12,7 @@
 
 #include "../../include/maf_b200.h"
 #include "capi_internal.hpp"
+#include "batch.hpp"
 #include "engine.hpp"
 #include "rk.hpp"
 
@@ -1644,7 +1645,18 @@ int maf_term_demag_set_tune(maf_term t, const int choices[3]) {
         check((choices[0] == 0 || choices[0] == 1) && (choices[1] == 0 || choices[1] == 1) &&
                   (choices[2] == 0 || choices[2] == 2 || choices[2] == 4),
               "maf_term_demag_set_tune: choices are {0|1, 0|1, 0|2|4}");
-        t->t->demag->tune = TuneChoice{choices[0], choices[1], choices[2]};
+        TuneChoice& tc = t->t->demag->tune;
+        tc.cols_wide = choices[0];
+        tc.convz_reg = choices[1];
+        tc.xinv_run = choices[2];
+    });
+}
+
+int maf_term_demag_set_generic(maf_term t, int on) {
+    return guarded([&] {
+        check(t && t->t->kind == TK_DEMAG && t->t->demag && !t->t->demag_pbc(),
+              "maf_term_demag_set_generic: not a DemagField");
+        t->t->demag->tune.generic = on ? 1 : 0;
     });
 }
 
@@ -2402,6 +2414,9 @@ int maf_string_image(maf_string h, int i, maf_state* image) {
 struct maf_stoch_batch_s {
     std::vector<maf_stoch_s*> its;
     std::vector<maf_state_s*> sts;
+    bool fused = false;                     // batched passes (one launch per pass for all members)
+    std::unique_ptr<mafb::FusedBatch> fb;   // built at capture time when every member qualifies
+    bool fused_active = false;              // the current graph runs the batched passes
     cudaStream_t root = nullptr;
     cudaEvent_t fork = nullptr, done = nullptr;
     std::vector<cudaEvent_t> join;
@@ -2427,6 +2442,7 @@ void batch_drop_graph(maf_stoch_batch_s* b) {
     if (b->graph) cudaGraphDestroy(b->graph);
     b->exec = nullptr;
     b->graph = nullptr;
+    b->fused_active = false;
 }
 
 // device counters <- host step counts
@@ -2438,10 +2454,84 @@ void batch_upload_counters(maf_stoch_batch_s* b) {
     MAF_CUDA(cudaStreamSynchronize(b->root));
 }
 
+// The integrator's scheme with its noise stream indices relative to the step
+// counter q (the stages stoch_step builds).
+FusedScheme fused_scheme(const maf_stoch_s* h) {
+    FusedScheme f;
+    const double dt = h->dt;
+    if (h->mode == 0) {
+        FusedStage a; a.noise = true; a.offset = 0; a.scale = dt;
+        FusedStage b; b.n = 1; b.j[0] = 0; b.c[0] = 1.0; b.noise = true; b.offset = 1; b.scale = dt;
+        f.stages = {a, b};
+        f.nfin = 2; f.fin_base = 0; f.fin_c[0] = 0.5; f.fin_c[1] = 0.5;
+        f.noise_mul = 1;
+    } else if (h->mode == 1) {
+        FusedStage a; a.noise = true; a.offset = 0; a.scale = dt / 2.;
+        f.stages.push_back(a);
+        for (int i = 1; i < 6; ++i) {
+            FusedStage b; b.n = 1; b.j[0] = i - 1; b.c[0] = 1.0; b.noise = true; b.offset = 1;
+            b.scale = i < 5 ? dt / 2. : dt;
+            f.stages.push_back(b);
+        }
+        f.nfin = 1; f.fin_base = 5; f.fin_c[0] = 1.0;
+        f.noise_mul = 2;
+    } else {
+        FusedStage a; a.scale = dt;
+        FusedStage b; b.n = 1; b.j[0] = 0; b.c[0] = 1. / 2.; b.scale = dt;
+        FusedStage c; c.n = 1; c.j[0] = 1; c.c[0] = 1. / 2.; c.scale = dt;
+        FusedStage d; d.n = 1; d.j[0] = 2; d.c[0] = 1.0; d.scale = dt;
+        f.stages = {a, b, c, d};
+        f.nfin = 4; f.fin_base = 0; f.fin_c[0] = 1. / 6.; f.fin_c[1] = 2. / 6.; f.fin_c[2] = 2. / 6.; f.fin_c[3] = 1. / 6.;
+    }
+    return f;
+}
+
+// The batched-pass plan of the batch's members, or null when a member does not
+// qualify (3-D mesh, no or periodic DemagField, parameter fields, mixed
+// precisions or schemes): those batches keep the per-member graph.
+std::unique_ptr<FusedBatch> make_fused(maf_stoch_batch_s* b) {
+    const size_t n = b->its.size();
+    const FusedScheme sch = fused_scheme(b->its[0]);
+    const bool f32 = b->sts[0]->s.precision == PREC_FP32_FIELD;
+    std::vector<FusedMember> mem;
+    for (size_t i = 0; i < n; ++i) {
+        maf_stoch_s* h = b->its[i];
+        maf_state_s* st = b->sts[i];
+        if (h->mode != b->its[0]->mode || h->dt != b->its[0]->dt) return nullptr;
+        if ((st->s.precision == PREC_FP32_FIELD) != f32) return nullptr;
+        FusedMember f;
+        f.md = st->s.md;
+        f.Ms = st->s.Ms;
+        for (auto& t : h->terms) {
+            if (t->kind == TK_DEMAG) f.demag = t->demag.get();
+            f.terms.push_back(t->desc());
+        }
+        f.m[0] = st->s.m64.as<double>();
+        f.m[1] = h->mcand.as<double>();
+        f.m32 = f32 ? st->s.m32.as<float>() : nullptr;
+        f.mstage64 = h->mstage64.as<double>();
+        f.mstage32 = f32 ? h->mstage32.as<float>() : nullptr;
+        for (size_t s = 0; s < sch.stages.size(); ++s) f.k[s] = h->k[s].as<double>();
+        f.c_prec = -kGamma / (1. + h->alpha * h->alpha);
+        f.c_damp = -h->alpha * kGamma / (1. + h->alpha * h->alpha);
+        f.sigma = thermal_sigma(h, st->s);
+        f.seed = h->seed;
+        f.member = h->member;
+        f.q = b->q.as<unsigned long long>() + i;
+        if (!f.m[1] || !f.mstage64 || (f32 && (!f.m32 || !f.mstage32))) return nullptr;
+        mem.push_back(std::move(f));
+    }
+    if (!fused_supported(mem, sch)) return nullptr;
+    return std::make_unique<FusedBatch>(std::move(mem), sch, f32, b->root);
+}
+
 void batch_capture(maf_stoch_batch_s* b) {
     batch_drop_graph(b);
     const size_t n = b->its.size();
     auto* q = b->q.as<unsigned long long>();
+    b->fb.reset();
+    b->fused_active = false;
+    if (b->fused) b->fb = make_fused(b);
     // host-side state advances while the work is only recorded: restore it
     std::vector<double> t(n);
     std::vector<unsigned long long> steps(n), calls(n);
@@ -2452,14 +2542,22 @@ void batch_capture(maf_stoch_batch_s* b) {
     }
     MAF_CUDA(cudaStreamBeginCapture(b->root, cudaStreamCaptureModeThreadLocal));
     try {
-        MAF_CUDA(cudaEventRecord(b->fork, b->root));
-        for (size_t i = 0; i < n; ++i) {
-            cudaStream_t s = b->sts[i]->s.stream;
-            MAF_CUDA(cudaStreamWaitEvent(s, b->fork, 0));
-            stoch_step(b->its[i], b->sts[i], q + i);
-            stoch_step(b->its[i], b->sts[i], q + i);
-            MAF_CUDA(cudaEventRecord(b->join[i], s));
-            MAF_CUDA(cudaStreamWaitEvent(b->root, b->join[i], 0));
+        if (b->fb) {
+            // two steps of every member: the first writes the candidates, the second
+            // the states again, so the graph leaves the buffers where it found them
+            b->fb->record_step(b->root, 0);
+            b->fb->record_step(b->root, 1);
+            b->fused_active = true;
+        } else {
+            MAF_CUDA(cudaEventRecord(b->fork, b->root));
+            for (size_t i = 0; i < n; ++i) {
+                cudaStream_t s = b->sts[i]->s.stream;
+                MAF_CUDA(cudaStreamWaitEvent(s, b->fork, 0));
+                stoch_step(b->its[i], b->sts[i], q + i);
+                stoch_step(b->its[i], b->sts[i], q + i);
+                MAF_CUDA(cudaEventRecord(b->join[i], s));
+                MAF_CUDA(cudaStreamWaitEvent(b->root, b->join[i], 0));
+            }
         }
     } catch (...) {
         cudaGraph_t g = nullptr;
@@ -2517,6 +2615,21 @@ int maf_stoch_batch_create(maf_stoch_batch* out, const maf_stoch* integrators, c
 
 int maf_stoch_batch_destroy(maf_stoch_batch b) {
     return guarded([&] { delete b; });
+}
+
+int maf_stoch_batch_set_fused(maf_stoch_batch b, int on) {
+    return guarded([&] {
+        check(b, "NULL argument");
+        if (b->fused != (on != 0)) batch_drop_graph(b);
+        b->fused = on != 0;
+    });
+}
+
+int maf_stoch_batch_is_fused(maf_stoch_batch b, int* active) {
+    return guarded([&] {
+        check(b && active, "NULL argument");
+        *active = b->fused_active ? 1 : 0;
+    });
 }
 
 int maf_stoch_batch_steps(maf_stoch_batch b, int nsteps) {

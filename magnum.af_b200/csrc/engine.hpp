@@ -52,6 +52,10 @@ struct MeshDims {
 class Twiddles {
   public:
     const void* get(int L, bool fp64);
+    // the table of get() followed by the per-stage twiddle rows of a radix
+    // sequence (fft_ct.cuh: entry (jm, r - 1) of the stage with NS, RAD is
+    // W_L^(r jm L / (NS RAD))), for the compile-time transforms of length L
+    const void* get_ct(int L, bool fp64, const int* radix, int nstages);
   private:
     std::map<std::pair<int, int>, DevBuf> tables_;
 };
@@ -130,6 +134,8 @@ struct TuneChoice {
     int cols_wide = 0;
     int convz_reg = 1;
     int xinv_run = 0;
+    int cols_pipe = 1;  // forward y pass: persistent kernel staging the next tile's input (cp.async)
+    int generic = 0;    // 1: the run-time-plan kernels for every pass (as the batched passes run)
 };
 
 // Demag plan: the symmetry-reduced real spectral Newell tensor and the
@@ -164,6 +170,10 @@ class Demag {
     size_t tensor_elems() const { return (size_t)ncomp() * (md_.nz == 1 ? 1 : md_.nz + 1) * (md_.ny + 1) * nxh(); }
     int pitch() const { return pitch_; }
     template <typename R> int edens_blocks() const;
+    // buffers and tables of the generic passes, for the batched passes (batch.cu)
+    template <typename R> cplx_t<R>* spectrum() { return S1<R>(); }
+    template <typename R> const R* tensor_data() { return tensor<R>(); }
+    const void* twiddles(int L, bool fp64) { return tw_.get(L, fp64); }
 
   private:
     template <typename R> const R* tensor() ;

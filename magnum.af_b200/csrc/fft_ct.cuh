@@ -99,16 +99,40 @@ template <int RAD, int DIR, typename R> __device__ __forceinline__ void bfly_ct(
     }
 }
 
-// One stage over NB columns of length L with NT threads.  HOUT (last stage only):
-// just the outputs i < L/2 are written, the arithmetic only the others need is dropped.
-template <typename R, int RAD, int DIR, bool BFAST, int L, int NS, int NB, int NT, bool HOUT = false>
+// ----------------------------------------------------------------------------
+// Index arithmetic.  Element i of column b sits at sidx(i, b) of the tile.
+// Between the elements i and i + STEP of a column, spad is linear whenever
+// STEP is a multiple of 16 (for any i), and so is the run i = 16q + r,
+// r < 16; the stages below then address a butterfly's RAD elements as one base
+// index plus compile-time offsets instead of evaluating spad per element.
+// ----------------------------------------------------------------------------
+template <bool BFAST, int NB> __device__ __forceinline__ int sidx(int i, int b, int sb) {
+    return BFAST ? spad(i) * NB + b : spad(i) + b * sb;
+}
+// index distance of STEP consecutive elements of a column (STEP % 16 == 0)
+template <bool BFAST, int NB, int STEP> constexpr int sdist() { return (STEP + STEP / 16) * (BFAST ? NB : 1); }
+
+// Twiddle layout of the compile-time transforms (ct_twiddles on the host): the
+// table W_L^k, k in [0, L), followed, for every stage after the first, by one
+// row of its RAD - 1 twiddles per jm in [0, NS): entry (jm, r - 1) =
+// W_L^(r jm L / (NS RAD)), the same values as the table's.  A butterfly reads
+// its twiddles from one row at compile-time offsets.
+template <int NS, int RAD> constexpr int tw_rows() { return NS > 1 ? NS * (RAD - 1) : 0; }
+
+// One stage over NB columns of length L with NT threads; TWO is the offset of
+// the stage's twiddle rows.  HOUT (last stage only): just the outputs i < L/2
+// are written, the arithmetic only the others need is dropped.
+template <typename R, int RAD, int DIR, bool BFAST, int L, int NS, int NB, int NT, int TWO, bool HOUT = false>
 __device__ __forceinline__ void ct_stage(cplx_t<R>* s, int sb, const cplx_t<R>* __restrict__ tw) {
     static_assert(!HOUT || NS * RAD == L, "output pruning is for the last stage");
     using C = cplx_t<R>;
     constexpr int NBF = L / RAD;
     constexpr int TOTAL = NBF * NB;
     constexpr int BPT = (TOTAL + NT - 1) / NT;
-    constexpr int TWST = L / (NS * RAD);
+    constexpr bool LIN_IN = NBF % 16 == 0;
+    constexpr int DIN = LIN_IN ? sdist<BFAST, NB, NBF>() : 0;
+    constexpr bool LIN_OUT = (NS % 16 == 0) || (NS == 1 && 16 % RAD == 0);
+    constexpr int DOUT = NS == 1 ? (BFAST ? NB : 1) : (LIN_OUT ? sdist<BFAST, NB, NS>() : 0);
     C v[BPT][RAD];
 #pragma unroll
     for (int k = 0; k < BPT; ++k) {
@@ -117,12 +141,13 @@ __device__ __forceinline__ void ct_stage(cplx_t<R>* s, int sb, const cplx_t<R>* 
             const int b = BFAST ? q % NB : q / NBF;
             const int j = BFAST ? q / NB : q % NBF;
             const int jm = j % NS;
+            const C* __restrict__ twr = tw + TWO + jm * (RAD - 1) - 1;
+            const int base = LIN_IN ? sidx<BFAST, NB>(j, b, sb) : 0;
 #pragma unroll
             for (int r = 0; r < RAD; ++r) {
-                const int i = j + r * NBF;
-                C x = s[BFAST ? spad(i) * NB + b : spad(i) + b * sb];
+                C x = s[LIN_IN ? base + r * DIN : sidx<BFAST, NB>(j + r * NBF, b, sb)];
                 if (NS > 1 && r > 0) {
-                    const C w = tw[r * jm * TWST];
+                    const C w = twr[r];
                     x = DIR < 0 ? cmul(x, w) : cmulc(x, w);
                 }
                 v[k][r] = x;
@@ -139,40 +164,42 @@ __device__ __forceinline__ void ct_stage(cplx_t<R>* s, int sb, const cplx_t<R>* 
             const int j = BFAST ? q / NB : q % NBF;
             const int jm = j % NS;
             const int d = (j - jm) * RAD + jm;
+            const int base = LIN_OUT ? sidx<BFAST, NB>(d, b, sb) : 0;
 #pragma unroll
             for (int r = 0; r < RAD; ++r) {
                 if (HOUT && r >= RAD / 2) continue;
-                const int i = d + r * NS;
-                s[BFAST ? spad(i) * NB + b : spad(i) + b * sb] = v[k][r];
+                s[LIN_OUT ? base + r * DOUT : sidx<BFAST, NB>(d + r * NS, b, sb)] = v[k][r];
             }
         }
     }
     __syncthreads();
 }
 
-template <typename R, int DIR, bool BFAST, int L, int NS, int NB, int NT, bool HOUT, int RAD, int... REST>
+template <typename R, int DIR, bool BFAST, int L, int NS, int NB, int NT, bool HOUT, int TWO, int RAD, int... REST>
 __device__ __forceinline__ void ct_run(cplx_t<R>* s, int sb, const cplx_t<R>* __restrict__ tw) {
     if constexpr (sizeof...(REST) > 0) {
-        ct_stage<R, RAD, DIR, BFAST, L, NS, NB, NT>(s, sb, tw);
-        ct_run<R, DIR, BFAST, L, NS * RAD, NB, NT, HOUT, REST...>(s, sb, tw);
+        ct_stage<R, RAD, DIR, BFAST, L, NS, NB, NT, TWO>(s, sb, tw);
+        ct_run<R, DIR, BFAST, L, NS * RAD, NB, NT, HOUT, TWO + tw_rows<NS, RAD>(), REST...>(s, sb, tw);
     } else {
-        ct_stage<R, RAD, DIR, BFAST, L, NS, NB, NT, HOUT>(s, sb, tw);
+        ct_stage<R, RAD, DIR, BFAST, L, NS, NB, NT, TWO, HOUT>(s, sb, tw);
     }
 }
 
 template <typename R, int DIR, bool BFAST, int L, int NB, int NT, int... RS>
 __device__ __forceinline__ void ct_fft(cplx_t<R>* s, int sb, const cplx_t<R>* __restrict__ tw, Radices<RS...>) {
-    ct_run<R, DIR, BFAST, L, 1, NB, NT, false, RS...>(s, sb, tw);
+    ct_run<R, DIR, BFAST, L, 1, NB, NT, false, L, RS...>(s, sb, tw);
 }
 
 // ----------------------------------------------------------------------------
 // Stages with global I/O fused in.  The first stage (Ns = 1, no twiddles) takes
-// its RAD inputs j + r L/RAD of column b from ld(b, i) -- straight from global
-// memory into registers, so the zero-padded half of a transform costs no
+// its RAD inputs j + r L/RAD of column b from ld(b, j, r L/RAD) -- straight from
+// global memory into registers, so the zero-padded half of a transform costs no
 // shared-memory traffic -- and writes its outputs j RAD + r to shared memory.
 // The last stage (Ns = L/RAD) reads shared memory and hands its outputs
-// j + r Ns to st(b, i, value), so rows that are truncated are never stored.
-// Each saves one shared-memory round trip and one barrier per element.
+// j + r Ns to st(b, j, r Ns, value), so rows that are truncated are never
+// stored.  The loader and the storer get the element as a per-butterfly part
+// (b, j) and a compile-time offset, so that they can form one address per
+// butterfly and add constant offsets to it.
 // ----------------------------------------------------------------------------
 template <bool BFAST, int NB, int NBF> __device__ __forceinline__ void ct_bj(int q, int& b, int& j) {
     b = BFAST ? q % NB : q / NBF;
@@ -189,6 +216,7 @@ __device__ __forceinline__ void ct_stage_in(cplx_t<R>* s, int sb, LD&& ld) {
     constexpr int TOTAL = NBF * NB;
     constexpr int BPT = (TOTAL + NT - 1) / NT;
     constexpr bool HALF = HIN && RAD == 16;
+    constexpr bool LIN_OUT = 16 % RAD == 0;
     C v[BPT][RAD];
 #pragma unroll
     for (int k = 0; k < BPT; ++k) {
@@ -197,7 +225,7 @@ __device__ __forceinline__ void ct_stage_in(cplx_t<R>* s, int sb, LD&& ld) {
             int b, j;
             ct_bj<BFAST, NB, NBF>(q, b, j);
 #pragma unroll
-            for (int r = 0; r < RAD; ++r) v[k][r] = (HALF && r >= RAD / 2) ? mk((R)0, (R)0) : ld(b, j + r * NBF);
+            for (int r = 0; r < RAD; ++r) v[k][r] = (HALF && r >= RAD / 2) ? mk((R)0, (R)0) : ld(b, j, r * NBF);
         }
     }
 #pragma unroll
@@ -210,11 +238,10 @@ __device__ __forceinline__ void ct_stage_in(cplx_t<R>* s, int sb, LD&& ld) {
                 bfly16_half<DIR, R>(v[k]);
             else
                 bfly_ct<RAD, DIR, R>(v[k]);
+            const int base = sidx<BFAST, NB>(j * RAD, b, sb);
 #pragma unroll
-            for (int r = 0; r < RAD; ++r) {
-                const int i = j * RAD + r;
-                s[BFAST ? spad(i) * NB + b : spad(i) + b * sb] = v[k][r];
-            }
+            for (int r = 0; r < RAD; ++r)
+                s[LIN_OUT ? base + r * (BFAST ? NB : 1) : sidx<BFAST, NB>(j * RAD + r, b, sb)] = v[k][r];
         }
     }
     __syncthreads();
@@ -224,26 +251,29 @@ __device__ __forceinline__ void ct_stage_in(cplx_t<R>* s, int sb, LD&& ld) {
 // barrier at the end: the caller synchronises before s is reused.
 // HOUT: only the outputs i < L/2 are wanted (a truncated transform): the others
 // are not stored, and the arithmetic that only they need is dropped.
-template <typename R, int RAD, int DIR, bool BFAST, int L, int NB, int NT, bool HOUT, typename ST>
+template <typename R, int RAD, int DIR, bool BFAST, int L, int NB, int NT, bool HOUT, int TWO, typename ST>
 __device__ __forceinline__ void ct_stage_out(const cplx_t<R>* s, int sb, const cplx_t<R>* __restrict__ tw, ST&& st) {
     using C = cplx_t<R>;
     constexpr int NBF = L / RAD;
     constexpr int NS = NBF;
     constexpr int TOTAL = NBF * NB;
     constexpr int BPT = (TOTAL + NT - 1) / NT;
+    constexpr bool LIN_IN = NBF % 16 == 0;
+    constexpr int DIN = LIN_IN ? sdist<BFAST, NB, NBF>() : 0;
 #pragma unroll
     for (int k = 0; k < BPT; ++k) {
         const int q = threadIdx.x + k * NT;
         if (TOTAL % NT == 0 || q < TOTAL) {
             int b, j;
             ct_bj<BFAST, NB, NBF>(q, b, j);
+            const C* __restrict__ twr = tw + TWO + j * (RAD - 1) - 1;
+            const int base = LIN_IN ? sidx<BFAST, NB>(j, b, sb) : 0;
             C v[RAD];
 #pragma unroll
             for (int r = 0; r < RAD; ++r) {
-                const int i = j + r * NBF;
-                C x = s[BFAST ? spad(i) * NB + b : spad(i) + b * sb];
+                C x = s[LIN_IN ? base + r * DIN : sidx<BFAST, NB>(j + r * NBF, b, sb)];
                 if (NS > 1 && r > 0) {
-                    const C w = tw[r * j];
+                    const C w = twr[r];
                     x = DIR < 0 ? cmul(x, w) : cmulc(x, w);
                 }
                 v[r] = x;
@@ -251,20 +281,20 @@ __device__ __forceinline__ void ct_stage_out(const cplx_t<R>* s, int sb, const c
             bfly_ct<RAD, DIR, R>(v);
 #pragma unroll
             for (int r = 0; r < RAD; ++r)
-                if (!HOUT || r < RAD / 2) st(b, j + r * NS, v[r]);
+                if (!HOUT || r < RAD / 2) st(b, j, r * NS, v[r]);
         }
     }
 }
 
-template <typename R, int DIR, bool BFAST, int L, int NS, int NB, int NT, bool HOUT, typename ST, int RAD,
+template <typename R, int DIR, bool BFAST, int L, int NS, int NB, int NT, bool HOUT, int TWO, typename ST, int RAD,
           int... REST>
 __device__ __forceinline__ void ct_run_out(cplx_t<R>* s, int sb, const cplx_t<R>* __restrict__ tw, ST&& st) {
     if constexpr (sizeof...(REST) == 0) {
         static_assert(NS * RAD == L, "radix sequence");
-        ct_stage_out<R, RAD, DIR, BFAST, L, NB, NT, HOUT>(s, sb, tw, st);
+        ct_stage_out<R, RAD, DIR, BFAST, L, NB, NT, HOUT, TWO>(s, sb, tw, st);
     } else {
-        ct_stage<R, RAD, DIR, BFAST, L, NS, NB, NT>(s, sb, tw);
-        ct_run_out<R, DIR, BFAST, L, NS * RAD, NB, NT, HOUT, ST, REST...>(s, sb, tw, st);
+        ct_stage<R, RAD, DIR, BFAST, L, NS, NB, NT, TWO>(s, sb, tw);
+        ct_run_out<R, DIR, BFAST, L, NS * RAD, NB, NT, HOUT, TWO + tw_rows<NS, RAD>(), ST, REST...>(s, sb, tw, st);
     }
 }
 
@@ -276,7 +306,7 @@ __device__ __forceinline__ void ct_fft_in(cplx_t<R>* s, int sb, const cplx_t<R>*
                                           Radices<R0, RS...>) {
     static_assert(!HOUT || sizeof...(RS) > 0, "output pruning needs a separate last stage");
     ct_stage_in<R, R0, DIR, BFAST, L, NB, NT, HIN>(s, sb, ld);
-    if constexpr (sizeof...(RS) > 0) ct_run<R, DIR, BFAST, L, R0, NB, NT, HOUT, RS...>(s, sb, tw);
+    if constexpr (sizeof...(RS) > 0) ct_run<R, DIR, BFAST, L, R0, NB, NT, HOUT, L, RS...>(s, sb, tw);
 }
 
 // ct_fft_in with a hook between the first stage and the others: the first stage
@@ -288,14 +318,14 @@ __device__ __forceinline__ void ct_fft_in_hook(cplx_t<R>* s, int sb, const cplx_
                                                MID&& mid, Radices<R0, RS...>) {
     ct_stage_in<R, R0, DIR, BFAST, L, NB, NT, HIN>(s, sb, ld);
     mid();
-    if constexpr (sizeof...(RS) > 0) ct_run<R, DIR, BFAST, L, R0, NB, NT, false, RS...>(s, sb, tw);
+    if constexpr (sizeof...(RS) > 0) ct_run<R, DIR, BFAST, L, R0, NB, NT, false, L, RS...>(s, sb, tw);
 }
 
 // shared memory -> ... -> last stage -> global (HOUT: only outputs i < L/2 are stored)
 template <typename R, int DIR, bool BFAST, int L, int NB, int NT, bool HOUT = false, typename ST, int... RS>
 __device__ __forceinline__ void ct_fft_out(cplx_t<R>* s, int sb, const cplx_t<R>* __restrict__ tw, ST&& st,
                                            Radices<RS...>) {
-    ct_run_out<R, DIR, BFAST, L, 1, NB, NT, HOUT, ST, RS...>(s, sb, tw, st);
+    ct_run_out<R, DIR, BFAST, L, 1, NB, NT, HOUT, L, ST, RS...>(s, sb, tw, st);
 }
 
 // global -> ... -> global; the caller synchronises before s is reused
@@ -315,20 +345,39 @@ __device__ __forceinline__ void ct_fft_io(cplx_t<R>* s, int sb, const cplx_t<R>*
             if (NB % NT == 0 || q < NB) {
                 C v[R0];
 #pragma unroll
-                for (int r = 0; r < R0; ++r) v[r] = (HALF && r >= R0 / 2) ? mk((R)0, (R)0) : ld(q, r);
+                for (int r = 0; r < R0; ++r) v[r] = (HALF && r >= R0 / 2) ? mk((R)0, (R)0) : ld(q, 0, r);
                 if constexpr (HALF)
                     bfly16_half<DIR, R>(v);
                 else
                     bfly_ct<R0, DIR, R>(v);
 #pragma unroll
                 for (int r = 0; r < R0; ++r)
-                    if (!HOUT || r < R0 / 2) st(q, r, v[r]);
+                    if (!HOUT || r < R0 / 2) st(q, 0, r, v[r]);
             }
         }
     } else {
         ct_stage_in<R, R0, DIR, BFAST, L, NB, NT, HIN>(s, sb, ld);
-        ct_run_out<R, DIR, BFAST, L, R0, NB, NT, HOUT, ST, RS...>(s, sb, tw, st);
+        ct_run_out<R, DIR, BFAST, L, R0, NB, NT, HOUT, L, ST, RS...>(s, sb, tw, st);
     }
+}
+
+// ct_fft_io with a hook between the first stage and the others (the first stage
+// ends with a barrier: its load source is free when mid() runs); more than one stage.
+template <typename R, int DIR, bool BFAST, int L, int NB, int NT, bool HIN, bool HOUT, typename LD, typename MID,
+          typename ST, int R0, int... RS>
+__device__ __forceinline__ void ct_fft_io_hook(cplx_t<R>* s, int sb, const cplx_t<R>* __restrict__ tw, LD&& ld,
+                                               MID&& mid, ST&& st, Radices<R0, RS...>) {
+    static_assert(sizeof...(RS) > 0, "a hook needs more than one stage");
+    ct_stage_in<R, R0, DIR, BFAST, L, NB, NT, HIN>(s, sb, ld);
+    mid();
+    ct_run_out<R, DIR, BFAST, L, R0, NB, NT, HOUT, L, ST, RS...>(s, sb, tw, st);
+}
+
+// radix sequence of a compile-time plan as a host array (for the twiddle rows)
+template <int... RS> constexpr int radix_count(Radices<RS...>) { return (int)sizeof...(RS); }
+template <int... RS> inline void radix_list(Radices<RS...>, int* out) {
+    const int v[] = {RS...};
+    for (int i = 0; i < (int)sizeof...(RS); ++i) out[i] = v[i];
 }
 
 // radix sequence per power-of-two length (16 first, smaller radices last)

@@ -71,6 +71,36 @@ const void* Twiddles::get(int L, bool fp64) {
     return p;
 }
 
+const void* Twiddles::get_ct(int L, bool fp64, const int* radix, int nstages) {
+    // one compile-time plan per length, so (L, precision) identifies the layout
+    auto key = std::make_pair(L, fp64 ? 3 : 2);
+    auto it = tables_.find(key);
+    if (it != tables_.end()) return it->second.p;
+    const void* base = get(L, fp64);
+    const size_t esz = fp64 ? sizeof(double2) : sizeof(float2);
+    std::vector<unsigned char> tab((size_t)L * esz);
+    MAF_CUDA(cudaMemcpy(tab.data(), base, (size_t)L * esz, cudaMemcpyDeviceToHost));
+    std::vector<unsigned char> out(tab);
+    int NS = 1;
+    for (int st = 0; st < nstages; ++st) {
+        const int RAD = radix[st];
+        if (NS > 1) {
+            const int twst = L / (NS * RAD);
+            for (int jm = 0; jm < NS; ++jm)
+                for (int r = 1; r < RAD; ++r) {
+                    const size_t k = (size_t)r * jm * twst;  // < L
+                    out.insert(out.end(), tab.begin() + k * esz, tab.begin() + (k + 1) * esz);
+                }
+        }
+        NS *= RAD;
+    }
+    DevBuf buf(out.size());
+    MAF_CUDA(cudaMemcpy(buf.p, out.data(), out.size(), cudaMemcpyHostToDevice));
+    const void* p = buf.p;
+    tables_.emplace(key, std::move(buf));
+    return p;
+}
+
 FFTPlan make_fft_plan(int L, const void* tw) {
     FFTPlan p;
     p.L = L;
@@ -249,22 +279,6 @@ template <typename K> static void set_smem(K kernel, size_t bytes) {
     if (bytes > 32 * 1024) MAF_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
 }
 
-static int round_threads(int t) {
-    t = std::max(t, 32);
-    t = (t + 31) / 32 * 32;
-    if (t > kMaxFftThreads) throw Error(6, "FFT tile needs more threads than one CTA has (transform length too large)");
-    return t;
-}
-
-// choose columns-per-tile so that the tile holds about `target` complex values
-static int pick_nb(int L, int target, int ncols, int nbmax) {
-    int nb = std::max(1, target / std::max(L, 1));
-    nb = std::min(nb, nbmax);
-    nb = std::min(nb, std::max(ncols, 1));
-    return nb;
-}
-
-template <typename R> static int tile_target() { return sizeof(R) == 4 ? 8192 : 4096; }
 
 template <typename R>
 static void launch_xfwd(const R* in, int n_in, int64_t rows, int64_t rows_pc, const R* msf, R ms, cplx_t<R>* out,
@@ -435,7 +449,7 @@ template <typename R> void Demag::forward_conv(const R* m, const MsInfo& ms, cud
     C* s1 = S1<R>();
     // the periodic form has no tensor and runs the run-time plans only
     const R* Nr = pbc_ ? nullptr : tensor<R>();
-    const bool ct = !pbc_;
+    const bool ct = !pbc_ && !tune.generic;
     const PbcOp pop{nx, ny, nz, md_.dx, md_.dy, md_.dz};
     // pass 1: x forward (zero pad fused)
     launch_xfwd<R>(m, nx, 3 * rows_pc, rows_pc, msf, (R)ms.Ms, s1, pitch_, Px(), tw_, st, ct);
@@ -518,7 +532,7 @@ void Demag::inverse_x_epilogue(const R* m, const MsInfo& ms, const TermList& tl,
                                cudaStream_t st, int* nblocks_out, PassMarks* marks) {
     const bool f64 = sizeof(R) == 8;
     const int Lc = Px() / 2;
-    if (!pbc_) {
+    if (!pbc_ && !tune.generic) {
         const R scale = (R)(1.0 / ((double)Px() * Py() * Pz()));
         if (ct_xinv<R>(S1<R>(), pitch_, Px(), tw_, md_.geom(), scale, m, ms, tl, ep, tune, st, nblocks_out)) {
             if (marks) marks->mark(st, "x_inv_local");

@@ -55,8 +55,9 @@ __global__ void __launch_bounds__(NT) k_xfwd_ct(const R* __restrict__ in, int n_
     static_assert(LC * NB % NT == 0, "tile");
     const int64_t r0 = (int64_t)blockIdx.x * NB;
     const bool even = (n_in & 1) == 0;
-    // packed pair (in[2k], in[2k+1]) * Ms of row b, loaded straight into the first stage
-    auto ld = [&](int b, int k) -> C {
+    // packed pair (in[2k], in[2k+1]) * Ms of row b, k = j + dk, loaded straight into the first stage
+    auto ld = [&](int b, int j, int dk) -> C {
+        const int k = j + dk;
         const int64_t row = r0 + b;
         R a = 0, c = 0;
         if (row < rows) {
@@ -139,10 +140,10 @@ __global__ void __launch_bounds__(NT, 4) k_xfwd_pipe(const R* __restrict__ in, i
         const int64_t r0 = tile * NB;
         asm volatile("cp.async.wait_all;\n" ::);
         __syncthreads();
-        auto ld = [&](int b, int k) -> C {
-            const int x0 = 2 * k;
-            if (r0 + b >= rows || x0 >= n_in) return mk((R)0, (R)0);
-            const C v = *reinterpret_cast<const C*>(stage + b * n_in + x0);
+        // the packed values k = j + dk < LC/2 of a pruned first stage are all inside the row (n_in = LC)
+        auto ld = [&](int b, int j, int dk) -> C {
+            if (r0 + b >= rows) return mk((R)0, (R)0);
+            const C v = reinterpret_cast<const C*>(stage + b * n_in)[j + dk];
             return mk(v.x * ms, v.y * ms);
         };
         const int64_t next = tile + gridDim.x;
@@ -186,11 +187,80 @@ __global__ void __launch_bounds__(NT, (kMinBlocks<R, NT * (L * NB / kE > NT ? L 
     const C* ib = in + (int64_t)blockIdx.y * in_sbat + c0;
     C* ob = out + (int64_t)blockIdx.y * out_sbat + c0;
     const int ncv = min(NB, ncols - c0);
-    auto ld = [&](int b, int i) -> C { return (i < n_in && b < ncv) ? ib[i * in_si + b] : mk((R)0, (R)0); };
-    auto st = [&](int b, int i, C v) {
-        if (i < n_out && b < ncv) ob[i * out_si + b] = v;
+    // element i = j + di of column b; the host guarantees n_in = L/2 (HIN) or L and
+    // n_out = L/2 (HOUT) or L, so every element the stages touch is in range
+    auto ld = [&](int b, int j, int di) -> C {
+        return b < ncv ? ib[(int64_t)j * in_si + b + (int64_t)di * in_si] : mk((R)0, (R)0);
+    };
+    auto st = [&](int b, int j, int di, C v) {
+        if (b < ncv) ob[(int64_t)j * out_si + b + (int64_t)di * out_si] = v;
     };
     ct_fft_io<R, DIR, true, L, NB, NT, HIN, HOUT>(s, 0, tw, ld, st, typename CtPlan<L>::T());
+}
+
+// Column transforms, persistent and pipelined: each CTA walks tiles of NB
+// columns (tile = column block x batch); the NIN input rows of the next tile
+// (L/2 with a zero-padded input, else L) are copied into a shared-memory
+// staging buffer [NIN][NB] with cp.async while the current tile's later stages
+// and stores run (issued right after the first stage, the buffer's only
+// reader).  Needs 16-byte row segments (NB * sizeof(C) and the pitch multiples
+// of 16 bytes); chunks beyond the pitch are skipped.
+template <typename R, int L, int NB> constexpr size_t cols_stage_offset() {
+    return (sizeof(cplx_t<R>) * NB * ((L - 1) + ((L - 1) >> 4) + 1) + 15) / 16 * 16;
+}
+template <typename R, int L, int NB, bool HIN> constexpr size_t cols_pipe_smem() {
+    return cols_stage_offset<R, L, NB>() + sizeof(cplx_t<R>) * NB * (HIN ? L / 2 : L);
+}
+
+template <typename R, int DIR, int L, int NB, int NT, bool HIN, bool HOUT>
+__global__ void __launch_bounds__(NT, NT >= 512 ? 1 : 2) k_cols_pipe(const cplx_t<R>* in, cplx_t<R>* out, int ncols, int64_t in_si,
+                                                   int64_t out_si, int64_t in_sbat, int64_t out_sbat, int nbat,
+                                                   int pitch, const cplx_t<R>* __restrict__ tw) {
+    using C = cplx_t<R>;
+    constexpr int NIN = HIN ? L / 2 : L;
+    constexpr int CPR = NB * (int)sizeof(C) / 16;  // 16-byte chunks per staged row
+    static_assert(NB * sizeof(C) % 16 == 0, "16-byte row segments");
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C* s = reinterpret_cast<C*>(smem_raw);
+    C* stage = reinterpret_cast<C*>(smem_raw + cols_stage_offset<R, L, NB>());
+    const int ntx = (ncols + NB - 1) / NB;
+    const int64_t ntiles = (int64_t)ntx * nbat;
+    constexpr int EPC = 16 / (int)sizeof(C);  // complex values per chunk
+    auto prefetch = [&](int64_t tile) {
+        const int tx = (int)(tile % ntx), bat = (int)(tile / ntx);
+        const unsigned char* src0 = reinterpret_cast<const unsigned char*>(in + bat * in_sbat + tx * NB);
+        const unsigned dst0 = (unsigned)__cvta_generic_to_shared(stage);
+        // chunks that start beyond the row pitch are not copied (their columns are
+        // beyond ncols: read from the staging buffer, never stored)
+        const int cmax = min(CPR, (pitch - tx * NB) / EPC);
+#pragma unroll 4
+        for (int q = threadIdx.x; q < NIN * CPR; q += NT) {
+            const int i = q / CPR, c = q - i * CPR;
+            if (c >= cmax) continue;
+            const unsigned char* src = src0 + (int64_t)i * in_si * (int64_t)sizeof(C) + c * 16;
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst0 + (unsigned)q * 16u), "l"(src));
+        }
+        asm volatile("cp.async.commit_group;\n" ::);
+    };
+    int64_t tile = blockIdx.x;
+    if (tile < ntiles) prefetch(tile);
+    for (; tile < ntiles; tile += gridDim.x) {
+        const int tx = (int)(tile % ntx), bat = (int)(tile / ntx);
+        const int c0 = tx * NB;
+        const int ncv = min(NB, ncols - c0);
+        C* ob = out + bat * out_sbat + c0;
+        asm volatile("cp.async.wait_all;\n" ::);
+        __syncthreads();
+        // element i = j + di of column b, from the staging buffer
+        auto ld = [&](int b, int j, int di) -> C { return stage[(j + di) * NB + b]; };
+        auto st = [&](int b, int j, int di, C v) {
+            if (b < ncv) ob[(int64_t)j * out_si + b + (int64_t)di * out_si] = v;
+        };
+        const int64_t next = tile + gridDim.x;
+        ct_fft_io_hook<R, DIR, true, L, NB, NT, HIN, HOUT>(
+            s, 0, tw, ld, [&] { if (next < ntiles) prefetch(next); }, st, typename CtPlan<L>::T());
+        __syncthreads();  // s is rewritten by the next tile's first stage
+    }
 }
 
 // -------------------------------------------------- z convolution (3-D meshes)
@@ -221,9 +291,9 @@ __global__ void __launch_bounds__(NT, (kMinBlocks<R, NT, 768, 512>)) k_convz_ct(
         ok = i < nz && b < ncv && (row == 0 || two);
         return comp * cs + i * si + (int64_t)(row ? ky2 : ky) * pitch + c0 + b;
     };
-    auto ld = [&](int col, int i) -> C {
+    auto ld = [&](int col, int j, int di) -> C {
         bool ok;
-        const int64_t o = at(col, i, ok);
+        const int64_t o = at(col, j + di, ok);
         return ok ? S[o] : mk((R)0, (R)0);
     };
     // L = 2 nz: the upper half of the input is the padding, of the output the truncation
@@ -252,9 +322,9 @@ __global__ void __launch_bounds__(NT, (kMinBlocks<R, NT, 768, 512>)) k_convz_ct(
         }
     }
     __syncthreads();
-    auto st = [&](int col, int i, C v) {
+    auto st = [&](int col, int j, int di, C v) {
         bool ok;
-        const int64_t o = at(col, i, ok);
+        const int64_t o = at(col, j + di, ok);
         if (ok) S[o] = v;
     };
     ct_fft_out<R, 1, true, L, NC, NT, true>(s, 0, tw, st, typename CtPlan<L>::T());
@@ -386,8 +456,9 @@ __global__ void __launch_bounds__(NT) k_convy_ct(cplx_t<R>* S, const R* __restri
     const int ncv = min(NB, nxh - c0);
     const int64_t cs = (int64_t)ny * pitch;
     // column col = (comp, b) at y = i; rows i >= ny are padding
-    auto ld = [&](int col, int i) -> C {
+    auto ld = [&](int col, int j, int di) -> C {
         const int comp = col / NB, b = col % NB;
+        const int i = j + di;
         return (i < ny && b < ncv) ? S[comp * cs + (int64_t)i * pitch + c0 + b] : mk((R)0, (R)0);
     };
     // L = 2 ny: zero-padded input, truncated output
@@ -408,8 +479,9 @@ __global__ void __launch_bounds__(NT) k_convy_ct(cplx_t<R>* S, const R* __restri
         s[base + 2 * NB] = cscale(mz, Nzz);
     }
     __syncthreads();
-    auto st = [&](int col, int i, C v) {
+    auto st = [&](int col, int j, int di, C v) {
         const int comp = col / NB, b = col % NB;
+        const int i = j + di;
         if (i < ny && b < ncv) S[comp * cs + (int64_t)i * pitch + c0 + b] = v;
     };
     ct_fft_out<R, 1, true, L, NC, NT, true>(s, 0, tw, st, typename CtPlan<L>::T());
@@ -431,15 +503,15 @@ __global__ void __launch_bounds__(NT, (kMinBlocks<R, NT, (RN == 2 ? MAF_XINV_THR
     const int ry0 = blockIdx.x * NBR;
     // Z[k] = (X[k] + X*[LC-k]) + i (X[k] - X*[LC-k]) W^-k of column (comp, row),
     // formed from global memory straight into the first stage
-    auto ld = [&](int col, int k) -> C {
+    auto ld = [&](int col, int j, int dk) -> C {
         const int comp = col / NBR;
         const int ry = ry0 + col % NBR;
         if (ry >= rows_pc) return mk((R)0, (R)0);
         const C* rp = S1 + ((int64_t)comp * rows_pc + ry) * pitch;
-        const C Xk = rp[k];
-        const C Xm = rp[LC - k];
+        const C Xk = (rp + j)[dk];
+        const C Xm = (rp + (LC - j))[-dk];
         const C E_ = cadd(Xk, cconj(Xm));
-        const C O = cmulc(csub(Xk, cconj(Xm)), twP[k]);
+        const C O = cmulc(csub(Xk, cconj(Xm)), (twP + j)[dk]);
         return cadd(E_, cmul_i<1>(O));
     };
     // only the first nx of the 2 LC real outputs (packed values k < LC/2) are kept
@@ -534,6 +606,15 @@ constexpr int pow2floor(int x) {
     return p;
 }
 
+// twiddles of the compile-time transform of length L: the W_L table and the
+// stage rows of its radix sequence
+template <int L> static const void* ct_tw(Twiddles& tw, bool f64) {
+    using P = typename CtPlan<L>::T;
+    int rad[8] = {};
+    radix_list(P(), rad);
+    return tw.get_ct(L, f64, rad, radix_count(P()));
+}
+
 template <typename R, int LC, bool HIN>
 static void xfwd_L(const R* in, int n_in, int64_t rows, int64_t rows_pc, const R* msf, R ms, cplx_t<R>* out, int pitch,
                    const void* tw, const void* twP, cudaStream_t st) {
@@ -576,11 +657,32 @@ static void xfwd_L(const R* in, int n_in, int64_t rows, int64_t rows_pc, const R
 
 template <typename R, int DIR, int L, int TILE, bool HIN, bool HOUT>
 static void cols_L(const cplx_t<R>* in, cplx_t<R>* out, int n_in, int n_out, int ncols, int64_t in_si, int64_t out_si,
-                   int64_t in_sbat, int64_t out_sbat, int nbat, const void* tw, cudaStream_t st) {
+                   int64_t in_sbat, int64_t out_sbat, int nbat, const void* tw, int pipe, int pitch, cudaStream_t st) {
     constexpr int NB = pow2floor(cmin(32, cmax(1, TILE / L)));
     constexpr int NT = L * NB / (kE * kColsBpt<R>) > 0 ? L * NB / (kE * kColsBpt<R>) : 1;
     static_assert(NT <= 1024, "CTA size");
     const size_t smem = sizeof(cplx_t<R>) * (size_t)NB * ((L - 1) + ((L - 1) >> 4) + 1);
+    if constexpr (HIN && !HOUT && L >= 256 && NB * sizeof(cplx_t<R>) % 16 == 0) {
+        // pipelined persistent variant: the column tiles stay inside the row pitch,
+        // 16-byte aligned rows and batches
+        const int ntx = (int)ceil_div(ncols, NB);
+        const bool ok = pipe && ncols <= pitch && (pitch * sizeof(cplx_t<R>)) % 16 == 0 && (uintptr_t)in % 16 == 0 &&
+                        (in_si * (int64_t)sizeof(cplx_t<R>)) % 16 == 0 &&
+                        (in_sbat * (int64_t)sizeof(cplx_t<R>)) % 16 == 0;
+        if (ok) {
+            auto kp = k_cols_pipe<R, DIR, L, NB, NT, HIN, HOUT>;
+            const size_t smem_p = cols_pipe_smem<R, L, NB, HIN>();
+            ct_smem(kp, smem_p);
+            int per_sm = 0;
+            MAF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kp, NT, smem_p));
+            const int64_t ntiles = (int64_t)ntx * nbat;
+            const unsigned grid = (unsigned)std::min<int64_t>(ntiles, (int64_t)std::max(per_sm, 1) * sm_count());
+            kp<<<grid, NT, smem_p, st>>>(in, out, ncols, in_si, out_si, in_sbat, out_sbat, nbat, pitch,
+                                         static_cast<const cplx_t<R>*>(tw));
+            MAF_LAUNCH_CHECK();
+            return;
+        }
+    }
     auto k = k_cols_ct<R, DIR, L, NB, NT, HIN, HOUT>;
     ct_smem(k, smem);
     dim3 grid((unsigned)ceil_div(ncols, NB), (unsigned)nbat);
@@ -699,9 +801,9 @@ bool ct_xfwd(const R* in, int n_in, int64_t rows, int64_t rows_pc, const R* msf,
 #define X(N)                                                                                                   \
     do {                                                                                                       \
         if (half)                                                                                              \
-            xfwd_L<R, N, true>(in, n_in, rows, rows_pc, msf, ms, out, pitch, tw.get(N, f64), tw.get(Px, f64), st); \
+            xfwd_L<R, N, true>(in, n_in, rows, rows_pc, msf, ms, out, pitch, ct_tw<N>(tw, f64), tw.get(Px, f64), st); \
         else if constexpr (sizeof(R) == 8)                                                                     \
-            xfwd_L<R, N, false>(in, n_in, rows, rows_pc, msf, ms, out, pitch, tw.get(N, f64), tw.get(Px, f64), st); \
+            xfwd_L<R, N, false>(in, n_in, rows, rows_pc, msf, ms, out, pitch, ct_tw<N>(tw, f64), tw.get(Px, f64), st); \
     } while (0)
     MAF_CT_SWITCH(LC, X)
 #undef X
@@ -715,9 +817,14 @@ bool ct_cols(const cplx_t<R>* in, cplx_t<R>* out, int L, int n_in, int n_out, in
     // (truncated output); the tensor's full transforms (FP64) run unpruned
     const bool hin = 2 * n_in <= L, hout = 2 * n_out <= L;
     if (hin && hout) return false;
+    // the kernels read exactly L/2 (pruned) or L rows and write L/2 or L
+    if ((hin ? 2 * n_in : n_in) != L || (hout ? 2 * n_out : n_out) != L) return false;
+    // the row stride bounds the column tiles the pipelined kernel copies whole
+    const int pitch = (int)std::min<int64_t>(in_si, 1 << 30);
     if (!hin && !hout && !f64) return false;
-#define C2(N, T, HI, HO) \
-    cols_L<R, DIR, N, T, HI, HO>(in, out, n_in, n_out, ncols, in_si, out_si, in_sbat, out_sbat, nbat, tw.get(N, f64), st)
+#define C2(N, T, HI, HO)                                                                                   \
+    cols_L<R, DIR, N, T, HI, HO>(in, out, n_in, n_out, ncols, in_si, out_si, in_sbat, out_sbat, nbat,        \
+                                 ct_tw<N>(tw, f64), tc.cols_pipe, pitch, st)
 #define C1(N, T)                                                \
     do {                                                        \
         if (hin)                                                \
@@ -748,9 +855,9 @@ bool ct_convz(cplx_t<R>* S, const R* Nred, int nz, int ny, int nxh, int pitch, T
 #define X(N)                                                                 \
     do {                                                                     \
         if (tc.convz_reg)                                                    \
-            convz_L<R, N, true>(S, Nred, nz, ny, nxh, pitch, tw.get(N, f64), st);  \
+            convz_L<R, N, true>(S, Nred, nz, ny, nxh, pitch, ct_tw<N>(tw, f64), st);  \
         else                                                                 \
-            convz_L<R, N, false>(S, Nred, nz, ny, nxh, pitch, tw.get(N, f64), st); \
+            convz_L<R, N, false>(S, Nred, nz, ny, nxh, pitch, ct_tw<N>(tw, f64), st); \
     } while (0)
     switch (L) {
         case 8: X(8); return true;
@@ -766,7 +873,7 @@ template <typename R>
 bool ct_convy(cplx_t<R>* S, const R* Nred, int ny, int nxh, int pitch, Twiddles& tw, cudaStream_t st) {
     const bool f64 = sizeof(R) == 8;
     const int L = 2 * ny;
-#define X(N) convy_L<R, N>(S, Nred, ny, nxh, pitch, tw.get(N, f64), st)
+#define X(N) convy_L<R, N>(S, Nred, ny, nxh, pitch, ct_tw<N>(tw, f64), st)
     switch (L) {
         case 16: X(16); return true;
         case 32: X(32); return true;
@@ -792,9 +899,9 @@ bool ct_xinv(const cplx_t<R>* S1, int pitch, int Px, Twiddles& tw, const Geom& g
 #define X(N)                                                                                                    \
     do {                                                                                                        \
         if (run == 4)                                                                                           \
-            xinv_L<R, N, 4>(S1, pitch, tw.get(N, f64), tw.get(Px, f64), g, scale, m, ms, tl, ep, st, nblocks);  \
+            xinv_L<R, N, 4>(S1, pitch, ct_tw<N>(tw, f64), tw.get(Px, f64), g, scale, m, ms, tl, ep, st, nblocks);  \
         else                                                                                                    \
-            xinv_L<R, N, 2>(S1, pitch, tw.get(N, f64), tw.get(Px, f64), g, scale, m, ms, tl, ep, st, nblocks);  \
+            xinv_L<R, N, 2>(S1, pitch, ct_tw<N>(tw, f64), tw.get(Px, f64), g, scale, m, ms, tl, ep, st, nblocks);  \
     } while (0)
     switch (LC) {
         case 16: X(16); return true;

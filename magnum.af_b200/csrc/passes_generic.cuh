@@ -7,6 +7,25 @@
 
 namespace mafb {
 
+// Launch shapes of the generic passes (host).
+inline int round_threads(int t) {
+    t = t > 32 ? t : 32;
+    t = (t + 31) / 32 * 32;
+    if (t > kMaxFftThreads) throw Error(6, "FFT tile needs more threads than one CTA has (transform length too large)");
+    return t;
+}
+
+// columns per tile so that the tile holds about `target` complex values
+inline int pick_nb(int L, int target, int ncols, int nbmax) {
+    int nb = target / (L > 1 ? L : 1);
+    nb = nb > 1 ? nb : 1;
+    nb = nb < nbmax ? nb : nbmax;
+    const int nc = ncols > 1 ? ncols : 1;
+    return nb < nc ? nb : nc;
+}
+
+template <typename R> inline int tile_target() { return sizeof(R) == 4 ? 8192 : 4096; }
+
 // x-forward: rows of n_in reals (times Ms) zero-padded to Px = 2*Lc, real FFT by
 // packing even/odd samples into Lc complex values; writes kx in [0, Lc].
 // Tile `tile` (rows [tile*nb, tile*nb + nb)) of the pass; the plan may sit in

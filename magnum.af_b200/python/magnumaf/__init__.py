@@ -133,6 +133,9 @@ _SIGS = {
     "maf_stoch_batch_create": (_I, [C.POINTER(_P), C.POINTER(_P), C.POINTER(_P), _I]),
     "maf_stoch_batch_destroy": (_I, [_P]),
     "maf_stoch_batch_steps": (_I, [_P, _I]),
+    "maf_stoch_batch_set_fused": (_I, [_P, _I]),
+    "maf_stoch_batch_is_fused": (_I, [_P, C.POINTER(_I)]),
+    "maf_term_demag_set_generic": (_I, [_P, _I]),
     "maf_string_create": (_I, [C.POINTER(_P), _P, C.POINTER(_P), _I, _I, _D, _P]),
     "maf_string_destroy": (_I, [_P]),
     "maf_string_step": (_I, [_P]),
@@ -476,6 +479,16 @@ class DemagField(FieldTerm):
     def tune(self, choices):
         ch = (_I * 3)(*[int(c) for c in choices])
         _ck(lib.maf_term_demag_set_tune(self._h, ch))
+
+    @property
+    def generic(self) -> bool:
+        return bool(getattr(self, "_generic", False))
+
+    @generic.setter
+    def generic(self, on):
+        """Run every pass with the run-time-plan kernels (those of the batched passes)."""
+        _ck(lib.maf_term_demag_set_generic(self._h, int(bool(on))))
+        self._generic = bool(on)
 
     def get_N(self, symmetric=False) -> np.ndarray:
         """Real-space Newell tensor [Px, Py, Pz, 6] (the reference's setup_N layout);
@@ -894,14 +907,28 @@ class ConvNet:
 class StochasticBatch:
     """Members (Stochastic_LLG, State) advanced together: after one eager step,
     pairs of steps of every member replay one captured CUDA graph with each member
-    on its own stream.  Bit-identical to stepping the members one by one."""
+    on its own stream.  Bit-identical to stepping the members one by one.
 
-    def __init__(self, members):
+    fused=True: every pass of a step is one launch for all members (a device
+    work table of (member, tile) pairs over the run-time-plan kernels) when every
+    member is a 2-D mesh with one DemagField and scalar parameters; bit-identical
+    to the members stepped one by one with DemagField.generic = True."""
+
+    def __init__(self, members, fused=False):
         self._members = list(members)
         its = (_P * len(self._members))(*[it._h for it, _ in self._members])
         sts = (_P * len(self._members))(*[st._h for _, st in self._members])
         self._h = _P()
         _ck(lib.maf_stoch_batch_create(C.byref(self._h), its, sts, len(self._members)))
+        if fused:
+            _ck(lib.maf_stoch_batch_set_fused(self._h, 1))
+
+    @property
+    def fused_active(self) -> bool:
+        """Whether the captured graph runs the batched passes."""
+        v = _I()
+        _ck(lib.maf_stoch_batch_is_fused(self._h, C.byref(v)))
+        return bool(v.value)
 
     def __del__(self):
         if getattr(self, "_h", None):
