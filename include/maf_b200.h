@@ -349,6 +349,13 @@ int maf_string_image(maf_string h, int i, maf_state* image);
  * array arguments are DEVICE pointers, NCHW: x [B][cin][H][W], y and target
  * [B][3][H][W].  Parameters: per layer W[cout][cin][3][3] then b[cout]. */
 typedef struct maf_cnn_s* maf_cnn;
+/* BF16 GEMM on the tensor cores (tcgen05.mma, FP32 accumulation in tensor memory), the contraction of
+ * the warm-start network's convolutions (no counterpart in the reference): C[M][N] (FP32, row stride ldc)
+ * = A[M][K] . B[N][K]^T with A, B BF16 device arrays whose K elements are contiguous (row strides lda,
+ * ldb and K multiples of 8, rows 16-byte aligned).  Queued on stream (NULL: the legacy default stream);
+ * returns after the stream finished it.  MAF_ERR_TIMEOUT if a bounded tensor-core wait gave up. */
+int maf_bf16_gemm(const void* A_dev, int lda, const void* B_dev, int ldb, float* C_dev, int ldc, int M, int N, int K,
+                  void* stream);
 int maf_cnn_create(maf_cnn* out, int cin, int width, int depth, unsigned long long seed);
 int maf_cnn_destroy(maf_cnn h);
 /* dilation of each layer's 3x3 kernel (n = depth values in 1..64; default 1): layer l reads its input at

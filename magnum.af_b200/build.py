@@ -36,6 +36,7 @@ SOURCES = {
     "noalloc.o": ("noalloc.cu", []),
     "cnn.o": ("cnn.cu", []),
     "batch.o": ("batch.cu", []),
+    "umma.o": ("umma.cu", []),
 }
 for _part in (1, 2, 3):
     for _real in (4, 8):

@@ -134,6 +134,7 @@ _SIGS = {
     "maf_stoch_batch_destroy": (_I, [_P]),
     "maf_stoch_batch_steps": (_I, [_P, _I]),
     "maf_stoch_batch_set_fused": (_I, [_P, _I]),
+    "maf_bf16_gemm": (_I, [_P, _I, _P, _I, _P, _I, _I, _I, _I, _P]),
     "maf_stoch_batch_is_fused": (_I, [_P, C.POINTER(_I)]),
     "maf_term_demag_set_generic": (_I, [_P, _I]),
     "maf_string_create": (_I, [C.POINTER(_P), _P, C.POINTER(_P), _I, _I, _D, _P]),
