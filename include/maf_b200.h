@@ -356,6 +356,50 @@ typedef struct maf_cnn_s* maf_cnn;
  * returns after the stream finished it.  MAF_ERR_TIMEOUT if a bounded tensor-core wait gave up. */
 int maf_bf16_gemm(const void* A_dev, int lda, const void* B_dev, int ldb, float* C_dev, int ldc, int M, int N, int K,
                   void* stream);
+/* Layer kernels of the warm-start U-net (magnumaf/unet.py; no counterpart in the reference).  Device
+ * pointers; activations pixel-major ([pixels][channels], pixel (b, y, x) at row (b H + y) W + x); BF16
+ * tensors that feed a GEMM have their channels padded with zeros to Cp, a multiple of 8; every call is
+ * queued on stream st (NULL: the legacy default stream) and returns without synchronising. */
+/* x [B][C][H][W] FP32 -> act [P][Cp] BF16 and m [P][3] FP32 (channels 0..2) */
+int maf_nn_input(const float* x, int B, int C, int H, int W, int Cp, void* act_bf16, float* m, void* st);
+/* 3x3 im2col (zero padding): col [P][9 Cp] (tap t = 3 (dy + 1) + (dx + 1)), or colT [9 Cp][P] */
+int maf_nn_im2col(const void* act, int B, int H, int W, int Cp, void* col, int transposed, void* st);
+/* maf_bf16_gemm without the synchronisation, and with the K range split over `splits` partial slabs
+ * work [splits][M][N] summed in split order into C [M][N] */
+int maf_nn_gemm(const void* A, int lda, const void* B, int ldb, float* C, int ldc, int M, int N, int K, void* st);
+int maf_nn_gemm_splitk(const void* A, int lda, const void* B, int ldb, float* C, int M, int N, int K, int splits,
+                       float* work, void* st);
+/* out [P][C] = relu?(y + bias) (FP32) and, when outb, its BF16 copy [P][Cp] */
+int maf_nn_bias_act(const float* y, int ldy, const float* bias, long long P, int C, int relu, float* out,
+                    void* outb, int Cp, void* st);
+/* 2x2 average pooling [B][H][W][C] -> [B][H/2][W/2][C] (FP32 and BF16 [.][Cp]) and its backward
+ * (din (+)= dout / 4 at the four children) */
+int maf_nn_pool(const float* in, int B, int H, int W, int C, float* out, void* outb, int Cp, void* st);
+int maf_nn_pool_bwd(const float* dout, int B, int H, int W, int C, float* din, int accumulate, void* st);
+/* out [B][H][W][Cp] BF16 = nearest-2x-upsampled a [B][H/2][W/2][Ca] | s [B][H][W][Cs]; backward:
+ * da = sum of the four children of the first Ca channels of dcat [P][Cp], ds += the next Cs */
+int maf_nn_up_cat(const float* a, int Ca, const float* s, int Cs, int B, int H, int W, void* out, int Cp, void* st);
+int maf_nn_up_cat_bwd(const float* dcat, int Cp, int Ca, int Cs, int B, int H, int W, float* da, float* ds,
+                      void* st);
+/* dY = dA * relu'(A) (FP32 [P][C], and BF16 [P][Cp]) */
+int maf_nn_relu_bwd(const float* dA, const float* A, long long P, int C, int relu, float* dY, void* dYb, int Cp,
+                    void* st);
+/* BF16 [R][C] -> [C][R] */
+int maf_nn_transpose(const void* in, long long R, int C, void* out, void* st);
+/* adjoint of im2col: dX [P][C] (+)= sum over taps of dcol [P][9 Cp] (first C channels) */
+int maf_nn_col2im(const float* dcol, int B, int H, int W, int Cp, int C, float* dX, int accumulate, void* st);
+/* db [C] = sum over pixels of dY [P][C] (fixed order) */
+int maf_nn_colsum(const float* dY, long long P, int C, float* db, void* st);
+/* FP32 weights W [Cout][9][Cin] -> BF16 Wb [Cout][9 Cp] and WtB [9 Cp][CoutP] (zero padded); the
+ * weight gradient [Cout][9][Cin] from a GEMM result [Cout][9 Cp] */
+int maf_nn_wcast(const float* W32, int Cout, int Cin, int Cp, int CoutP, void* Wb, void* WtB, void* st);
+int maf_nn_wgrad(const float* g, int Cout, int Cin, int Cp, float* dW, void* st);
+/* y = normalize(m + d) [P][3]; with a target t: per-pixel |y - t|^2, its mean in *loss (device) and
+ * dL/dd [P][3] in gd */
+int maf_nn_head(const float* m, const float* d, int ldd, const float* t, long long P, float* y, float* gd,
+                float* cell_loss, float* loss, void* st);
+/* one Adam step (beta 0.9 / 0.999, eps 1e-8), step = the 1-based step count for the bias corrections */
+int maf_nn_adam(float* w, const float* g, float* m1, float* m2, long long n, float lr, int step, void* st);
 int maf_cnn_create(maf_cnn* out, int cin, int width, int depth, unsigned long long seed);
 int maf_cnn_destroy(maf_cnn h);
 /* dilation of each layer's 3x3 kernel (n = depth values in 1..64; default 1): layer l reads its input at

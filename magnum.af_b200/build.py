@@ -37,6 +37,7 @@ SOURCES = {
     "cnn.o": ("cnn.cu", []),
     "batch.o": ("batch.cu", []),
     "umma.o": ("umma.cu", []),
+    "nn.o": ("nn.cu", []),
 }
 for _part in (1, 2, 3):
     for _real in (4, 8):

@@ -61,10 +61,12 @@ __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t phase) {
     }
 }
 
+// blockIdx.z = split s of the K range (kchunk values each, a multiple of 64):
+// its partial product goes to the slab C + s M ldc.
 template <int BN>
 __global__ void __launch_bounds__(128) k_umma_gemm(const __nv_bfloat16* __restrict__ A, int lda,
                                                    const __nv_bfloat16* __restrict__ B, int ldb, float* __restrict__ C,
-                                                   int ldc, int M, int N, int K, int* err) {
+                                                   int ldc, int M, int N, int K, int kchunk, int* err) {
     static_assert(BN == 32 || BN == 64 || BN == 128 || BN == 256, "tile width");
     constexpr uint32_t A_KC = (kBM / 8) * 128;  // bytes between the K chunks of the A tile (LBO)
     constexpr uint32_t B_KC = (BN / 8) * 128;   // of the B tile
@@ -92,14 +94,17 @@ __global__ void __launch_bounds__(128) k_umma_gemm(const __nv_bfloat16* __restri
     const uint32_t tmem = tmem_sh;
     uint32_t phase = 0;
     const uint32_t sa = smem_u32(sA), sb = smem_u32(sB);
-    for (int k0 = 0; k0 < K; k0 += kBK) {
+    const int kbeg = blockIdx.z * kchunk;
+    const int kend = min(K, kbeg + kchunk);
+    C += (int64_t)blockIdx.z * M * ldc;
+    for (int k0 = kbeg; k0 < kend; k0 += kBK) {
         // A tile: 128 rows x 8 chunks of 8 BF16 (16 bytes); thread q takes chunk (q & 7) of row q >> 3
 #pragma unroll
         for (int i = 0; i < 8; ++i) {
             const int q = tid + 128 * i, r = q >> 3, kc = q & 7;
             const int gm = m0 + r, gk = k0 + kc * 8;
             uint4 v = make_uint4(0, 0, 0, 0);
-            if (gm < M && gk < K) v = *reinterpret_cast<const uint4*>(A + (int64_t)gm * lda + gk);
+            if (gm < M && gk < kend) v = *reinterpret_cast<const uint4*>(A + (int64_t)gm * lda + gk);
             *reinterpret_cast<uint4*>(sA + kc * A_KC + (r >> 3) * 128 + (r & 7) * 16) = v;
         }
 #pragma unroll
@@ -107,7 +112,7 @@ __global__ void __launch_bounds__(128) k_umma_gemm(const __nv_bfloat16* __restri
             const int q = tid + 128 * i, r = q >> 3, kc = q & 7;
             const int gn = n0 + r, gk = k0 + kc * 8;
             uint4 v = make_uint4(0, 0, 0, 0);
-            if (gn < N && gk < K) v = *reinterpret_cast<const uint4*>(B + (int64_t)gn * ldb + gk);
+            if (gn < N && gk < kend) v = *reinterpret_cast<const uint4*>(B + (int64_t)gn * ldb + gk);
             *reinterpret_cast<uint4*>(sB + kc * B_KC + (r >> 3) * 128 + (r & 7) * 16) = v;
         }
         // the tiles were written through the generic proxy; the MMA reads them through the async proxy
@@ -119,7 +124,7 @@ __global__ void __launch_bounds__(128) k_umma_gemm(const __nv_bfloat16* __restri
             for (int s = 0; s < kBK / 16; ++s) {
                 const uint64_t ad = sdesc(sa + 2 * s * A_KC, A_KC, 128);
                 const uint64_t bd = sdesc(sb + 2 * s * B_KC, B_KC, 128);
-                const uint32_t acc = (k0 > 0 || s > 0) ? 1u : 0u;
+                const uint32_t acc = (k0 > kbeg || s > 0) ? 1u : 0u;
                 asm volatile(
                     "{\n\t.reg .pred p;\n\t"
                     "setp.ne.b32 p, %4, 0;\n\t"
@@ -170,10 +175,15 @@ DevBuf g_umma_err;  // device error flag of the tensor-core GEMM (one per proces
 
 }  // namespace
 
-// Host launcher (cnn.cu and the C ABI): the tile width follows N.
+// Host launcher (nn.cu and the C ABI): the tile width follows N; with splits > 1
+// the K range is cut into that many chunks whose partial products land in
+// consecutive slabs C + s M ldc (the caller sums them).
 void umma_gemm(const void* A, int lda, const void* B, int ldb, float* C, int ldc, int M, int N, int K,
-               cudaStream_t st, bool check) {
+               cudaStream_t st, bool check, int splits = 1) {
     if (M <= 0 || N <= 0 || K <= 0) return;
+    if (splits < 1) splits = 1;
+    const int kchunk = (int)ceil_div(ceil_div(K, splits), kBK) * kBK;
+    splits = (int)ceil_div(K, kchunk);
     if (K % 8 || lda % 8 || ldb % 8 || lda < K || ldb < K || ldc < N || ((uintptr_t)A | (uintptr_t)B) % 16)
         throw Error(1, "bf16 gemm: K and the row strides must be multiples of 8 elements, rows 16-byte aligned");
     if (!g_umma_err.p) {
@@ -184,12 +194,14 @@ void umma_gemm(const void* A, int lda, const void* B, int ldb, float* C, int ldc
     const auto* a = static_cast<const __nv_bfloat16*>(A);
     const auto* b = static_cast<const __nv_bfloat16*>(B);
     const unsigned gx = (unsigned)ceil_div(M, kBM);
+    const unsigned gz = (unsigned)splits;
     if (N <= 32) {
-        k_umma_gemm<32><<<dim3(gx, 1), 128, 0, st>>>(a, lda, b, ldb, C, ldc, M, N, K, err);
+        k_umma_gemm<32><<<dim3(gx, 1, gz), 128, 0, st>>>(a, lda, b, ldb, C, ldc, M, N, K, kchunk, err);
     } else if (N <= 64) {
-        k_umma_gemm<64><<<dim3(gx, 1), 128, 0, st>>>(a, lda, b, ldb, C, ldc, M, N, K, err);
+        k_umma_gemm<64><<<dim3(gx, 1, gz), 128, 0, st>>>(a, lda, b, ldb, C, ldc, M, N, K, kchunk, err);
     } else {
-        k_umma_gemm<128><<<dim3(gx, (unsigned)ceil_div(N, 128)), 128, 0, st>>>(a, lda, b, ldb, C, ldc, M, N, K, err);
+        k_umma_gemm<128><<<dim3(gx, (unsigned)ceil_div(N, 128), gz), 128, 0, st>>>(a, lda, b, ldb, C, ldc, M, N, K,
+                                                                                    kchunk, err);
     }
     MAF_LAUNCH_CHECK();
     if (check) {

@@ -135,6 +135,24 @@ _SIGS = {
     "maf_stoch_batch_steps": (_I, [_P, _I]),
     "maf_stoch_batch_set_fused": (_I, [_P, _I]),
     "maf_bf16_gemm": (_I, [_P, _I, _P, _I, _P, _I, _I, _I, _I, _P]),
+    # layer kernels of the warm-start U-net (magnumaf.unet)
+    "maf_nn_input": (_I, [_P, _I, _I, _I, _I, _I, _P, _P, _P]),
+    "maf_nn_im2col": (_I, [_P, _I, _I, _I, _I, _P, _I, _P]),
+    "maf_nn_gemm": (_I, [_P, _I, _P, _I, _P, _I, _I, _I, _I, _P]),
+    "maf_nn_gemm_splitk": (_I, [_P, _I, _P, _I, _P, _I, _I, _I, _I, _P, _P]),
+    "maf_nn_bias_act": (_I, [_P, _I, _P, C.c_longlong, _I, _I, _P, _P, _I, _P]),
+    "maf_nn_pool": (_I, [_P, _I, _I, _I, _I, _P, _P, _I, _P]),
+    "maf_nn_pool_bwd": (_I, [_P, _I, _I, _I, _I, _P, _I, _P]),
+    "maf_nn_up_cat": (_I, [_P, _I, _P, _I, _I, _I, _I, _P, _I, _P]),
+    "maf_nn_up_cat_bwd": (_I, [_P, _I, _I, _I, _I, _I, _I, _P, _P, _P]),
+    "maf_nn_relu_bwd": (_I, [_P, _P, C.c_longlong, _I, _I, _P, _P, _I, _P]),
+    "maf_nn_transpose": (_I, [_P, C.c_longlong, _I, _P, _P]),
+    "maf_nn_col2im": (_I, [_P, _I, _I, _I, _I, _I, _P, _I, _P]),
+    "maf_nn_colsum": (_I, [_P, C.c_longlong, _I, _P, _P]),
+    "maf_nn_wcast": (_I, [_P, _I, _I, _I, _I, _P, _P, _P]),
+    "maf_nn_wgrad": (_I, [_P, _I, _I, _I, _P, _P]),
+    "maf_nn_head": (_I, [_P, _P, _I, _P, C.c_longlong, _P, _P, _P, _P, _P]),
+    "maf_nn_adam": (_I, [_P, _P, _P, _P, C.c_longlong, C.c_float, _I, _P]),
     "maf_stoch_batch_is_fused": (_I, [_P, C.POINTER(_I)]),
     "maf_term_demag_set_generic": (_I, [_P, _I]),
     "maf_string_create": (_I, [C.POINTER(_P), _P, C.POINTER(_P), _I, _I, _D, _P]),
