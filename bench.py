@@ -458,6 +458,45 @@ def other_configs(M, stream):
     return out
 
 
+def kernel_sweep(args):
+    """--kernel-sweep: a few launches of every kernel family of the path on the
+    --mesh mesh, for profiler captures (nothing is timed or printed but a
+    summary line): the field passes in both forms, the local terms alone, one
+    DP45 attempt per form (combine, finalize, FP32 copy of m), two Heun steps of
+    a 2-D film and a few LBFGS iterations (its vector kernels and energy
+    partials) on a 128 x 128 film."""
+    import torch
+
+    import magnumaf as M
+
+    mesh = M.Mesh(NX, NY, NZ, DX, DX, DX)
+    m, h_ext = workload()
+    terms = [M.DemagField(mesh), M.ExchangeField(A_EX), M.CubicAnisotropyField(K1), M.ExternalField.uniform(*h_ext)]
+    llg = M.LLGIntegrator(0.01, terms, "DP45")
+    loc = M.LLGIntegrator(0.01, terms[1:], "DP45")
+    for prec in ("fp32_field", "fp64"):
+        st = M.State(mesh, MS, m, precision=prec)
+        llg.H_in_Apm_f32(st) if prec == "fp32_field" else llg.H_in_Apm(st)
+        loc.H_in_Apm_f32(st) if prec == "fp32_field" else loc.H_in_Apm(st)
+        llg.attempt_profile(st, 1e-14)
+        del st
+    film = M.Mesh(256, 256, 1, 2e-9, 2e-9, 1e-9)
+    fst = M.State(film, 1.1e6, np.broadcast_to(np.array([0.0, 0.0, 1.0]), (256, 256, 1, 3)).copy(),
+                  precision="fp32_field")
+    heun = M.Stochastic_LLG(0.1, 300.0, 5e-15, fst, [M.DemagField(film), M.ExchangeField(1.6e-11),
+                                                        M.UniaxialAnisotropyField(1e6)], "Heun", seed=1)
+    heun.steps(fst, 2)
+    small = M.Mesh(128, 128, 1, 2e-9, 2e-9, 2e-9)
+    rng = np.random.default_rng(5)
+    ms = rng.normal(size=(128, 128, 1, 3))
+    sst = M.State(small, 8e5, ms / np.linalg.norm(ms, axis=3, keepdims=True))
+    mini = M.LBFGS_Minimizer([M.ExchangeField(1.3e-11), M.DmiField(3e-3), M.UniaxialAnisotropyField(8e5)], tol=1e-6,
+                             maxiter=5)
+    mini.minimize(sst)
+    torch.cuda.synchronize()
+    print(json.dumps({"kernel_sweep": "%dx%dx%d" % (NX, NY, NZ)}), flush=True)
+
+
 def run_ours(args):
     import ctypes as C
 
@@ -525,7 +564,7 @@ def run_ours(args):
 
     tune = None
     if not args.no_autotune:  # kernel variants per pass, measured on this mesh (FP32-field form)
-        tune = llg.autotune(s32, reps=3)
+        tune = llg.autotune_ex(s32, reps=3)
 
     f32 = lambda: llg.heff_device(s32, m32_dev.data_ptr(), H32.data_ptr())
     f64 = lambda: llg.heff_device(s64, m64_dev.data_ptr(), H64.data_ptr())
@@ -592,6 +631,15 @@ def run_ours(args):
         cfgs["heun_ensemble_64"] = heun_ensemble(M, args.heun_steps)
         # the same with 64 small members (64 x 64): launch-bound, where one launch per pass pays
         cfgs["heun_ensemble_64_small"] = heun_ensemble(M, args.heun_steps, shapes=[(64, 64)] * 64)
+    if not args.no_trajectory and args.warm_start_samples > 0:
+        # the learned warm start: plain against warm-started LBFGS on fresh samples of the
+        # 128 x 128 configuration with the pretrained U-net (seeds never used in training)
+        from magnumaf import warmstart as WS
+
+        ws = WS.gain(WS.pretrained_unet(), args.warm_start_samples, 128, 128, seed=30_000)
+        ws["config"] = ("128x128x1 cells of 2 nm, exchange + interface DMI + uniaxial + z field, parameters uniform "
+                        "per sample, initial m random on the sphere per cell; LBFGS tol 1e-6, maxiter 2000")
+        cfgs["warm_start_128"] = ws
 
     # per-pass timing (CUDA events between the pass kernels on the launching stream)
     passes = {}
@@ -698,7 +746,8 @@ def run_ours(args):
                                % (NX, NY, NZ),
                    "cells": NX * NY * NZ, "parallelism": "replicas x%d" % world,
                    "l2": "inputs larger than L2 (m 201 MB, spectra 403-806 MB per pass)",
-                   "tune": None if tune is None else {k: tune[k] for k in ("cols_wide", "convz_reg", "xinv_run")}},
+                   "tune": None if tune is None else {k: tune[k] for k in ("cols_wide", "convz_reg", "xinv_run",
+                                                                          "cols_pipe", "cols_plan")}},
         "fp64_form": {"value": world * args.steps / (ms64 * 1e-3), "ms_per_step": ms64 / args.steps,
                       "fp32_speedup": ms64 / ms32},
         "rel_err_fp32_vs_fp64": {"l2": rel_err, "max": rel_max, "per_term": per_term},
@@ -775,6 +824,9 @@ def main():
     ap.add_argument("--no-autotune", action="store_true", help="keep the default kernel variants")
     ap.add_argument("--rk-steps", type=int, default=300, help="DP45 steps of the plain step loop per form")
     ap.add_argument("--heun-steps", type=int, default=1000, help="steps of the 64-member Heun ensemble")
+    ap.add_argument("--warm-start-samples", type=int, default=16, help="held-out samples of the warm-start gain")
+    ap.add_argument("--kernel-sweep", action="store_true",
+                    help="launch every kernel family once or twice (for profiler captures) and exit")
     ap.add_argument("--mesh", type=int, nargs=3, default=None, metavar=("NX", "NY", "NZ"),
                     help="smaller mesh for profiling captures (the reported metric is defined at 1024 1024 16)")
     args = ap.parse_args()
@@ -783,6 +835,8 @@ def main():
         NX, NY, NZ = args.mesh
     if args.impl == "reference":
         run_reference(args)
+    elif args.kernel_sweep:
+        kernel_sweep(args)
     else:
         run_ours(args)
 

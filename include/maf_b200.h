@@ -201,6 +201,15 @@ int maf_llg_heff_pipeline_m32(maf_llg l, maf_state s, const float* const* m_host
  * values) receives the per-pass times of the two configurations.  Every variant computes the same field
  * up to rounding. */
 int maf_llg_autotune(maf_llg l, maf_state s, int reps, int choices[3], double* pass_ms);
+/* The autotuner's full search: four configurations of the passes are timed (defaults; all alternatives;
+ * and two mixed ones), and the y passes' column tile, pipelining and radix sequence (16 16 R or 16 R 16)
+ * are chosen jointly, the z convolution and the x-inverse run length per pass.  choices[5] = {cols_wide,
+ * convz_reg, xinv_run, cols_pipe, cols_plan}; pass_ms (optional) receives 4 x 5 per-pass times; the
+ * result is cached per (mesh, precision, term kinds) for the process, and *cached (optional) reports a
+ * cache hit (no timing then). */
+int maf_llg_autotune_ex(maf_llg l, maf_state s, int reps, int choices[5], double* pass_ms, int* cached);
+int maf_term_demag_get_tune_ex(maf_term t, int choices[5]);
+int maf_term_demag_set_tune_ex(maf_term t, const int choices[5]);
 int maf_term_demag_get_tune(maf_term t, int choices[3]);
 int maf_term_demag_set_tune(maf_term t, const int choices[3]);
 /* Runs every pass of this DemagField with the run-time-plan kernels (the ones the batched passes of

@@ -6,7 +6,9 @@
 #include <fstream>
 #include <iomanip>
 #include <limits>
+#include <map>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1565,7 +1567,26 @@ int maf_llg_heff_device_profile(maf_llg l, maf_state s, const void* m_dev, void*
 // Autotuner: times both kernel configurations of every tunable pass on this
 // state's mesh and precision (one warm-up, then the mean of `reps` evaluations
 // with CUDA events between the passes) and keeps the faster variant per pass.
-int maf_llg_autotune(maf_llg l, maf_state s, int reps, int choices[3], double* pass_ms) {
+// Autotuner: times four kernel configurations of the demag passes on this
+// state's mesh and precision (one warm-up, then the mean of `reps` evaluations
+// with CUDA events between the passes) and keeps the fastest variant per pass:
+// y passes (column tile x pipelining x radix sequence, chosen jointly since the
+// two passes share the tile and the plan), z convolution, x-inverse epilogue run.
+// The choices are cached per (mesh, precision, term kinds) for the process.
+namespace {
+std::mutex g_tune_mu;
+std::map<std::string, TuneChoice> g_tune_cache;
+
+std::string tune_key(const maf_llg_s* l, const StateD& st) {
+    std::string k = std::to_string(st.md.nx) + "," + std::to_string(st.md.ny) + "," + std::to_string(st.md.nz) + "," +
+                    std::to_string(st.md.dx) + "," + std::to_string(st.md.dy) + "," + std::to_string(st.md.dz) +
+                    "," + std::to_string(st.precision) + ",";
+    for (auto& t : l->terms) k += std::to_string(t->kind) + ":";
+    return k;
+}
+}  // namespace
+
+int maf_llg_autotune_ex(maf_llg l, maf_state s, int reps, int choices[5], double* pass_ms, int* cached) {
     return guarded([&] {
         check_llg_state(l, s);
         check(choices && reps > 0, "maf_llg_autotune: bad argument");
@@ -1573,57 +1594,133 @@ int maf_llg_autotune(maf_llg l, maf_state s, int reps, int choices[3], double* p
         for (auto& t : l->terms)
             if (t->kind == TK_DEMAG && !t->demag_pbc()) dm = t->demag.get();  // the periodic form has no variants
         TuneChoice best;
+        if (cached) *cached = 0;
         if (dm) {
             StateD& st = s->s;
-            const bool f32 = st.precision == PREC_FP32_FIELD;
-            const int64_t n3 = 3 * st.md.N();
-            g_tmp.ensure((f32 ? sizeof(float) : sizeof(double)) * n3);
-            if (f32) ensure_m32(s);
-            const auto terms = raw_terms(l->terms);
-            auto run = [&](const TuneChoice& c) {
-                dm->tune = c;
-                std::vector<double> acc;
-                for (int r = -1; r < reps; ++r) {  // r = -1: warm-up
-                    EpilogueArgs ep;
-                    ep.kind = EPI_H;
-                    ep.out = g_tmp.p;
-                    PassMarks marks;
-                    if (f32)
-                        eval_terms<float>(terms, st.md, st.m32.as<float>(), st.msinfo(), ep, st.stream, s->scratch,
-                                          nullptr, &marks);
-                    else
-                        eval_terms<double>(terms, st.md, st.m64.as<double>(), st.msinfo(), ep, st.stream, s->scratch,
-                                           nullptr, &marks);
-                    MAF_CUDA(cudaStreamSynchronize(st.stream));
-                    if (r < 0) continue;
-                    acc.resize(marks.ev.size() - 1, 0.0);
-                    for (size_t i = 1; i < marks.ev.size(); ++i) {
-                        float ms = 0;
-                        MAF_CUDA(cudaEventElapsedTime(&ms, marks.ev[i - 1], marks.ev[i]));
-                        acc[i - 1] += ms / reps;
-                    }
+            const std::string key = tune_key(l, st);
+            bool hit = false;
+            {
+                std::lock_guard<std::mutex> lock(g_tune_mu);
+                auto it = g_tune_cache.find(key);
+                if (it != g_tune_cache.end()) {
+                    best = it->second;
+                    best.generic = dm->tune.generic;
+                    dm->tune = best;
+                    hit = true;
                 }
-                return acc;
-            };
-            const TuneChoice A{0, 1, 2}, B{1, 0, 4};
-            const std::vector<double> ta = run(A), tb = run(B);
-            if (st.md.nz > 1 && ta.size() == 5 && tb.size() == 5) {
-                best.cols_wide = tb[1] + tb[3] < ta[1] + ta[3] ? 1 : 0;
-                best.convz_reg = ta[2] <= tb[2] ? 1 : 0;
-                best.xinv_run = ta[4] <= tb[4] ? 2 : 4;
-            } else if (ta.size() == 3 && tb.size() == 3) {
-                best.xinv_run = ta[2] <= tb[2] ? 2 : 4;
             }
-            dm->tune = best;
-            if (pass_ms)
-                for (size_t i = 0; i < 5; ++i) {
-                    pass_ms[i] = i < ta.size() ? ta[i] : 0.0;
-                    pass_ms[5 + i] = i < tb.size() ? tb[i] : 0.0;
+            if (cached) *cached = hit ? 1 : 0;
+            if (!hit) {
+                const bool f32 = st.precision == PREC_FP32_FIELD;
+                const int64_t n3 = 3 * st.md.N();
+                g_tmp.ensure((f32 ? sizeof(float) : sizeof(double)) * n3);
+                if (f32) ensure_m32(s);
+                const auto terms = raw_terms(l->terms);
+                const int generic = dm->tune.generic;
+                auto run = [&](TuneChoice c) {
+                    c.generic = generic;
+                    dm->tune = c;
+                    std::vector<double> acc;
+                    for (int r = -1; r < reps; ++r) {  // r = -1: warm-up
+                        EpilogueArgs ep;
+                        ep.kind = EPI_H;
+                        ep.out = g_tmp.p;
+                        PassMarks marks;
+                        if (f32)
+                            eval_terms<float>(terms, st.md, st.m32.as<float>(), st.msinfo(), ep, st.stream, s->scratch,
+                                              nullptr, &marks);
+                        else
+                            eval_terms<double>(terms, st.md, st.m64.as<double>(), st.msinfo(), ep, st.stream,
+                                               s->scratch, nullptr, &marks);
+                        MAF_CUDA(cudaStreamSynchronize(st.stream));
+                        if (r < 0) continue;
+                        acc.resize(marks.ev.size() - 1, 0.0);
+                        for (size_t i = 1; i < marks.ev.size(); ++i) {
+                            float ms = 0;
+                            MAF_CUDA(cudaEventElapsedTime(&ms, marks.ev[i - 1], marks.ev[i]));
+                            acc[i - 1] += ms / reps;
+                        }
+                    }
+                    return acc;
+                };
+                //                    wide reg run pipe plan
+                const TuneChoice cfg[4] = {{0, 1, 2, 1, 0}, {1, 0, 4, 0, 1}, {0, 1, 2, 0, 1}, {1, 0, 4, 1, 0}};
+                std::vector<double> t[4];
+                for (int c = 0; c < 4; ++c) t[c] = run(cfg[c]);
+                best = cfg[0];
+                if (st.md.nz > 1 && t[0].size() == 5) {
+                    int by = 0;  // y passes: the whole (tile, pipelining, plan) triple of the fastest configuration
+                    for (int c = 1; c < 4; ++c)
+                        if (t[c].size() == 5 && t[c][1] + t[c][3] < t[by][1] + t[by][3]) by = c;
+                    best.cols_wide = cfg[by].cols_wide;
+                    best.cols_pipe = cfg[by].cols_pipe;
+                    best.cols_plan = cfg[by].cols_plan;
+                    best.convz_reg = (t[0][2] + t[2][2]) <= (t[1][2] + t[3][2]) ? 1 : 0;
+                    best.xinv_run = (t[0][4] + t[2][4]) <= (t[1][4] + t[3][4]) ? 2 : 4;
+                } else if (t[0].size() == 3) {
+                    best.xinv_run = (t[0][2] + t[2][2]) <= (t[1][2] + t[3][2]) ? 2 : 4;
                 }
+                best.generic = generic;
+                dm->tune = best;
+                {
+                    std::lock_guard<std::mutex> lock(g_tune_mu);
+                    g_tune_cache[key] = best;
+                }
+                if (pass_ms)
+                    for (int c = 0; c < 4; ++c)
+                        for (size_t i = 0; i < 5; ++i) pass_ms[5 * c + i] = i < t[c].size() ? t[c][i] : 0.0;
+            }
         }
         choices[0] = best.cols_wide;
         choices[1] = best.convz_reg;
         choices[2] = best.xinv_run;
+        choices[3] = best.cols_pipe;
+        choices[4] = best.cols_plan;
+    });
+}
+
+int maf_llg_autotune(maf_llg l, maf_state s, int reps, int choices[3], double* pass_ms) {
+    int c5[5];
+    double ms[20];
+    const int rc = maf_llg_autotune_ex(l, s, reps, c5, pass_ms ? ms : nullptr, nullptr);
+    if (rc == 0) {
+        for (int i = 0; i < 3; ++i) choices[i] = c5[i];
+        if (pass_ms)
+            for (int i = 0; i < 5; ++i) {  // the defaults and the all-alternative configuration
+                pass_ms[i] = ms[i];
+                pass_ms[5 + i] = ms[5 + i];
+            }
+    }
+    return rc;
+}
+
+int maf_term_demag_get_tune_ex(maf_term t, int choices[5]) {
+    return guarded([&] {
+        check(t && choices && t->t->kind == TK_DEMAG && !t->t->demag_pbc(),
+              "maf_term_demag_get_tune_ex: not a DemagField");
+        const TuneChoice& c = t->t->demag->tune;
+        choices[0] = c.cols_wide;
+        choices[1] = c.convz_reg;
+        choices[2] = c.xinv_run;
+        choices[3] = c.cols_pipe;
+        choices[4] = c.cols_plan;
+    });
+}
+
+int maf_term_demag_set_tune_ex(maf_term t, const int choices[5]) {
+    return guarded([&] {
+        check(t && choices && t->t->kind == TK_DEMAG && !t->t->demag_pbc(),
+              "maf_term_demag_set_tune_ex: not a DemagField");
+        check((choices[0] == 0 || choices[0] == 1) && (choices[1] == 0 || choices[1] == 1) &&
+                  (choices[2] == 0 || choices[2] == 2 || choices[2] == 4) && (choices[3] == 0 || choices[3] == 1) &&
+                  (choices[4] == 0 || choices[4] == 1),
+              "maf_term_demag_set_tune_ex: choices are {0|1, 0|1, 0|2|4, 0|1, 0|1}");
+        TuneChoice& c = t->t->demag->tune;
+        c.cols_wide = choices[0];
+        c.convz_reg = choices[1];
+        c.xinv_run = choices[2];
+        c.cols_pipe = choices[3];
+        c.cols_plan = choices[4];
     });
 }
 

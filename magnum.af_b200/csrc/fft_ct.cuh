@@ -395,4 +395,12 @@ template <> struct CtPlan<1024> { using T = Radices<16, 16, 4>; };
 template <> struct CtPlan<2048> { using T = Radices<16, 16, 8>; };
 template <> struct CtPlan<4096> { using T = Radices<16, 16, 16>; };
 
+// Radix sequences the autotuner can choose for the column passes: V = 0 the
+// plan above, V = 1 the small radix in the middle (16 R 16) for lengths whose
+// plan ends in one (the pruned first stage keeps its radix 16 either way).
+template <int L, int V> struct CtPlanV { using T = typename CtPlan<L>::T; };
+template <> struct CtPlanV<512, 1> { using T = Radices<16, 2, 16>; };
+template <> struct CtPlanV<1024, 1> { using T = Radices<16, 4, 16>; };
+template <> struct CtPlanV<2048, 1> { using T = Radices<16, 8, 16>; };
+
 }  // namespace mafb

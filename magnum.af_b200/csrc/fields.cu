@@ -72,8 +72,10 @@ const void* Twiddles::get(int L, bool fp64) {
 }
 
 const void* Twiddles::get_ct(int L, bool fp64, const int* radix, int nstages) {
-    // one compile-time plan per length, so (L, precision) identifies the layout
-    auto key = std::make_pair(L, fp64 ? 3 : 2);
+    // (L, precision, radix sequence) identifies the layout
+    int code = 0;
+    for (int i = 0; i < nstages; ++i) code = code * 17 + radix[i];
+    auto key = std::make_pair(L, 2 + (fp64 ? 1 : 0) + 2 * code);
     auto it = tables_.find(key);
     if (it != tables_.end()) return it->second.p;
     const void* base = get(L, fp64);

@@ -176,7 +176,7 @@ __global__ void __launch_bounds__(NT, 4) k_xfwd_pipe(const R* __restrict__ in, i
 // n_out are truncated and not written).
 // HIN: n_in <= L/2 (zero-padded input), HOUT: n_out <= L/2 (truncated output);
 // both prune the transform at compile time
-template <typename R, int DIR, int L, int NB, int NT, bool HIN, bool HOUT>
+template <typename R, int DIR, int L, int NB, int NT, bool HIN, bool HOUT, int PV>
 __global__ void __launch_bounds__(NT, (kMinBlocks<R, NT * (L * NB / kE > NT ? L * NB / kE / NT : 1), 1024, 512>)) k_cols_ct(const cplx_t<R>* in, cplx_t<R>* out, int n_in, int n_out, int ncols,
                                                 int64_t in_si, int64_t out_si, int64_t in_sbat, int64_t out_sbat,
                                                 const cplx_t<R>* __restrict__ tw) {
@@ -195,7 +195,7 @@ __global__ void __launch_bounds__(NT, (kMinBlocks<R, NT * (L * NB / kE > NT ? L 
     auto st = [&](int b, int j, int di, C v) {
         if (b < ncv) ob[(int64_t)j * out_si + b + (int64_t)di * out_si] = v;
     };
-    ct_fft_io<R, DIR, true, L, NB, NT, HIN, HOUT>(s, 0, tw, ld, st, typename CtPlan<L>::T());
+    ct_fft_io<R, DIR, true, L, NB, NT, HIN, HOUT>(s, 0, tw, ld, st, typename CtPlanV<L, PV>::T());
 }
 
 // Column transforms, persistent and pipelined: each CTA walks tiles of NB
@@ -212,7 +212,7 @@ template <typename R, int L, int NB, bool HIN> constexpr size_t cols_pipe_smem()
     return cols_stage_offset<R, L, NB>() + sizeof(cplx_t<R>) * NB * (HIN ? L / 2 : L);
 }
 
-template <typename R, int DIR, int L, int NB, int NT, bool HIN, bool HOUT>
+template <typename R, int DIR, int L, int NB, int NT, bool HIN, bool HOUT, int PV>
 __global__ void __launch_bounds__(NT, NT >= 512 ? 1 : 2) k_cols_pipe(const cplx_t<R>* in, cplx_t<R>* out, int ncols, int64_t in_si,
                                                    int64_t out_si, int64_t in_sbat, int64_t out_sbat, int nbat,
                                                    int pitch, const cplx_t<R>* __restrict__ tw) {
@@ -258,7 +258,7 @@ __global__ void __launch_bounds__(NT, NT >= 512 ? 1 : 2) k_cols_pipe(const cplx_
         };
         const int64_t next = tile + gridDim.x;
         ct_fft_io_hook<R, DIR, true, L, NB, NT, HIN, HOUT>(
-            s, 0, tw, ld, [&] { if (next < ntiles) prefetch(next); }, st, typename CtPlan<L>::T());
+            s, 0, tw, ld, [&] { if (next < ntiles) prefetch(next); }, st, typename CtPlanV<L, PV>::T());
         __syncthreads();  // s is rewritten by the next tile's first stage
     }
 }
@@ -608,8 +608,8 @@ constexpr int pow2floor(int x) {
 
 // twiddles of the compile-time transform of length L: the W_L table and the
 // stage rows of its radix sequence
-template <int L> static const void* ct_tw(Twiddles& tw, bool f64) {
-    using P = typename CtPlan<L>::T;
+template <int L, int PV = 0> static const void* ct_tw(Twiddles& tw, bool f64) {
+    using P = typename CtPlanV<L, PV>::T;
     int rad[8] = {};
     radix_list(P(), rad);
     return tw.get_ct(L, f64, rad, radix_count(P()));
@@ -655,7 +655,7 @@ static void xfwd_L(const R* in, int n_in, int64_t rows, int64_t rows_pc, const R
     MAF_LAUNCH_CHECK();
 }
 
-template <typename R, int DIR, int L, int TILE, bool HIN, bool HOUT>
+template <typename R, int DIR, int L, int TILE, bool HIN, bool HOUT, int PV>
 static void cols_L(const cplx_t<R>* in, cplx_t<R>* out, int n_in, int n_out, int ncols, int64_t in_si, int64_t out_si,
                    int64_t in_sbat, int64_t out_sbat, int nbat, const void* tw, int pipe, int pitch, cudaStream_t st) {
     constexpr int NB = pow2floor(cmin(32, cmax(1, TILE / L)));
@@ -670,7 +670,7 @@ static void cols_L(const cplx_t<R>* in, cplx_t<R>* out, int n_in, int n_out, int
                         (in_si * (int64_t)sizeof(cplx_t<R>)) % 16 == 0 &&
                         (in_sbat * (int64_t)sizeof(cplx_t<R>)) % 16 == 0;
         if (ok) {
-            auto kp = k_cols_pipe<R, DIR, L, NB, NT, HIN, HOUT>;
+            auto kp = k_cols_pipe<R, DIR, L, NB, NT, HIN, HOUT, PV>;
             const size_t smem_p = cols_pipe_smem<R, L, NB, HIN>();
             ct_smem(kp, smem_p);
             int per_sm = 0;
@@ -683,7 +683,7 @@ static void cols_L(const cplx_t<R>* in, cplx_t<R>* out, int n_in, int n_out, int
             return;
         }
     }
-    auto k = k_cols_ct<R, DIR, L, NB, NT, HIN, HOUT>;
+    auto k = k_cols_ct<R, DIR, L, NB, NT, HIN, HOUT, PV>;
     ct_smem(k, smem);
     dim3 grid((unsigned)ceil_div(ncols, NB), (unsigned)nbat);
     k<<<grid, NT, smem, st>>>(in, out, n_in, n_out, ncols, in_si, out_si, in_sbat, out_sbat,
@@ -822,9 +822,20 @@ bool ct_cols(const cplx_t<R>* in, cplx_t<R>* out, int L, int n_in, int n_out, in
     // the row stride bounds the column tiles the pipelined kernel copies whole
     const int pitch = (int)std::min<int64_t>(in_si, 1 << 30);
     if (!hin && !hout && !f64) return false;
-#define C2(N, T, HI, HO)                                                                                   \
-    cols_L<R, DIR, N, T, HI, HO>(in, out, n_in, n_out, ncols, in_si, out_si, in_sbat, out_sbat, nbat,        \
-                                 ct_tw<N>(tw, f64), tc.cols_pipe, pitch, st)
+#define C3(N, T, HI, HO, V)                                                                                \
+    cols_L<R, DIR, N, T, HI, HO, V>(in, out, n_in, n_out, ncols, in_si, out_si, in_sbat, out_sbat, nbat,     \
+                                    ct_tw<N, V>(tw, f64), tc.cols_pipe, pitch, st)
+#define C2(N, T, HI, HO)               \
+    do {                               \
+        if constexpr (N >= 512) {      \
+            if (tc.cols_plan)          \
+                C3(N, T, HI, HO, 1);   \
+            else                       \
+                C3(N, T, HI, HO, 0);   \
+        } else {                       \
+            C3(N, T, HI, HO, 0);       \
+        }                              \
+    } while (0)
 #define C1(N, T)                                                \
     do {                                                        \
         if (hin)                                                \
@@ -845,6 +856,7 @@ bool ct_cols(const cplx_t<R>* in, cplx_t<R>* out, int L, int n_in, int n_out, in
 #undef X
 #undef C1
 #undef C2
+#undef C3
 }
 
 template <typename R>

@@ -92,6 +92,9 @@ _SIGS = {
     "maf_llg_heff_pipeline": (_I, [_P, _P, C.POINTER(_P), C.POINTER(_P), _I]),
     "maf_llg_heff_pipeline_m32": (_I, [_P, _P, C.POINTER(_P), C.POINTER(_P), _I]),
     "maf_llg_autotune": (_I, [_P, _P, _I, C.POINTER(_I), _DP]),
+    "maf_llg_autotune_ex": (_I, [_P, _P, _I, C.POINTER(_I), _DP, C.POINTER(_I)]),
+    "maf_term_demag_get_tune_ex": (_I, [_P, C.POINTER(_I)]),
+    "maf_term_demag_set_tune_ex": (_I, [_P, C.POINTER(_I)]),
     "maf_term_demag_get_tune": (_I, [_P, C.POINTER(_I)]),
     "maf_term_demag_set_tune": (_I, [_P, C.POINTER(_I)]),
     "maf_llg_heff_device_profile": (_I, [_P, _P, _P, _P, _DP, _I, C.POINTER(_I)]),
@@ -509,6 +512,18 @@ class DemagField(FieldTerm):
         _ck(lib.maf_term_demag_set_generic(self._h, int(bool(on))))
         self._generic = bool(on)
 
+    @property
+    def tune_ex(self):
+        """All kernel choices: (cols_wide, convz_reg, xinv_run, cols_pipe, cols_plan)."""
+        ch = (_I * 5)()
+        _ck(lib.maf_term_demag_get_tune_ex(self._h, ch))
+        return tuple(ch)
+
+    @tune_ex.setter
+    def tune_ex(self, choices):
+        ch = (_I * 5)(*[int(c) for c in choices])
+        _ck(lib.maf_term_demag_set_tune_ex(self._h, ch))
+
     def get_N(self, symmetric=False) -> np.ndarray:
         """Real-space Newell tensor [Px, Py, Pz, 6] (the reference's setup_N layout);
         symmetric=True returns the parity-exact tensor the spectral pipeline uses."""
@@ -784,6 +799,20 @@ class LLGIntegrator:
     def heff_device(self, state: State, m_dev_ptr: int, H_dev_ptr: int):
         """Field of a device-resident m into a device-resident H (no sync)."""
         _ck(lib.maf_llg_heff_device(self._h, state._h, C.c_void_p(m_dev_ptr), C.c_void_p(H_dev_ptr)))
+
+    def autotune_ex(self, state: State, reps: int = 3) -> dict:
+        """The full autotuner search (maf_llg_autotune_ex): four timed configurations,
+        the y passes' tile, pipelining and radix sequence chosen jointly; cached per
+        mesh, precision and term kinds within the process."""
+        ch = (_I * 5)()
+        ms = np.zeros(20)
+        cached = _I()
+        _ck(lib.maf_llg_autotune_ex(self._h, state._h, int(reps), ch, _dptr(ms), C.byref(cached)))
+        names = ("cols_wide", "convz_reg", "xinv_run", "cols_pipe", "cols_plan")
+        out = {k: ch[i] for i, k in enumerate(names)}
+        out["cached"] = bool(cached.value)
+        out["pass_ms"] = [ms[5 * c:5 * c + 5].tolist() for c in range(4)]
+        return out
 
     def autotune(self, state: State, reps: int = 3) -> dict:
         """Pick the faster kernel variant per demag pass on this state's mesh

@@ -55,8 +55,9 @@ def _case(shape, seed):
     return gm, m, d, gterms, ref
 
 
-# (cols_wide, convz_reg, xinv_run): the defaults first, then every alternative
-VARIANTS = [(0, 1, 2), (1, 1, 2), (0, 0, 4), (1, 0, 4)]
+# (cols_wide, convz_reg, xinv_run, cols_pipe, cols_plan): the defaults first, then
+# every alternative of each pass
+VARIANTS = [(0, 1, 2, 1, 0), (1, 1, 2, 1, 0), (0, 0, 4, 1, 0), (1, 0, 4, 0, 1), (0, 1, 2, 0, 1), (0, 1, 2, 1, 1)]
 
 
 @pytest.mark.parametrize("shape", [(1024, 1024, 2), (256, 256, 16)])
@@ -66,7 +67,7 @@ def test_heff_headline_sizes_vs_oracle(shape):
     s64 = M.State(gm, MS, m)
     s32 = M.State(gm, MS, m, precision="fp32_field")
     for tune in VARIANTS:
-        d.tune = tune
+        d.tune_ex = tune
         h64 = llg.H_in_Apm(s64)
         assert rel_l2(h64, ref) < 1e-12 and rel_max(h64, ref) < 1e-12, (tune, rel_l2(h64, ref), rel_max(h64, ref))
         h32 = llg.H_in_Apm_f32(s32)
