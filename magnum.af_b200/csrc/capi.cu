@@ -309,8 +309,10 @@ double rk_attempt(maf_llg_s* l, maf_state_s* st, const Scheme& sch, double dt, i
             ep.llg.m64 = s.m64.as<double>();
             if (marks) {
                 marks->mark(s.stream, "attempt");
-                ensure_m32(st);
-                marks->mark(s.stream, "stage_m32");
+                if (s.precision == PREC_FP32_FIELD) {  // the FP64 form has no FP32 copy
+                    ensure_m32(st);
+                    marks->mark(s.stream, "stage_m32");
+                }
             }
             eval_on_state(st, terms, ep, nullptr, nullptr, marks);
         } else {
