@@ -1,13 +1,17 @@
 // Batched passes of an ensemble of 2-D states (batch.hpp): every pass of a
-// fixed-step stochastic / RK4 step is one launch over a device work table of
-// (member, tile) pairs.  The tile bodies are the generic kernels' (run-time
-// FFT plans, passes_generic.cuh) and the element-wise kernels repeat the
+// fixed-step stochastic / RK4 step is one launch per transform length over a
+// device work table of (member, tile) pairs, the launches of a pass on
+// parallel graph branches.  Members whose lengths have compile-time kernels run
+// those kernels' tile bodies (fields_ct.cu), the others the generic kernels'
+// (run-time FFT plans, passes_generic.cuh); members of a DemagField set to the
+// run-time-plan kernels run those.  The element-wise kernels repeat the
 // arithmetic of llg.cu's, so a member's trajectory is bit-identical to the one
-// the per-state path computes with its generic kernels.
+// the per-state path computes with the same kernels.
 #include <algorithm>
 #include <cstring>
 
 #include "batch.hpp"
+#include "ct_dispatch.hpp"
 #include "passes_generic.cuh"
 
 namespace mafb {
@@ -177,21 +181,89 @@ int tile_threads(const FFTPlan& p, int ncols, int elems) {
 
 }  // namespace
 
+// The members of one compile-time kernel of a pass (same transform length L and,
+// for the x inverse, run length): their argument items, [parity][stage][member
+// of the class] for the x passes and [member of the class] for the convolution,
+// and the work table of (member of the class, tile).
+struct CtClass {
+    int L = 0, run = 0;
+    std::vector<int> members;
+    DevBuf items, work;
+    int nwork = 0;
+    const void* tw = nullptr;
+    const void* twP = nullptr;
+};
+
+// The members of a pass on the generic kernels with one transform length: their
+// work table of (member, tile) and the CTA shape the per-state launch uses.
+struct GenClass {
+    int L = 0;
+    std::vector<int2> w;
+    DevBuf work;
+    int nwork = 0, threads = 32;
+    size_t smem = 0;
+};
+
 struct FusedBatch::Impl {
     bool f32 = false;
     int M = 0, S = 0;
     FusedScheme scheme;
     std::vector<FusedMember> mem;
-    // argument arrays: [parity][stage][member] (x passes), [member] (conv)
+    // generic-kernel argument arrays: [parity][stage][member] (x passes), [member] (conv)
     DevBuf xfwd, conv, xinv, comb, fin, stage32, qptr;
-    DevBuf w_xfwd, w_conv, w_xinv, w_el3, w_cell;
-    int n_xfwd = 0, n_conv = 0, n_xinv = 0, n_el3 = 0, n_cell = 0;
-    int t_xfwd = 32, t_conv = 32, t_xinv = 32;
-    size_t s_xfwd = 0, s_conv = 0, s_xinv = 0;
+    DevBuf w_el3, w_cell;
+    int n_el3 = 0, n_cell = 0;
+    // the launches of a pass: one per transform length (generic and compile-time)
+    std::vector<GenClass> gx, gc, gi;
+    std::vector<CtClass> cx, cc, ci;
+    // the launches of a pass run on parallel branches: side streams and fork/join events
+    std::vector<cudaStream_t> side;
+    std::vector<cudaEvent_t> ev;
+    cudaEvent_t fork_ev = nullptr;
 
+    ~Impl() {
+        for (cudaStream_t q : side) cudaStreamDestroy(q);
+        for (cudaEvent_t e : ev) cudaEventDestroy(e);
+        if (fork_ev) cudaEventDestroy(fork_ev);
+    }
     template <typename R> void build(cudaStream_t st);
     template <typename R> void record(cudaStream_t st, int p);
+    // runs launch(b, stream) for b < n, branch 0 on st and the others on side streams
+    template <typename F> void branches(cudaStream_t st, int n, F&& launch);
 };
+
+template <typename F> void FusedBatch::Impl::branches(cudaStream_t st, int n, F&& launch) {
+    if (n <= 1) {
+        if (n == 1) launch(0, st);
+        return;
+    }
+    MAF_CUDA(cudaEventRecord(fork_ev, st));
+    for (int b = 1; b < n; ++b) MAF_CUDA(cudaStreamWaitEvent(side[b - 1], fork_ev, 0));
+    launch(0, st);
+    for (int b = 1; b < n; ++b) {
+        launch(b, side[b - 1]);
+        MAF_CUDA(cudaEventRecord(ev[b - 1], side[b - 1]));
+        MAF_CUDA(cudaStreamWaitEvent(st, ev[b - 1], 0));
+    }
+}
+
+// the class of cls with length L (and run), created on first use
+static CtClass& ct_class(std::vector<CtClass>& cls, int L, int run) {
+    for (CtClass& c : cls)
+        if (c.L == L && c.run == run) return c;
+    cls.emplace_back();
+    cls.back().L = L;
+    cls.back().run = run;
+    return cls.back();
+}
+
+static GenClass& gen_class(std::vector<GenClass>& cls, int L) {
+    for (GenClass& c : cls)
+        if (c.L == L) return c;
+    cls.emplace_back();
+    cls.back().L = L;
+    return cls.back();
+}
 
 template <typename R> void FusedBatch::Impl::build(cudaStream_t st) {
     using C = cplx_t<R>;
@@ -203,7 +275,42 @@ template <typename R> void FusedBatch::Impl::build(cudaStream_t st) {
     std::vector<FinA> fn((size_t)2 * M);
     std::vector<StageA> sg((size_t)2 * M);
     std::vector<unsigned long long*> qs(M);
-    std::vector<int2> wx, wc, wi, we, wn;
+    std::vector<int2> we, wn;
+    // compile-time kernel per pass and member (the per-state path's choice: ct_xfwd,
+    // ct_convy and ct_xinv run for these lengths unless the DemagField is set to the
+    // run-time-plan kernels); cx_of[i] etc.: the member's class, -1 for generic
+    std::vector<int> cx_of(M, -1), cc_of(M, -1), ci_of(M, -1), pos_x(M), pos_c(M), pos_i(M);
+    for (int i = 0; i < M; ++i) {
+        Demag* dm = mem[i].demag;
+        if (dm->tune.generic) continue;
+        const int Lc = dm->Px() / 2, Py = dm->Py();
+        const int run = dm->tune.xinv_run ? dm->tune.xinv_run : 2;
+        if (ct_batch_tile<R>(0, Lc) > 0) {
+            CtClass& c = ct_class(cx, Lc, 0);
+            cx_of[i] = (int)(&c - cx.data());
+            pos_x[i] = (int)c.members.size();
+            c.members.push_back(i);
+        }
+        if (ct_batch_tile<R>(1, Py) > 0) {
+            CtClass& c = ct_class(cc, Py, 0);
+            cc_of[i] = (int)(&c - cc.data());
+            pos_c[i] = (int)c.members.size();
+            c.members.push_back(i);
+        }
+        if (ct_batch_tile<R>(2, Lc) > 0 && mem[i].md.nx == Lc) {
+            CtClass& c = ct_class(ci, Lc, run);
+            ci_of[i] = (int)(&c - ci.data());
+            pos_i[i] = (int)c.members.size();
+            c.members.push_back(i);
+        }
+    }
+    std::vector<std::vector<CtXfwdItem<R>>> ixf(cx.size());
+    std::vector<std::vector<CtConvyItem<R>>> icv(cc.size());
+    std::vector<std::vector<CtXinvItem<R>>> ixi(ci.size());
+    std::vector<std::vector<int2>> wcx(cx.size()), wcc(cc.size()), wci(ci.size());
+    for (size_t c = 0; c < cx.size(); ++c) ixf[c].resize((size_t)2 * S * cx[c].members.size());
+    for (size_t c = 0; c < cc.size(); ++c) icv[c].resize(cc[c].members.size());
+    for (size_t c = 0; c < ci.size(); ++c) ixi[c].resize((size_t)2 * S * ci[c].members.size());
     for (int i = 0; i < M; ++i) {
         const FusedMember& f = mem[i];
         Demag* dm = f.demag;
@@ -211,6 +318,28 @@ template <typename R> void FusedBatch::Impl::build(cudaStream_t st) {
         const int64_t N = f.md.N(), rows_pc = (int64_t)ny * f.md.nz;
         const int Px = dm->Px(), Py = dm->Py(), Lc = Px / 2, nxh = dm->nxh(), pitch = dm->pitch();
         C* s1 = dm->spectrum<R>();
+        if (cx_of[i] >= 0) {
+            CtClass& c = cx[cx_of[i]];
+            if (!c.tw) {
+                c.tw = ct_batch_twiddles<R>(0, Lc, dm->twiddle_tables());
+                c.twP = dm->twiddles(Px, f64);
+            }
+            add_items(wcx[cx_of[i]], pos_x[i], ceil_div(3 * rows_pc, ct_batch_tile<R>(0, Lc)));
+        }
+        if (cc_of[i] >= 0) {
+            CtClass& c = cc[cc_of[i]];
+            if (!c.tw) c.tw = ct_batch_twiddles<R>(1, Py, dm->twiddle_tables());
+            add_items(wcc[cc_of[i]], pos_c[i], ceil_div(nxh, ct_batch_tile<R>(1, Py)));
+            icv[cc_of[i]][pos_c[i]] = CtConvyItem<R>{s1, dm->tensor_data<R>(), nxh, pitch};
+        }
+        if (ci_of[i] >= 0) {
+            CtClass& c = ci[ci_of[i]];
+            if (!c.tw) {
+                c.tw = ct_batch_twiddles<R>(2, Lc, dm->twiddle_tables());
+                c.twP = dm->twiddles(Px, f64);
+            }
+            add_items(wci[ci_of[i]], pos_i[i], ceil_div(rows_pc, ct_batch_tile<R>(2, Lc)));
+        }
         // x forward (launch_xfwd's generic shape)
         const FFTPlan px = make_fft_plan(Lc, dm->twiddles(Lc, f64));
         int nbx = pick_nb(Lc, tile_target<R>(), (int)std::min<int64_t>(3 * rows_pc, 1 << 20), 64);
@@ -219,9 +348,12 @@ template <typename R> void FusedBatch::Impl::build(cudaStream_t st) {
             if (th <= kMaxFftThreads || nbx == 1) break;
             nbx = std::max(1, nbx / 2);
         }
-        t_xfwd = std::max(t_xfwd, tile_threads(px, nbx, nbx * Lc));
-        s_xfwd = std::max(s_xfwd, sizeof(C) * (size_t)nbx * spad_len(Lc));
-        add_items(wx, i, ceil_div(3 * rows_pc, nbx));
+        if (cx_of[i] < 0) {
+            GenClass& g = gen_class(gx, Lc);
+            g.threads = std::max(g.threads, tile_threads(px, nbx, nbx * Lc));
+            g.smem = std::max(g.smem, sizeof(C) * (size_t)nbx * spad_len(Lc));
+            add_items(g.w, i, ceil_div(3 * rows_pc, nbx));
+        }
         // y convolution (forward_conv's generic nz == 1 shape)
         const FFTPlan py = make_fft_plan(Py, dm->twiddles(Py, f64));
         int nbc = pick_nb(3 * Py, tile_target<R>(), nxh, 64);
@@ -230,9 +362,12 @@ template <typename R> void FusedBatch::Impl::build(cudaStream_t st) {
             if (th <= kMaxFftThreads || nbc == 1) break;
             nbc = std::max(1, nbc / 2);
         }
-        t_conv = std::max(t_conv, tile_threads(py, 3 * nbc, 3 * nbc * Py));
-        s_conv = std::max(s_conv, sizeof(C) * (size_t)3 * nbc * spad_len(Py));
-        add_items(wc, i, ceil_div(nxh, nbc));
+        if (cc_of[i] < 0) {
+            GenClass& g = gen_class(gc, Py);
+            g.threads = std::max(g.threads, tile_threads(py, 3 * nbc, 3 * nbc * Py));
+            g.smem = std::max(g.smem, sizeof(C) * (size_t)3 * nbc * spad_len(Py));
+            add_items(g.w, i, ceil_div(nxh, nbc));
+        }
         cv[i] = ConvA<R>{s1, dm->tensor_data<R>(), py, ny, (int64_t)pitch, (int64_t)ny * pitch, nxh, nbc, ny, 1, nxh};
         // x inverse + LLG epilogue (inverse_x_epilogue's generic shape)
         int nbr = pick_nb(3 * Lc, tile_target<R>(), (int)std::min<int64_t>(rows_pc, 1 << 20), 32);
@@ -241,9 +376,12 @@ template <typename R> void FusedBatch::Impl::build(cudaStream_t st) {
             if (th <= kMaxFftThreads || nbr == 1) break;
             nbr = std::max(1, nbr / 2);
         }
-        t_xinv = std::max(t_xinv, tile_threads(px, 3 * nbr, 3 * nbr * Lc));
-        s_xinv = std::max(s_xinv, sizeof(C) * (size_t)3 * nbr * spad_len(Lc));
-        add_items(wi, i, ceil_div(rows_pc, nbr));
+        if (ci_of[i] < 0) {
+            GenClass& g = gen_class(gi, Lc);
+            g.threads = std::max(g.threads, tile_threads(px, 3 * nbr, 3 * nbr * Lc));
+            g.smem = std::max(g.smem, sizeof(C) * (size_t)3 * nbr * spad_len(Lc));
+            add_items(g.w, i, ceil_div(rows_pc, nbr));
+        }
         add_items(we, i, ceil_div(3 * N, kElemChunk));
         add_items(wn, i, ceil_div(N, kElemChunk));
         TermList tl;
@@ -279,6 +417,17 @@ template <typename R> void FusedBatch::Impl::build(cudaStream_t st) {
                     ep.llg.noise_index = fs.offset;
                 }
                 xi[a] = XinvA<R>{s1, pitch, px, twP, f.md.geom(), scale, in, ms, tl, ep, nbr};
+                if (cx_of[i] >= 0) {
+                    const size_t nc = cx[cx_of[i]].members.size();
+                    ixf[cx_of[i]][((size_t)p * S + s) * nc + pos_x[i]] =
+                        CtXfwdItem<R>{in, nx, 3 * rows_pc, (R)f.Ms, s1, pitch};
+                }
+                if (ci_of[i] >= 0) {
+                    const size_t nc = ci[ci_of[i]].members.size();
+                    CtXinvItem<R> it{s1, pitch, f.md.geom(), scale, in, ms, tl, ep, 0};
+                    ct_batch_xinv_prepare<R>(it);
+                    ixi[ci_of[i]][((size_t)p * S + s) * nc + pos_i[i]] = it;
+                }
                 CombA c{};
                 c.m = mp;
                 c.n = fs.n;
@@ -311,14 +460,42 @@ template <typename R> void FusedBatch::Impl::build(cudaStream_t st) {
     upload(fin, fn, st);
     upload(stage32, sg, st);
     upload(qptr, qs, st);
-    upload(w_xfwd, wx, st);
-    upload(w_conv, wc, st);
-    upload(w_xinv, wi, st);
+    size_t s_xfwd = 0, s_conv = 0, s_xinv = 0;
+    for (std::vector<GenClass>* v : {&gx, &gc, &gi})
+        for (GenClass& g : *v) {
+            upload(g.work, g.w, st);
+            g.nwork = (int)g.w.size();
+        }
+    for (const GenClass& g : gx) s_xfwd = std::max(s_xfwd, g.smem);
+    for (const GenClass& g : gc) s_conv = std::max(s_conv, g.smem);
+    for (const GenClass& g : gi) s_xinv = std::max(s_xinv, g.smem);
+    for (size_t c = 0; c < cx.size(); ++c) {
+        upload(cx[c].items, ixf[c], st);
+        upload(cx[c].work, wcx[c], st);
+        cx[c].nwork = (int)wcx[c].size();
+    }
+    for (size_t c = 0; c < cc.size(); ++c) {
+        upload(cc[c].items, icv[c], st);
+        upload(cc[c].work, wcc[c], st);
+        cc[c].nwork = (int)wcc[c].size();
+    }
+    for (size_t c = 0; c < ci.size(); ++c) {
+        upload(ci[c].items, ixi[c], st);
+        upload(ci[c].work, wci[c], st);
+        ci[c].nwork = (int)wci[c].size();
+    }
     upload(w_el3, we, st);
     upload(w_cell, wn, st);
-    n_xfwd = (int)wx.size();
-    n_conv = (int)wc.size();
-    n_xinv = (int)wi.size();
+    const size_t nbr_max = std::max({gx.size() + cx.size(), gc.size() + cc.size(), gi.size() + ci.size(), (size_t)1});
+    for (size_t b = 1; b < nbr_max; ++b) {
+        cudaStream_t q;
+        MAF_CUDA(cudaStreamCreateWithFlags(&q, cudaStreamNonBlocking));
+        side.push_back(q);
+        cudaEvent_t e;
+        MAF_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        ev.push_back(e);
+    }
+    MAF_CUDA(cudaEventCreateWithFlags(&fork_ev, cudaEventDisableTiming));
     n_el3 = (int)we.size();
     n_cell = (int)wn.size();
     auto smem_attr = [](auto k, size_t bytes) {
@@ -342,12 +519,39 @@ template <typename R> void FusedBatch::Impl::record(cudaStream_t st, int p) {
             kb_combine<<<n_el3, kElemThreads, 0, st>>>(comb.as<CombA>() + a, w_el3.as<int2>());
             MAF_LAUNCH_CHECK();
         }
-        kb_xfwd<R><<<n_xfwd, t_xfwd, s_xfwd, st>>>(xfwd.as<XfwdA<R>>() + a, w_xfwd.as<int2>());
-        MAF_LAUNCH_CHECK();
-        kb_conv<R><<<n_conv, t_conv, s_conv, st>>>(conv.as<ConvA<R>>(), w_conv.as<int2>());
-        MAF_LAUNCH_CHECK();
-        kb_xinv<R><<<n_xinv, t_xinv, s_xinv, st>>>(xinv.as<XinvA<R>>() + a, w_xinv.as<int2>());
-        MAF_LAUNCH_CHECK();
+        const int ngx = (int)gx.size(), ngc = (int)gc.size(), ngi = (int)gi.size();
+        branches(st, ngx + (int)cx.size(), [&](int b, cudaStream_t q) {
+            if (b < ngx) {
+                const GenClass& g = gx[b];
+                kb_xfwd<R><<<g.nwork, g.threads, g.smem, q>>>(xfwd.as<XfwdA<R>>() + a, g.work.as<int2>());
+                MAF_LAUNCH_CHECK();
+            } else {
+                const CtClass& c = cx[b - ngx];
+                ct_batch_xfwd<R>(c.items.as<CtXfwdItem<R>>() + ((size_t)p * S + s) * c.members.size(),
+                                 c.work.as<int2>(), c.nwork, c.L, c.tw, c.twP, q);
+            }
+        });
+        branches(st, ngc + (int)cc.size(), [&](int b, cudaStream_t q) {
+            if (b < ngc) {
+                const GenClass& g = gc[b];
+                kb_conv<R><<<g.nwork, g.threads, g.smem, q>>>(conv.as<ConvA<R>>(), g.work.as<int2>());
+                MAF_LAUNCH_CHECK();
+            } else {
+                const CtClass& c = cc[b - ngc];
+                ct_batch_convy<R>(c.items.as<CtConvyItem<R>>(), c.work.as<int2>(), c.nwork, c.L, c.tw, q);
+            }
+        });
+        branches(st, ngi + (int)ci.size(), [&](int b, cudaStream_t q) {
+            if (b < ngi) {
+                const GenClass& g = gi[b];
+                kb_xinv<R><<<g.nwork, g.threads, g.smem, q>>>(xinv.as<XinvA<R>>() + a, g.work.as<int2>());
+                MAF_LAUNCH_CHECK();
+            } else {
+                const CtClass& c = ci[b - ngi];
+                ct_batch_xinv<R>(c.items.as<CtXinvItem<R>>() + ((size_t)p * S + s) * c.members.size(),
+                                 c.work.as<int2>(), c.nwork, c.L, c.run, c.tw, c.twP, q);
+            }
+        });
     }
     kb_finalize<<<n_cell, kElemThreads, 0, st>>>(fin.as<FinA>() + (size_t)p * M, w_cell.as<int2>());
     MAF_LAUNCH_CHECK();
@@ -382,7 +586,11 @@ void FusedBatch::record_step(cudaStream_t st, int parity) {
         impl_->record<double>(st, parity & 1);
 }
 
-int FusedBatch::launches_per_step() const { return (impl_->f32 ? 1 : 0) + 4 * impl_->S - 1 + 2; }
+int FusedBatch::launches_per_step() const {
+    const Impl& b = *impl_;
+    const int per_stage = (int)(b.gx.size() + b.gc.size() + b.gi.size() + b.cx.size() + b.cc.size() + b.ci.size());
+    return (b.f32 ? 1 : 0) + b.S * (per_stage + 1) - 1 + 2;
+}
 
 bool fused_supported(const std::vector<FusedMember>& members, const FusedScheme& scheme) {
     if (members.empty() || scheme.stages.empty() || scheme.stages.size() > 6 || scheme.nfin < 1) return false;

@@ -175,6 +175,7 @@ class Demag {
     template <typename R> cplx_t<R>* spectrum() { return S1<R>(); }
     template <typename R> const R* tensor_data() { return tensor<R>(); }
     const void* twiddles(int L, bool fp64) { return tw_.get(L, fp64); }
+    Twiddles& twiddle_tables() { return tw_; }
 
   private:
     template <typename R> const R* tensor() ;

@@ -43,17 +43,19 @@ template <typename R, int LC, int NB> constexpr size_t xfwd_pipe_smem() {
 // ------------------------------------------------------------------ x forward
 // HIN: n_in <= LC, so the packed values k >= LC/2 are the zero padding (pruned
 // from the first stage)
+// (tile body: rows [tile NB, tile NB + NB); k_xfwd_ct runs tile blockIdx.x, the
+// batched kernel the tile of its work item)
 template <typename R, int LC, int NB, int NT, bool HIN>
-__global__ void __launch_bounds__(NT) k_xfwd_ct(const R* __restrict__ in, int n_in, int64_t rows, int64_t rows_pc,
-                                                const R* __restrict__ msf, R ms, cplx_t<R>* __restrict__ out,
-                                                int pitch, const cplx_t<R>* __restrict__ tw,
-                                                const cplx_t<R>* __restrict__ twP) {
+__device__ __forceinline__ void xfwd_ct_tile(const R* __restrict__ in, int n_in, int64_t rows, int64_t rows_pc,
+                                             const R* __restrict__ msf, R ms, cplx_t<R>* __restrict__ out,
+                                             int pitch, const cplx_t<R>* __restrict__ tw,
+                                             const cplx_t<R>* __restrict__ twP, int64_t tile) {
     using C = cplx_t<R>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C* s = reinterpret_cast<C*>(smem_raw);
     constexpr int SB = (LC - 1) + ((LC - 1) >> 4) + 1;
     static_assert(LC * NB % NT == 0, "tile");
-    const int64_t r0 = (int64_t)blockIdx.x * NB;
+    const int64_t r0 = tile * NB;
     const bool even = (n_in & 1) == 0;
     // packed pair (in[2k], in[2k+1]) * Ms of row b, k = j + dk, loaded straight into the first stage
     auto ld = [&](int b, int j, int dk) -> C {
@@ -104,6 +106,14 @@ __global__ void __launch_bounds__(NT) k_xfwd_ct(const R* __restrict__ in, int n_
         o[k] = cadd(E_, t);
         if (k < LC / 2) o[LC - k] = cconj(csub(E_, t));
     }
+}
+
+template <typename R, int LC, int NB, int NT, bool HIN>
+__global__ void __launch_bounds__(NT) k_xfwd_ct(const R* __restrict__ in, int n_in, int64_t rows, int64_t rows_pc,
+                                                const R* __restrict__ msf, R ms, cplx_t<R>* __restrict__ out,
+                                                int pitch, const cplx_t<R>* __restrict__ tw,
+                                                const cplx_t<R>* __restrict__ twP) {
+    xfwd_ct_tile<R, LC, NB, NT, HIN>(in, n_in, rows, rows_pc, msf, ms, out, pitch, tw, twP, blockIdx.x);
 }
 
 // x forward, persistent and pipelined: each CTA walks tiles of NB rows; the m rows
@@ -444,15 +454,16 @@ __global__ void __launch_bounds__(6 * NB, (kMinBlocks<R, 6 * NB, 576, 288>))
 }
 
 // -------------------------------------------------- y convolution (nz == 1)
+// (tile body: kx columns [tile NB, tile NB + NB))
 template <typename R, int L, int NB, int NT>
-__global__ void __launch_bounds__(NT) k_convy_ct(cplx_t<R>* S, const R* __restrict__ Nred, int ny, int nxh, int pitch,
-                                                 const cplx_t<R>* __restrict__ tw) {
+__device__ __forceinline__ void convy_ct_tile(cplx_t<R>* S, const R* __restrict__ Nred, int ny, int nxh, int pitch,
+                                              const cplx_t<R>* __restrict__ tw, int tile) {
     using C = cplx_t<R>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C* s = reinterpret_cast<C*>(smem_raw);
     constexpr int NC = 3 * NB;
     static_assert(L * NC % NT == 0, "tile");
-    const int c0 = blockIdx.x * NB;
+    const int c0 = tile * NB;
     const int ncv = min(NB, nxh - c0);
     const int64_t cs = (int64_t)ny * pitch;
     // column col = (comp, b) at y = i; rows i >= ny are padding
@@ -487,12 +498,19 @@ __global__ void __launch_bounds__(NT) k_convy_ct(cplx_t<R>* S, const R* __restri
     ct_fft_out<R, 1, true, L, NC, NT, true>(s, 0, tw, st, typename CtPlan<L>::T());
 }
 
+template <typename R, int L, int NB, int NT>
+__global__ void __launch_bounds__(NT) k_convy_ct(cplx_t<R>* S, const R* __restrict__ Nred, int ny, int nxh, int pitch,
+                                                 const cplx_t<R>* __restrict__ tw) {
+    convy_ct_tile<R, L, NB, NT>(S, Nred, ny, nxh, pitch, tw, blockIdx.x);
+}
+
 // --------------------------------------------------- x inverse + epilogue
+// (tile body: (y, z) rows [tile NBR, tile NBR + NBR))
 template <typename R, int EPI, int LC, int NBR, int NT, int RN>
-__global__ void __launch_bounds__(NT, (kMinBlocks<R, NT, (RN == 2 ? MAF_XINV_THREADS : 384), 192>)) k_xinv_ct(const cplx_t<R>* __restrict__ S1, int pitch,
-                                                const cplx_t<R>* __restrict__ tw, const cplx_t<R>* __restrict__ twP,
-                                                Geom g, R scale, const R* __restrict__ m, MsInfo ms, TermList tl,
-                                                EpilogueArgs ep, int run4) {
+__device__ __forceinline__ void xinv_ct_tile(const cplx_t<R>* __restrict__ S1, int pitch,
+                                             const cplx_t<R>* __restrict__ tw, const cplx_t<R>* __restrict__ twP,
+                                             const Geom& g, R scale, const R* __restrict__ m, const MsInfo& ms,
+                                             const TermList& tl, const EpilogueArgs& ep, int run4, int tile) {
     using C = cplx_t<R>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C* s = reinterpret_cast<C*>(smem_raw);
@@ -500,7 +518,7 @@ __global__ void __launch_bounds__(NT, (kMinBlocks<R, NT, (RN == 2 ? MAF_XINV_THR
     constexpr int SB = (LC - 1) + ((LC - 1) >> 4) + 1;
     static_assert(LC * NC % NT == 0, "tile");
     const int rows_pc = g.ny * g.nz;
-    const int ry0 = blockIdx.x * NBR;
+    const int ry0 = tile * NBR;
     // Z[k] = (X[k] + X*[LC-k]) + i (X[k] - X*[LC-k]) W^-k of column (comp, row),
     // formed from global memory straight into the first stage
     auto ld = [&](int col, int j, int dk) -> C {
@@ -573,6 +591,42 @@ __global__ void __launch_bounds__(NT, (kMinBlocks<R, NT, (RN == 2 ? MAF_XINV_THR
         epilogue_cell<R, EPI>(g, x, y, z, cell, m, ms, tl, ep, hd, eacc);
     }
     if constexpr (EPI == EPI_EDENS || EPI == EPI_EGRAD) block_sum_store(eacc, ep.partials);
+}
+
+template <typename R, int EPI, int LC, int NBR, int NT, int RN>
+__global__ void __launch_bounds__(NT, (kMinBlocks<R, NT, (RN == 2 ? MAF_XINV_THREADS : 384), 192>)) k_xinv_ct(const cplx_t<R>* __restrict__ S1, int pitch,
+                                                const cplx_t<R>* __restrict__ tw, const cplx_t<R>* __restrict__ twP,
+                                                Geom g, R scale, const R* __restrict__ m, MsInfo ms, TermList tl,
+                                                EpilogueArgs ep, int run4) {
+    xinv_ct_tile<R, EPI, LC, NBR, NT, RN>(S1, pitch, tw, twP, g, scale, m, ms, tl, ep, run4, blockIdx.x);
+}
+
+// ---------------------------------------------- batched (work-table) passes
+// One CTA per work item (item, tile): the item's arguments come from a device
+// array, the tile body is the per-state kernel's.
+template <typename R, int LC, int NB, int NT>
+__global__ void __launch_bounds__(NT) kbt_xfwd(const CtXfwdItem<R>* __restrict__ items, const int2* __restrict__ work,
+                                               const cplx_t<R>* __restrict__ tw, const cplx_t<R>* __restrict__ twP) {
+    const int2 w = work[blockIdx.x];
+    const CtXfwdItem<R> d = items[w.x];
+    xfwd_ct_tile<R, LC, NB, NT, true>(d.in, d.n_in, d.rows, d.rows, nullptr, d.ms, d.out, d.pitch, tw, twP, w.y);
+}
+
+template <typename R, int L, int NB, int NT>
+__global__ void __launch_bounds__(NT) kbt_convy(const CtConvyItem<R>* __restrict__ items, const int2* __restrict__ work,
+                                                const cplx_t<R>* __restrict__ tw) {
+    const int2 w = work[blockIdx.x];
+    const CtConvyItem<R> d = items[w.x];
+    convy_ct_tile<R, L, NB, NT>(d.S, d.Nred, L / 2, d.nxh, d.pitch, tw, w.y);
+}
+
+template <typename R, int LC, int NBR, int NT, int RN>
+__global__ void __launch_bounds__(NT, (kMinBlocks<R, NT, (RN == 2 ? MAF_XINV_THREADS : 384), 192>))
+    kbt_xinv(const CtXinvItem<R>* __restrict__ items, const int2* __restrict__ work, const cplx_t<R>* __restrict__ tw,
+             const cplx_t<R>* __restrict__ twP) {
+    const int2 w = work[blockIdx.x];
+    const CtXinvItem<R>& d = items[w.x];
+    xinv_ct_tile<R, EPI_LLG, LC, NBR, NT, RN>(d.S1, d.pitch, tw, twP, d.g, d.scale, d.m, d.ms, d.tl, d.ep, d.run4, w.y);
 }
 
 // ------------------------------------------------------------------ launches
@@ -775,6 +829,54 @@ static void xinv_L(const cplx_t<R>* S1, int pitch, const void* tw, const void* t
     MAF_LAUNCH_CHECK();
 }
 
+// Tile shapes of the per-state launches (xfwd_L, convy_L, xinv_L), shared by the batched ones.
+template <typename R, int LC> struct XfwdShape {
+    static constexpr int NB = pow2floor(cmax(1, kTileX<R> / LC));
+    static constexpr int NT = LC * NB / kE;
+    static constexpr size_t smem = sizeof(cplx_t<R>) * (size_t)NB * ((LC - 1) + ((LC - 1) >> 4) + 1);
+};
+template <typename R, int L> struct ConvyShape {
+    static constexpr int NB = pow2floor(cmin(32, cmax(1, kTileC<R> / (3 * L))));
+    static constexpr int NT = L * 3 * NB / kE;
+    static constexpr size_t smem = sizeof(cplx_t<R>) * (size_t)3 * NB * ((L - 1) + ((L - 1) >> 4) + 1);
+};
+template <typename R, int LC> struct XinvShape {
+    static constexpr int NBR = pow2floor(cmax(1, kTileC<R> / (6 * LC)));
+    static constexpr int NT = LC * 3 * NBR / kE;
+    static constexpr size_t smem = sizeof(cplx_t<R>) * (size_t)3 * NBR * ((LC - 1) + ((LC - 1) >> 4) + 1);
+};
+
+template <typename R, int LC>
+static void batch_xfwd_L(const CtXfwdItem<R>* items, const int2* work, int nwork, const void* tw, const void* twP,
+                         cudaStream_t st) {
+    using S = XfwdShape<R, LC>;
+    auto k = kbt_xfwd<R, LC, S::NB, S::NT>;
+    ct_smem(k, S::smem);
+    k<<<(unsigned)nwork, S::NT, S::smem, st>>>(items, work, static_cast<const cplx_t<R>*>(tw),
+                                                static_cast<const cplx_t<R>*>(twP));
+    MAF_LAUNCH_CHECK();
+}
+
+template <typename R, int L>
+static void batch_convy_L(const CtConvyItem<R>* items, const int2* work, int nwork, const void* tw, cudaStream_t st) {
+    using S = ConvyShape<R, L>;
+    auto k = kbt_convy<R, L, S::NB, S::NT>;
+    ct_smem(k, S::smem);
+    k<<<(unsigned)nwork, S::NT, S::smem, st>>>(items, work, static_cast<const cplx_t<R>*>(tw));
+    MAF_LAUNCH_CHECK();
+}
+
+template <typename R, int LC, int RN>
+static void batch_xinv_L(const CtXinvItem<R>* items, const int2* work, int nwork, const void* tw, const void* twP,
+                         cudaStream_t st) {
+    using S = XinvShape<R, LC>;
+    auto k = kbt_xinv<R, LC, S::NBR, S::NT, RN>;
+    ct_smem(k, S::smem);
+    k<<<(unsigned)nwork, S::NT, S::smem, st>>>(items, work, static_cast<const cplx_t<R>*>(tw),
+                                                static_cast<const cplx_t<R>*>(twP));
+    MAF_LAUNCH_CHECK();
+}
+
 #define MAF_CT_SWITCH(L, CALL) \
     switch (L) {               \
         case 16: CALL(16); return true;     \
@@ -929,6 +1031,74 @@ bool ct_xinv(const cplx_t<R>* S1, int pitch, int Px, Twiddles& tw, const Geom& g
 #undef X
 }
 
+// lengths of the batched kernels: x passes L = Px / 2 and y convolution L = Py, 16..2048
+#define MAF_CT_BATCH_SWITCH(L, CALL)  \
+    switch (L) {                      \
+        case 16: CALL(16); break;     \
+        case 32: CALL(32); break;     \
+        case 64: CALL(64); break;     \
+        case 128: CALL(128); break;   \
+        case 256: CALL(256); break;   \
+        case 512: CALL(512); break;   \
+        case 1024: CALL(1024); break; \
+        case 2048: CALL(2048); break; \
+        default: break;               \
+    }
+
+template <typename R> int ct_batch_tile(int pass, int L) {
+    int t = 0;
+#define X(N) t = pass == 0 ? XfwdShape<R, N>::NB : pass == 1 ? ConvyShape<R, N>::NB : XinvShape<R, N>::NBR
+    MAF_CT_BATCH_SWITCH(L, X)
+#undef X
+    return t;
+}
+
+template <typename R> const void* ct_batch_twiddles(int pass, int L, Twiddles& tw) {
+    (void)pass;  // every pass of these lengths runs the default radix plan
+    const void* p = nullptr;
+#define X(N) p = ct_tw<N>(tw, sizeof(R) == 8)
+    MAF_CT_BATCH_SWITCH(L, X)
+#undef X
+    return p;
+}
+
+template <typename R> void ct_batch_xinv_prepare(CtXinvItem<R>& it) {
+    it.run4 = run4_eligible(it.g, it.m, it.ms, it.tl, it.ep) ? 1 : 0;
+    if (it.run4) prepare_run4(it.tl, it.g, it.ms.Ms);
+}
+
+template <typename R>
+void ct_batch_xfwd(const CtXfwdItem<R>* items, const int2* work, int nwork, int L, const void* tw, const void* twP,
+                   cudaStream_t st) {
+    if (nwork <= 0) return;
+#define X(N) batch_xfwd_L<R, N>(items, work, nwork, tw, twP, st)
+    MAF_CT_BATCH_SWITCH(L, X)
+#undef X
+}
+
+template <typename R>
+void ct_batch_convy(const CtConvyItem<R>* items, const int2* work, int nwork, int L, const void* tw, cudaStream_t st) {
+    if (nwork <= 0) return;
+#define X(N) batch_convy_L<R, N>(items, work, nwork, tw, st)
+    MAF_CT_BATCH_SWITCH(L, X)
+#undef X
+}
+
+template <typename R>
+void ct_batch_xinv(const CtXinvItem<R>* items, const int2* work, int nwork, int L, int run, const void* tw,
+                   const void* twP, cudaStream_t st) {
+    if (nwork <= 0) return;
+#define X(N)                                                        \
+    do {                                                            \
+        if (run == 4)                                               \
+            batch_xinv_L<R, N, 4>(items, work, nwork, tw, twP, st); \
+        else                                                        \
+            batch_xinv_L<R, N, 2>(items, work, nwork, tw, twP, st); \
+    } while (0)
+    MAF_CT_BATCH_SWITCH(L, X)
+#undef X
+}
+
 // The instantiations are split over several compilations of this file
 // (MAF_CT_PART = 1: x forward and convolutions, 2: y passes, 3: x inverse;
 // MAF_CT_REAL = 4 or 8 selects FP32 or FP64), so that the build compiles them
@@ -939,7 +1109,13 @@ bool ct_xinv(const cplx_t<R>* S1, int pitch, int Px, Twiddles& tw, const Geom& g
                              cudaStream_t);                                                                          \
     template bool ct_convz<R>(cplx_t<R>*, const R*, int, int, int, int, Twiddles&, const TuneChoice&,                \
                               cudaStream_t);                                                                         \
-    template bool ct_convy<R>(cplx_t<R>*, const R*, int, int, int, Twiddles&, cudaStream_t);
+    template bool ct_convy<R>(cplx_t<R>*, const R*, int, int, int, Twiddles&, cudaStream_t);                    \
+    template int ct_batch_tile<R>(int, int);                                                                      \
+    template const void* ct_batch_twiddles<R>(int, int, Twiddles&);                                               \
+    template void ct_batch_xinv_prepare<R>(CtXinvItem<R>&);                                                       \
+    template void ct_batch_xfwd<R>(const CtXfwdItem<R>*, const int2*, int, int, const void*, const void*,        \
+                                   cudaStream_t);                                                                \
+    template void ct_batch_convy<R>(const CtConvyItem<R>*, const int2*, int, int, const void*, cudaStream_t);
 #else
 #define MAF_INST1(R)
 #endif
@@ -955,7 +1131,9 @@ bool ct_xinv(const cplx_t<R>* S1, int pitch, int Px, Twiddles& tw, const Geom& g
 #if !defined(MAF_CT_PART) || MAF_CT_PART == 3
 #define MAF_INST3(R)                                                                                                  \
     template bool ct_xinv<R>(const cplx_t<R>*, int, int, Twiddles&, const Geom&, R, const R*, const MsInfo&,          \
-                             const TermList&, const EpilogueArgs&, const TuneChoice&, cudaStream_t, int*);
+                             const TermList&, const EpilogueArgs&, const TuneChoice&, cudaStream_t, int*);        \
+    template void ct_batch_xinv<R>(const CtXinvItem<R>*, const int2*, int, int, int, const void*, const void*,      \
+                                   cudaStream_t);
 #else
 #define MAF_INST3(R)
 #endif

@@ -1,11 +1,11 @@
 """Batched passes of a stochastic ensemble (StochasticBatch(fused=True),
-maf_stoch_batch_set_fused): every pass of a step is one launch over a device
-work table of (member, tile) pairs for members of uneven 2-D meshes.  Each
-member's trajectory must equal, bit for bit, the one its own integrator
-computes with the same (run-time-plan) kernels, for odd and even step counts,
-after a member was stepped alone in between, and in the FP32-field and FP64
-forms and the three schemes; the default compile-time kernels agree to
-rounding."""
+maf_stoch_batch_set_fused): every pass of a step is one launch per transform
+length over a device work table of (member, tile) pairs for members of uneven
+2-D meshes -- the compile-time kernels' tile bodies where the length has them,
+the run-time-plan kernels' for the others.  Each member's trajectory must
+equal, bit for bit, the one its own integrator computes with the same kernels,
+for odd and even step counts, after a member was stepped alone in between, and
+in the FP32-field and FP64 forms and the three schemes."""
 import numpy as np
 import pytest
 
@@ -57,18 +57,27 @@ def test_fused_batch_matches_members_bitwise(prec, scheme):
         assert np.array_equal(np.asarray(stb.m), np.asarray(sts.m))
 
 
-def test_fused_batch_close_to_compile_time_kernels():
-    """The compile-time kernels (default) and the run-time-plan ones compute the
-    same fields up to rounding: trajectories agree to FP32 accuracy."""
-    sides = [(64, 64), (128, 128)]
-    bm = _members("fp32_field", "Heun", generic=False, sides=sides, T=0.0)
-    sm = _members("fp32_field", "Heun", generic=False, sides=sides, T=0.0)
+# power-of-two and other sides: each pass mixes compile-time classes (x length
+# 64, 128, 32 / y length 128, 256) with members on the run-time-plan kernels
+CT_SIDES = [(64, 64), (128, 96), (96, 64), (32, 128), (64, 128), (40, 24)]
+
+
+@pytest.mark.parametrize("prec,scheme", [("fp32_field", "Heun"), ("fp64", "Heun"), ("fp32_field", "detRK4")])
+def test_fused_batch_compile_time_kernels_bitwise(prec, scheme):
+    """The default (compile-time) kernels: the batch groups the members by
+    transform length and runs the per-state kernels' tile bodies, so every
+    member's trajectory equals its own integrator's bit for bit."""
+    bm = _members(prec, scheme, generic=False, sides=CT_SIDES)
+    sm = _members(prec, scheme, generic=False, sides=CT_SIDES)
     batch = M.StochasticBatch([(it, st) for it, st, _ in bm], fused=True)
-    batch.steps(6)
-    for it, st, _ in sm:
-        it.steps(st, 6)
-    for (_, stb, _), (_, sts, _) in zip(bm, sm):
-        assert np.abs(np.asarray(stb.m) - np.asarray(sts.m)).max() < 1e-6
+    for n in (5, 4):
+        batch.steps(n)
+        assert batch.fused_active
+        for it, st, _ in sm:
+            it.steps(st, n)
+        for (itb, stb, _), (its, sts, _) in zip(bm, sm):
+            assert np.array_equal(np.asarray(stb.m), np.asarray(sts.m))
+            assert stb.t == sts.t and itb.calls == its.calls
 
 
 def test_fused_batch_falls_back_for_3d_members():
