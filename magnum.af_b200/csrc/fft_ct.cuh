@@ -1,4 +1,5 @@
-// Compile-time specialised FFT stages for power-of-two lengths.
+// Compile-time specialised FFT stages for power-of-two lengths and three times
+// a power of two.
 //
 // The transform length, the radix sequence, the number of columns in the tile
 // and the CTA size are template parameters, so every index is a constant
@@ -86,15 +87,30 @@ template <int DIR, typename R> __host__ __device__ __forceinline__ void bfly16_h
     }
 }
 
+// 3-point DFT: with W3 = -1/2 + i DIR sqrt(3)/2, y0 = a + (b + c),
+// y1,2 = a - (b + c)/2 +- i DIR (sqrt(3)/2) (b - c).
+template <int DIR, typename R> __host__ __device__ __forceinline__ void bfly3(cplx_t<R>* v) {
+    const R h3 = (R)0.86602540378443864676;  // sqrt(3)/2
+    const cplx_t<R> t1 = cadd(v[1], v[2]);
+    const cplx_t<R> t2 = csub(v[0], cscale(t1, (R)0.5));
+    const cplx_t<R> d = csub(v[1], v[2]);
+    const cplx_t<R> t3 = mk(-(R)DIR * h3 * d.y, (R)DIR * h3 * d.x);  // i DIR h3 (b - c)
+    v[0] = cadd(v[0], t1);
+    v[1] = cadd(t2, t3);
+    v[2] = csub(t2, t3);
+}
+
 template <int RAD, int DIR, typename R> __device__ __forceinline__ void bfly_ct(cplx_t<R>* v) {
     if constexpr (RAD == 2) {
         bfly2<DIR>(v[0], v[1]);
+    } else if constexpr (RAD == 3) {
+        bfly3<DIR, R>(v);
     } else if constexpr (RAD == 4) {
         bfly4<DIR>(v);
     } else if constexpr (RAD == 8) {
         bfly8<DIR, R>(v);
     } else {
-        static_assert(RAD == 16, "power-of-two radix");
+        static_assert(RAD == 16, "radix 2, 3, 4, 8 or 16");
         bfly16<DIR, R>(v);
     }
 }
@@ -119,12 +135,90 @@ template <bool BFAST, int NB, int STEP> constexpr int sdist() { return (STEP + S
 // its twiddles from one row at compile-time offsets.
 template <int NS, int RAD> constexpr int tw_rows() { return NS > 1 ? NS * (RAD - 1) : 0; }
 
+// How a stage after the first gets its twiddles (build options per precision):
+// 0 every twiddle of a butterfly is loaded from its row when the stage starts
+// (correctly rounded twiddles); 1 only W^t, W^2t, W^4t and W^8t are loaded
+// (t = the butterfly's row step) and the others are formed as products of at
+// most four of them (a few ulp; 8-10 % faster x and y passes in FP32, field
+// error unchanged at the 6e-8 level); 2 as 1, with the loads issued by the
+// previous stage right before its closing barrier.  The FP64 form, the
+// accuracy reference, keeps 0.
+#ifndef MAF_TW_MODE_F32
+#define MAF_TW_MODE_F32 1
+#endif
+#ifndef MAF_TW_MODE_F64
+#define MAF_TW_MODE_F64 0
+#endif
+static_assert(MAF_TW_MODE_F32 >= 0 && MAF_TW_MODE_F32 <= 2 && MAF_TW_MODE_F64 >= 0 && MAF_TW_MODE_F64 <= 2,
+              "twiddle mode");
+template <typename R> constexpr int tw_mode() { return sizeof(R) == 4 ? MAF_TW_MODE_F32 : MAF_TW_MODE_F64; }
+
+template <int A, int... REST> struct FirstOf { static constexpr int value = A; };
+
+// The twiddles of this thread's butterflies in one stage (nothing for NS = 1).
+template <typename R, int RAD, int NS, int L, int NB, int NT, bool BFAST, int TWO> struct TwStage {
+    using C = cplx_t<R>;
+    static constexpr int NBF = L / RAD;
+    static constexpr int TOTAL = NBF * NB;
+    static constexpr int BPT = (TOTAL + NT - 1) / NT;
+    // (a radix-3 stage loads both of its twiddles)
+    static constexpr bool FULL = tw_mode<R>() == 0 || RAD == 3;
+    static constexpr int NBASE = NS == 1 ? 0 : FULL ? RAD - 1 : (RAD == 16 ? 4 : RAD == 8 ? 3 : RAD == 4 ? 2 : 1);
+    C w[BPT][NBASE > 0 ? NBASE : 1];
+    __device__ __forceinline__ void load(const C* __restrict__ tw) {
+        if constexpr (NBASE > 0) {
+#pragma unroll
+            for (int k = 0; k < BPT; ++k) {
+                const int q = threadIdx.x + k * NT;
+                if (TOTAL % NT == 0 || q < TOTAL) {
+                    const int j = BFAST ? q / NB : q % NBF;
+                    const C* __restrict__ twr = tw + TWO + (j % NS) * (RAD - 1) - 1;
+                    if constexpr (FULL) {
+#pragma unroll
+                        for (int r = 1; r < RAD; ++r) w[k][r - 1] = twr[r];
+                    } else {
+#pragma unroll
+                        for (int e = 0; e < NBASE; ++e) w[k][e] = twr[1 << e];
+                    }
+                }
+            }
+        }
+    }
+    // the RAD - 1 twiddles of butterfly k: out[r] = W^(r t), r = 1 .. RAD - 1
+    __device__ __forceinline__ void expand(int k, C* out) const {
+        if constexpr (FULL || RAD == 2) {
+#pragma unroll
+            for (int r = 1; r < RAD; ++r) out[r] = w[k][r - 1];
+        } else {
+            out[1] = w[k][0];
+            out[2] = w[k][1];
+            out[3] = cmul(out[1], out[2]);
+            if constexpr (RAD >= 8) {
+                out[4] = w[k][2];
+                out[5] = cmul(out[1], out[4]);
+                out[6] = cmul(out[2], out[4]);
+                out[7] = cmul(out[3], out[4]);
+            }
+            if constexpr (RAD == 16) {
+                out[8] = w[k][3];
+#pragma unroll
+                for (int r = 9; r < 16; ++r) out[r] = cmul(out[r - 8], out[8]);
+            }
+        }
+    }
+};
+
 // One stage over NB columns of length L with NT threads; TWO is the offset of
 // the stage's twiddle rows.  HOUT (last stage only): just the outputs i < L/2
 // are written, the arithmetic only the others need is dropped.
-template <typename R, int RAD, int DIR, bool BFAST, int L, int NS, int NB, int NT, int TWO, bool HOUT = false>
-__device__ __forceinline__ void ct_stage(cplx_t<R>* s, int sb, const cplx_t<R>* __restrict__ tw) {
+// cur: the stage's twiddles (preloaded in mode 2, else loaded here); pre() runs
+// after the outputs are written, before the closing barrier (the next stage's
+// twiddle prefetch).
+template <typename R, int RAD, int DIR, bool BFAST, int L, int NS, int NB, int NT, int TWO, bool HOUT = false,
+          typename TWC, typename PRE>
+__device__ __forceinline__ void ct_stage(cplx_t<R>* s, int sb, const cplx_t<R>* __restrict__ tw, TWC& cur, PRE&& pre) {
     static_assert(!HOUT || NS * RAD == L, "output pruning is for the last stage");
+    if constexpr (tw_mode<R>() != 2) cur.load(tw);
     using C = cplx_t<R>;
     constexpr int NBF = L / RAD;
     constexpr int TOTAL = NBF * NB;
@@ -140,16 +234,13 @@ __device__ __forceinline__ void ct_stage(cplx_t<R>* s, int sb, const cplx_t<R>* 
         if (TOTAL % NT == 0 || q < TOTAL) {
             const int b = BFAST ? q % NB : q / NBF;
             const int j = BFAST ? q / NB : q % NBF;
-            const int jm = j % NS;
-            const C* __restrict__ twr = tw + TWO + jm * (RAD - 1) - 1;
             const int base = LIN_IN ? sidx<BFAST, NB>(j, b, sb) : 0;
+            C w[RAD];
+            if constexpr (NS > 1) cur.expand(k, w);
 #pragma unroll
             for (int r = 0; r < RAD; ++r) {
                 C x = s[LIN_IN ? base + r * DIN : sidx<BFAST, NB>(j + r * NBF, b, sb)];
-                if (NS > 1 && r > 0) {
-                    const C w = twr[r];
-                    x = DIR < 0 ? cmul(x, w) : cmulc(x, w);
-                }
+                if (NS > 1 && r > 0) x = DIR < 0 ? cmul(x, w[r]) : cmulc(x, w[r]);
                 v[k][r] = x;
             }
             bfly_ct<RAD, DIR, R>(v[k]);
@@ -172,22 +263,33 @@ __device__ __forceinline__ void ct_stage(cplx_t<R>* s, int sb, const cplx_t<R>* 
             }
         }
     }
+    pre();
     __syncthreads();
 }
 
-template <typename R, int DIR, bool BFAST, int L, int NS, int NB, int NT, bool HOUT, int TWO, int RAD, int... REST>
-__device__ __forceinline__ void ct_run(cplx_t<R>* s, int sb, const cplx_t<R>* __restrict__ tw) {
+// the twiddle set of the stage with radix RAD after NS, whose rows start at TWO
+template <typename R, int RAD, int NS, int L, int NB, int NT, bool BFAST, int TWO>
+using TwOf = TwStage<R, RAD, NS, L, NB, NT, BFAST, TWO>;
+
+template <typename R, int DIR, bool BFAST, int L, int NS, int NB, int NT, bool HOUT, int TWO, typename TWC, int RAD,
+          int... REST>
+__device__ __forceinline__ void ct_run(cplx_t<R>* s, int sb, const cplx_t<R>* __restrict__ tw, TWC& cur) {
     if constexpr (sizeof...(REST) > 0) {
-        ct_stage<R, RAD, DIR, BFAST, L, NS, NB, NT, TWO>(s, sb, tw);
-        ct_run<R, DIR, BFAST, L, NS * RAD, NB, NT, HOUT, TWO + tw_rows<NS, RAD>(), REST...>(s, sb, tw);
+        constexpr int TWN = TWO + tw_rows<NS, RAD>();
+        TwOf<R, FirstOf<REST...>::value, NS * RAD, L, NB, NT, BFAST, TWN> nxt;
+        ct_stage<R, RAD, DIR, BFAST, L, NS, NB, NT, TWO>(s, sb, tw, cur, [&] {
+            if constexpr (tw_mode<R>() == 2) nxt.load(tw);
+        });
+        ct_run<R, DIR, BFAST, L, NS * RAD, NB, NT, HOUT, TWN, decltype(nxt), REST...>(s, sb, tw, nxt);
     } else {
-        ct_stage<R, RAD, DIR, BFAST, L, NS, NB, NT, TWO, HOUT>(s, sb, tw);
+        ct_stage<R, RAD, DIR, BFAST, L, NS, NB, NT, TWO, HOUT>(s, sb, tw, cur, [] {});
     }
 }
 
 template <typename R, int DIR, bool BFAST, int L, int NB, int NT, int... RS>
 __device__ __forceinline__ void ct_fft(cplx_t<R>* s, int sb, const cplx_t<R>* __restrict__ tw, Radices<RS...>) {
-    ct_run<R, DIR, BFAST, L, 1, NB, NT, false, L, RS...>(s, sb, tw);
+    TwOf<R, FirstOf<RS...>::value, 1, L, NB, NT, BFAST, L> none;
+    ct_run<R, DIR, BFAST, L, 1, NB, NT, false, L, decltype(none), RS...>(s, sb, tw, none);
 }
 
 // ----------------------------------------------------------------------------
@@ -209,8 +311,8 @@ template <bool BFAST, int NB, int NBF> __device__ __forceinline__ void ct_bj(int
 // The caller synchronises before s is overwritten; ends with a barrier.
 // HIN: the inputs i >= L/2 are zero (a zero-padded transform) -- with a radix-16
 // first stage they are neither loaded nor fed through the butterfly.
-template <typename R, int RAD, int DIR, bool BFAST, int L, int NB, int NT, bool HIN, typename LD>
-__device__ __forceinline__ void ct_stage_in(cplx_t<R>* s, int sb, LD&& ld) {
+template <typename R, int RAD, int DIR, bool BFAST, int L, int NB, int NT, bool HIN, typename LD, typename PRE>
+__device__ __forceinline__ void ct_stage_in(cplx_t<R>* s, int sb, LD&& ld, PRE&& pre) {
     using C = cplx_t<R>;
     constexpr int NBF = L / RAD;
     constexpr int TOTAL = NBF * NB;
@@ -244,6 +346,7 @@ __device__ __forceinline__ void ct_stage_in(cplx_t<R>* s, int sb, LD&& ld) {
                 s[LIN_OUT ? base + r * (BFAST ? NB : 1) : sidx<BFAST, NB>(j * RAD + r, b, sb)] = v[k][r];
         }
     }
+    pre();
     __syncthreads();
 }
 
@@ -251,9 +354,11 @@ __device__ __forceinline__ void ct_stage_in(cplx_t<R>* s, int sb, LD&& ld) {
 // barrier at the end: the caller synchronises before s is reused.
 // HOUT: only the outputs i < L/2 are wanted (a truncated transform): the others
 // are not stored, and the arithmetic that only they need is dropped.
-template <typename R, int RAD, int DIR, bool BFAST, int L, int NB, int NT, bool HOUT, int TWO, typename ST>
-__device__ __forceinline__ void ct_stage_out(const cplx_t<R>* s, int sb, const cplx_t<R>* __restrict__ tw, ST&& st) {
+template <typename R, int RAD, int DIR, bool BFAST, int L, int NB, int NT, bool HOUT, int TWO, typename TWC, typename ST>
+__device__ __forceinline__ void ct_stage_out(const cplx_t<R>* s, int sb, const cplx_t<R>* __restrict__ tw, TWC& cur,
+                                             ST&& st) {
     using C = cplx_t<R>;
+    if constexpr (tw_mode<R>() != 2) cur.load(tw);
     constexpr int NBF = L / RAD;
     constexpr int NS = NBF;
     constexpr int TOTAL = NBF * NB;
@@ -266,16 +371,13 @@ __device__ __forceinline__ void ct_stage_out(const cplx_t<R>* s, int sb, const c
         if (TOTAL % NT == 0 || q < TOTAL) {
             int b, j;
             ct_bj<BFAST, NB, NBF>(q, b, j);
-            const C* __restrict__ twr = tw + TWO + j * (RAD - 1) - 1;
             const int base = LIN_IN ? sidx<BFAST, NB>(j, b, sb) : 0;
-            C v[RAD];
+            C v[RAD], w[RAD];
+            if constexpr (NS > 1) cur.expand(k, w);
 #pragma unroll
             for (int r = 0; r < RAD; ++r) {
                 C x = s[LIN_IN ? base + r * DIN : sidx<BFAST, NB>(j + r * NBF, b, sb)];
-                if (NS > 1 && r > 0) {
-                    const C w = twr[r];
-                    x = DIR < 0 ? cmul(x, w) : cmulc(x, w);
-                }
+                if (NS > 1 && r > 0) x = DIR < 0 ? cmul(x, w[r]) : cmulc(x, w[r]);
                 v[r] = x;
             }
             bfly_ct<RAD, DIR, R>(v);
@@ -286,15 +388,19 @@ __device__ __forceinline__ void ct_stage_out(const cplx_t<R>* s, int sb, const c
     }
 }
 
-template <typename R, int DIR, bool BFAST, int L, int NS, int NB, int NT, bool HOUT, int TWO, typename ST, int RAD,
-          int... REST>
-__device__ __forceinline__ void ct_run_out(cplx_t<R>* s, int sb, const cplx_t<R>* __restrict__ tw, ST&& st) {
+template <typename R, int DIR, bool BFAST, int L, int NS, int NB, int NT, bool HOUT, int TWO, typename ST,
+          typename TWC, int RAD, int... REST>
+__device__ __forceinline__ void ct_run_out(cplx_t<R>* s, int sb, const cplx_t<R>* __restrict__ tw, TWC& cur, ST&& st) {
     if constexpr (sizeof...(REST) == 0) {
         static_assert(NS * RAD == L, "radix sequence");
-        ct_stage_out<R, RAD, DIR, BFAST, L, NB, NT, HOUT, TWO>(s, sb, tw, st);
+        ct_stage_out<R, RAD, DIR, BFAST, L, NB, NT, HOUT, TWO>(s, sb, tw, cur, st);
     } else {
-        ct_stage<R, RAD, DIR, BFAST, L, NS, NB, NT, TWO>(s, sb, tw);
-        ct_run_out<R, DIR, BFAST, L, NS * RAD, NB, NT, HOUT, TWO + tw_rows<NS, RAD>(), ST, REST...>(s, sb, tw, st);
+        constexpr int TWN = TWO + tw_rows<NS, RAD>();
+        TwOf<R, FirstOf<REST...>::value, NS * RAD, L, NB, NT, BFAST, TWN> nxt;
+        ct_stage<R, RAD, DIR, BFAST, L, NS, NB, NT, TWO>(s, sb, tw, cur, [&] {
+            if constexpr (tw_mode<R>() == 2) nxt.load(tw);
+        });
+        ct_run_out<R, DIR, BFAST, L, NS * RAD, NB, NT, HOUT, TWN, ST, decltype(nxt), REST...>(s, sb, tw, nxt, st);
     }
 }
 
@@ -305,8 +411,15 @@ template <typename R, int DIR, bool BFAST, int L, int NB, int NT, bool HIN = fal
 __device__ __forceinline__ void ct_fft_in(cplx_t<R>* s, int sb, const cplx_t<R>* __restrict__ tw, LD&& ld,
                                           Radices<R0, RS...>) {
     static_assert(!HOUT || sizeof...(RS) > 0, "output pruning needs a separate last stage");
-    ct_stage_in<R, R0, DIR, BFAST, L, NB, NT, HIN>(s, sb, ld);
-    if constexpr (sizeof...(RS) > 0) ct_run<R, DIR, BFAST, L, R0, NB, NT, HOUT, L, RS...>(s, sb, tw);
+    if constexpr (sizeof...(RS) > 0) {
+        TwOf<R, FirstOf<RS...>::value, R0, L, NB, NT, BFAST, L> nxt;
+        ct_stage_in<R, R0, DIR, BFAST, L, NB, NT, HIN>(s, sb, ld, [&] {
+            if constexpr (tw_mode<R>() == 2) nxt.load(tw);
+        });
+        ct_run<R, DIR, BFAST, L, R0, NB, NT, HOUT, L, decltype(nxt), RS...>(s, sb, tw, nxt);
+    } else {
+        ct_stage_in<R, R0, DIR, BFAST, L, NB, NT, HIN>(s, sb, ld, [] {});
+    }
 }
 
 // ct_fft_in with a hook between the first stage and the others: the first stage
@@ -316,16 +429,25 @@ template <typename R, int DIR, bool BFAST, int L, int NB, int NT, bool HIN, type
           int... RS>
 __device__ __forceinline__ void ct_fft_in_hook(cplx_t<R>* s, int sb, const cplx_t<R>* __restrict__ tw, LD&& ld,
                                                MID&& mid, Radices<R0, RS...>) {
-    ct_stage_in<R, R0, DIR, BFAST, L, NB, NT, HIN>(s, sb, ld);
-    mid();
-    if constexpr (sizeof...(RS) > 0) ct_run<R, DIR, BFAST, L, R0, NB, NT, false, L, RS...>(s, sb, tw);
+    if constexpr (sizeof...(RS) > 0) {
+        TwOf<R, FirstOf<RS...>::value, R0, L, NB, NT, BFAST, L> nxt;
+        ct_stage_in<R, R0, DIR, BFAST, L, NB, NT, HIN>(s, sb, ld, [&] {
+            if constexpr (tw_mode<R>() == 2) nxt.load(tw);
+        });
+        mid();
+        ct_run<R, DIR, BFAST, L, R0, NB, NT, false, L, decltype(nxt), RS...>(s, sb, tw, nxt);
+    } else {
+        ct_stage_in<R, R0, DIR, BFAST, L, NB, NT, HIN>(s, sb, ld, [] {});
+        mid();
+    }
 }
 
 // shared memory -> ... -> last stage -> global (HOUT: only outputs i < L/2 are stored)
 template <typename R, int DIR, bool BFAST, int L, int NB, int NT, bool HOUT = false, typename ST, int... RS>
 __device__ __forceinline__ void ct_fft_out(cplx_t<R>* s, int sb, const cplx_t<R>* __restrict__ tw, ST&& st,
                                            Radices<RS...>) {
-    ct_run_out<R, DIR, BFAST, L, 1, NB, NT, HOUT, L, ST, RS...>(s, sb, tw, st);
+    TwOf<R, FirstOf<RS...>::value, 1, L, NB, NT, BFAST, L> none;
+    ct_run_out<R, DIR, BFAST, L, 1, NB, NT, HOUT, L, ST, decltype(none), RS...>(s, sb, tw, none, st);
 }
 
 // global -> ... -> global; the caller synchronises before s is reused
@@ -356,8 +478,11 @@ __device__ __forceinline__ void ct_fft_io(cplx_t<R>* s, int sb, const cplx_t<R>*
             }
         }
     } else {
-        ct_stage_in<R, R0, DIR, BFAST, L, NB, NT, HIN>(s, sb, ld);
-        ct_run_out<R, DIR, BFAST, L, R0, NB, NT, HOUT, L, ST, RS...>(s, sb, tw, st);
+        TwOf<R, FirstOf<RS...>::value, R0, L, NB, NT, BFAST, L> nxt;
+        ct_stage_in<R, R0, DIR, BFAST, L, NB, NT, HIN>(s, sb, ld, [&] {
+            if constexpr (tw_mode<R>() == 2) nxt.load(tw);
+        });
+        ct_run_out<R, DIR, BFAST, L, R0, NB, NT, HOUT, L, ST, decltype(nxt), RS...>(s, sb, tw, nxt, st);
     }
 }
 
@@ -368,9 +493,12 @@ template <typename R, int DIR, bool BFAST, int L, int NB, int NT, bool HIN, bool
 __device__ __forceinline__ void ct_fft_io_hook(cplx_t<R>* s, int sb, const cplx_t<R>* __restrict__ tw, LD&& ld,
                                                MID&& mid, ST&& st, Radices<R0, RS...>) {
     static_assert(sizeof...(RS) > 0, "a hook needs more than one stage");
-    ct_stage_in<R, R0, DIR, BFAST, L, NB, NT, HIN>(s, sb, ld);
+    TwOf<R, FirstOf<RS...>::value, R0, L, NB, NT, BFAST, L> nxt;
+    ct_stage_in<R, R0, DIR, BFAST, L, NB, NT, HIN>(s, sb, ld, [&] {
+        if constexpr (tw_mode<R>() == 2) nxt.load(tw);
+    });
     mid();
-    ct_run_out<R, DIR, BFAST, L, R0, NB, NT, HOUT, L, ST, RS...>(s, sb, tw, st);
+    ct_run_out<R, DIR, BFAST, L, R0, NB, NT, HOUT, L, ST, decltype(nxt), RS...>(s, sb, tw, nxt, st);
 }
 
 // radix sequence of a compile-time plan as a host array (for the twiddle rows)
@@ -394,6 +522,13 @@ template <> struct CtPlan<512> { using T = Radices<16, 16, 2>; };
 template <> struct CtPlan<1024> { using T = Radices<16, 16, 4>; };
 template <> struct CtPlan<2048> { using T = Radices<16, 16, 8>; };
 template <> struct CtPlan<4096> { using T = Radices<16, 16, 16>; };
+// three times a power of two: the radix-3 stage second (after the pruned radix-16
+// first stage, before an even last stage that output pruning can halve)
+template <> struct CtPlan<96> { using T = Radices<16, 3, 2>; };
+template <> struct CtPlan<192> { using T = Radices<16, 3, 4>; };
+template <> struct CtPlan<384> { using T = Radices<16, 3, 8>; };
+template <> struct CtPlan<768> { using T = Radices<16, 3, 16>; };
+template <> struct CtPlan<1536> { using T = Radices<16, 3, 16, 2>; };
 
 // Radix sequences the autotuner can choose for the column passes: V = 0 the
 // plan above, V = 1 the small radix in the middle (16 R 16) for lengths whose

@@ -201,8 +201,9 @@ __global__ void __launch_bounds__(256) k_local_epi(Geom g, const R* __restrict__
 // Local terms only, in runs of RN consecutive cells along x: the x-inverse's
 // run epilogue with a zero demag contribution (eligibility: run4_eligible).
 // Thread q takes run q of the flattened (row, run) index (fewer than 2^31 runs).
+// FP32: capped for two CTAs per SM (128 registers); FP64 uncapped (it would spill).
 template <typename R, int EPI, int RN>
-__global__ void __launch_bounds__(256) k_local_run(Geom g, const R* __restrict__ m, TermList tl, EpilogueArgs ep,
+__global__ void __launch_bounds__(256, sizeof(R) == 4 ? 2 : 1) k_local_run(Geom g, const R* __restrict__ m, TermList tl, EpilogueArgs ep,
                                                    int nruns) {
     const int runs_row = g.nx / RN;
     R hd[RN][3];

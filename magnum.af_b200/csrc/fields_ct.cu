@@ -1,5 +1,6 @@
 // Demag pass kernels specialised at compile time for power-of-two transform
-// lengths 8..4096 (every configuration of the benchmarks).  Same data flow and
+// lengths 8..4096 and three times a power of two, 96..1536 (every configuration
+// of the benchmarks).  Same data flow and
 // arithmetic as the generic kernels in fields.cu; the transform length, radix
 // sequence, tile width and CTA size are constants, each thread keeps 16
 // complex values in registers per FFT stage, global loads are issued as a
@@ -122,7 +123,9 @@ __global__ void __launch_bounds__(NT) k_xfwd_ct(const R* __restrict__ in, int n_
 // the staging buffer's only reader).  For a scalar Ms, n_in <= LC (zero-padded
 // half pruned) and rows of whole 16-byte chunks; the same arithmetic as k_xfwd_ct.
 template <typename R, int LC, int NB, int NT>
-__global__ void __launch_bounds__(NT, 4) k_xfwd_pipe(const R* __restrict__ in, int n_in, int64_t rows, R ms,
+// (four 256-thread CTAs per SM for power-of-two lengths; three 192-thread CTAs for
+// three times a power of two, whose radix-3 stage holds more values per thread)
+__global__ void __launch_bounds__(NT, (NT % 3 == 0 ? 3 : 4)) k_xfwd_pipe(const R* __restrict__ in, int n_in, int64_t rows, R ms,
                                                   cplx_t<R>* __restrict__ out, int pitch,
                                                   const cplx_t<R>* __restrict__ tw,
                                                   const cplx_t<R>* __restrict__ twP) {
@@ -888,6 +891,11 @@ static void batch_xinv_L(const CtXinvItem<R>* items, const int2* work, int nwork
         case 1024: CALL(1024); return true; \
         case 2048: CALL(2048); return true; \
         case 4096: CALL(4096); return true; \
+        case 96: CALL(96); return true;     \
+        case 192: CALL(192); return true;   \
+        case 384: CALL(384); return true;   \
+        case 768: CALL(768); return true;   \
+        case 1536: CALL(1536); return true; \
         default: return false;              \
     }
 
@@ -929,7 +937,7 @@ bool ct_cols(const cplx_t<R>* in, cplx_t<R>* out, int L, int n_in, int n_out, in
                                     ct_tw<N, V>(tw, f64), tc.cols_pipe, pitch, st)
 #define C2(N, T, HI, HO)               \
     do {                               \
-        if constexpr (N >= 512) {      \
+        if constexpr (N >= 512 && (N & (N - 1)) == 0) {  \
             if (tc.cols_plan)          \
                 C3(N, T, HI, HO, 1);   \
             else                       \
@@ -997,6 +1005,11 @@ bool ct_convy(cplx_t<R>* S, const R* Nred, int ny, int nxh, int pitch, Twiddles&
         case 512: X(512); return true;
         case 1024: X(1024); return true;
         case 2048: X(2048); return true;
+        case 96: X(96); return true;
+        case 192: X(192); return true;
+        case 384: X(384); return true;
+        case 768: X(768); return true;
+        case 1536: X(1536); return true;
         default: return false;
     }
 #undef X
@@ -1026,12 +1039,18 @@ bool ct_xinv(const cplx_t<R>* S1, int pitch, int Px, Twiddles& tw, const Geom& g
         case 512: X(512); return true;
         case 1024: X(1024); return true;
         case 2048: X(2048); return true;
+        case 96: X(96); return true;
+        case 192: X(192); return true;
+        case 384: X(384); return true;
+        case 768: X(768); return true;
+        case 1536: X(1536); return true;
         default: return false;
     }
 #undef X
 }
 
-// lengths of the batched kernels: x passes L = Px / 2 and y convolution L = Py, 16..2048
+// lengths of the batched kernels: x passes L = Px / 2 and y convolution L = Py in 16..2048 (powers of two)
+// and 96..1536 (three times a power of two)
 #define MAF_CT_BATCH_SWITCH(L, CALL)  \
     switch (L) {                      \
         case 16: CALL(16); break;     \
@@ -1042,6 +1061,11 @@ bool ct_xinv(const cplx_t<R>* S1, int pitch, int Px, Twiddles& tw, const Geom& g
         case 512: CALL(512); break;   \
         case 1024: CALL(1024); break; \
         case 2048: CALL(2048); break; \
+        case 96: CALL(96); break;     \
+        case 192: CALL(192); break;   \
+        case 384: CALL(384); break;   \
+        case 768: CALL(768); break;   \
+        case 1536: CALL(1536); break; \
         default: break;               \
     }
 
