@@ -265,7 +265,17 @@ def main():
                     help="comma-separated dilation per layer ('' for none)")
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--out", default=None)
+    ap.add_argument("--gain", type=int, default=0, metavar="N",
+                    help="only evaluate the pretrained 128 x 128 U-net on N held-out samples (seed --gain-seed)")
+    ap.add_argument("--gain-seed", type=int, default=50_000)
     a = ap.parse_args()
+    if a.gain:
+        res = gain(pretrained_unet(), a.gain, 128, 128, seed=a.gain_seed)
+        print(json.dumps(res), flush=True)
+        if a.out:
+            with open(a.out, "w") as f:
+                f.write(json.dumps(res) + "\n")
+        return
     t0 = time.perf_counter()
     ranges = PARAM_RANGES_128 if a.config128 else None
     train_set = generate(a.n_train, a.mesh[0], a.mesh[1], a.seed, maxiter=a.maxiter, ranges=ranges,
