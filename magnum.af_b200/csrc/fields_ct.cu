@@ -343,6 +343,35 @@ __global__ void __launch_bounds__(NT, (kMinBlocks<R, NT, 768, 512>)) k_convz_ct(
     ct_fft_out<R, 1, true, L, NC, NT, true>(s, 0, tw, st, typename CtPlan<L>::T());
 }
 
+// ------------------------------------------- z-transform twiddles as constants
+// cos(pi k / 64) for k = 0 .. 32 (21 digits, from the Taylor series of cos
+// evaluated in 50-digit decimal arithmetic).
+__host__ __device__ constexpr double cos_pi64(int k) {
+    constexpr double t[33] = {
+        1.000000000000000000000, 0.998795456205172392715, 0.995184726672196886245, 0.989176509964780973452,
+        0.980785280403230449126, 0.970031253194543992604, 0.956940335732208864936, 0.941544065183020778413,
+        0.923879532511286756128, 0.903989293123443331586, 0.881921264348355029713, 0.857728610000272069902,
+        0.831469612302545237079, 0.803207531480644909807, 0.773010453362736960811, 0.740951125354959091176,
+        0.707106781186547524401, 0.671558954847018400625, 0.634393284163645498215, 0.595699304492433343467,
+        0.555570233019602224743, 0.514102744193221726594, 0.471396736825997648556, 0.427555093430282094321,
+        0.382683432365089771728, 0.336889853392220050689, 0.290284677254462367636, 0.242980179903263889948,
+        0.195090322016128267848, 0.146730474455361751659, 0.098017140329560601994, 0.049067674327418014255,
+        0.0,
+    };
+    return t[k];
+}
+
+// W_{2 NZ}^n = exp(-i pi n / NZ) (the forward sign) for n < NZ, NZ a divisor of
+// 64: with n a compile-time constant (an unrolled loop) the value is an
+// immediate operand, no table load.
+template <typename R, int NZ> __device__ __forceinline__ cplx_t<R> wz_const(int n) {
+    static_assert(64 % NZ == 0, "NZ divides 64");
+    const int k = n * (64 / NZ);  // angle pi k / 64, 0 <= k < 64
+    const double c = k <= 32 ? cos_pi64(k) : -cos_pi64(64 - k);
+    const double s = k <= 32 ? cos_pi64(32 - k) : cos_pi64(k - 32);
+    return mk((R)c, (R)-s);
+}
+
 // ------------------------------ z convolution, transforms in registers (nz <= 16)
 // Same tile as k_convz_ct, one thread per column (row, comp, b).  The zero-padded
 // length-L (= 2 nz) transform is two length-nz DFTs held in registers:
@@ -400,8 +429,13 @@ __global__ void __launch_bounds__(6 * NB, (kMinBlocks<R, 6 * NB, 576, 288>))
         C e[NZ], o[NZ];
 #pragma unroll
         for (int n = 0; n < NZ; ++n) e[n] = ok ? src[n * si] : mk((R)0, (R)0);
+        // the twiddles W_L^n: immediates in FP32, the correctly rounded table in FP64
+        auto wz = [&](int n) -> C {
+            if constexpr (sizeof(R) == 4) return wz_const<R, NZ>(n);
+            else return tw[n];
+        };
 #pragma unroll
-        for (int n = 0; n < NZ; ++n) o[n] = cmul(e[n], tw[n]);
+        for (int n = 0; n < NZ; ++n) o[n] = cmul(e[n], wz(n));
         bfly_ct<NZ, -1, R>(e);
         bfly_ct<NZ, -1, R>(o);
 #pragma unroll
@@ -451,7 +485,12 @@ __global__ void __launch_bounds__(6 * NB, (kMinBlocks<R, 6 * NB, 576, 288>))
         if (ok) {
             C* dst = S + comp * cs + (int64_t)(row ? Py - ky : ky) * pitch + c0 + b;
 #pragma unroll
-            for (int n = 0; n < NZ; ++n) dst[n * si] = cadd(e[n], cmulc(o[n], tw[n]));
+            for (int n = 0; n < NZ; ++n) {
+                C w;
+                if constexpr (sizeof(R) == 4) w = wz_const<R, NZ>(n);
+                else w = tw[n];
+                dst[n * si] = cadd(e[n], cmulc(o[n], w));
+            }
         }
     }
 }
