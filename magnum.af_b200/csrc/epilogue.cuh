@@ -200,6 +200,8 @@ __device__ __forceinline__ void runN_load(const R* __restrict__ m, const Geom& g
 //   cubic     q = -2Kc1/(mu0 Ms), -2Kc2/(mu0 Ms), -4Kc3/(mu0 Ms)
 template <typename R, int N>
 __device__ __forceinline__ void runN_fields(const TermList& tl, const RunN<R, N>& r, const R hd[N][3], R h[N][3]) {
+    // FP32: the constants come pre-rounded (TermDesc::qf), the same values as a device-side rounding
+    constexpr bool kF32 = sizeof(R) == 4;
 #pragma unroll
     for (int i = 0; i < N; ++i) h[i][0] = h[i][1] = h[i][2] = 0;
     for (int it = 0; it < tl.n; ++it) {
@@ -210,7 +212,8 @@ __device__ __forceinline__ void runN_fields(const TermList& tl, const RunN<R, N>
                 for (int i = 0; i < N; ++i) { h[i][0] += hd[i][0]; h[i][1] += hd[i][1]; h[i][2] += hd[i][2]; }
                 break;
             case TK_EXCHANGE: {
-                const R qx = (R)t.q[0], qy = (R)t.q[1], qz = (R)t.q[2];
+                const R qx = kF32 ? (R)t.qf[0] : (R)t.q[0], qy = kF32 ? (R)t.qf[1] : (R)t.q[1];
+                const R qz = kF32 ? (R)t.qf[2] : (R)t.q[2];
 #pragma unroll
                 for (int c = 0; c < 3; ++c) {
 #pragma unroll
@@ -226,8 +229,10 @@ __device__ __forceinline__ void runN_fields(const TermList& tl, const RunN<R, N>
                 break;
             }
             case TK_DMI: {
-                const R coef = (R)t.q[0], hx = (R)t.q[1], hy = (R)t.q[2], hz = (R)t.q[3];
-                const R n0 = (R)t.p[1], n1 = (R)t.p[2], n2 = (R)t.p[3];
+                const R coef = kF32 ? (R)t.qf[0] : (R)t.q[0], hx = kF32 ? (R)t.qf[1] : (R)t.q[1];
+                const R hy = kF32 ? (R)t.qf[2] : (R)t.q[2], hz = kF32 ? (R)t.qf[3] : (R)t.q[3];
+                const R n0 = kF32 ? (R)t.qf[4] : (R)t.p[1], n1 = kF32 ? (R)t.qf[5] : (R)t.p[2];
+                const R n2 = kF32 ? (R)t.qf[6] : (R)t.p[3];
                 auto nm = [&](const R v0, const R v1, const R v2) { return n0 * v0 + n1 * v1 + n2 * v2; };
 #pragma unroll
                 for (int i = 0; i < N; ++i) {
@@ -248,8 +253,9 @@ __device__ __forceinline__ void runN_fields(const TermList& tl, const RunN<R, N>
                 break;
             }
             case TK_UNIAXIAL: {
-                const R e0 = (R)t.p[1], e1 = (R)t.p[2], e2 = (R)t.p[3];
-                const R coef = (R)t.q[0];
+                const R e0 = kF32 ? (R)t.qf[1] : (R)t.p[1], e1 = kF32 ? (R)t.qf[2] : (R)t.p[2];
+                const R e2 = kF32 ? (R)t.qf[3] : (R)t.p[3];
+                const R coef = kF32 ? (R)t.qf[0] : (R)t.q[0];
 #pragma unroll
                 for (int i = 0; i < N; ++i) {
                     const R em = coef * (e0 * r.c[0][i] + e1 * r.c[1][i] + e2 * r.c[2][i]);
@@ -260,10 +266,15 @@ __device__ __forceinline__ void runN_fields(const TermList& tl, const RunN<R, N>
                 break;
             }
             case TK_CUBIC: {
-                const R c1[3] = {(R)t.p[3], (R)t.p[4], (R)t.p[5]};
-                const R c2[3] = {(R)t.p[6], (R)t.p[7], (R)t.p[8]};
-                const R c3[3] = {(R)t.p[9], (R)t.p[10], (R)t.p[11]};
-                const R k1 = (R)t.q[0], k2 = (R)t.q[1], k3 = (R)t.q[2];
+                R c1[3], c2[3], c3[3];
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    c1[c] = kF32 ? (R)t.qf[3 + c] : (R)t.p[3 + c];
+                    c2[c] = kF32 ? (R)t.qf[6 + c] : (R)t.p[6 + c];
+                    c3[c] = kF32 ? (R)t.qf[9 + c] : (R)t.p[9 + c];
+                }
+                const R k1 = kF32 ? (R)t.qf[0] : (R)t.q[0], k2 = kF32 ? (R)t.qf[1] : (R)t.q[1];
+                const R k3 = kF32 ? (R)t.qf[2] : (R)t.q[2];
 #pragma unroll
                 for (int i = 0; i < N; ++i) {
                     const R m0 = r.c[0][i], m1 = r.c[1][i], m2 = r.c[2][i];
@@ -281,7 +292,8 @@ __device__ __forceinline__ void runN_fields(const TermList& tl, const RunN<R, N>
                 break;
             }
             case TK_ZEEMAN: {
-                const R z0 = (R)t.p[0], z1 = (R)t.p[1], z2 = (R)t.p[2];
+                const R z0 = kF32 ? (R)t.qf[0] : (R)t.p[0], z1 = kF32 ? (R)t.qf[1] : (R)t.p[1];
+                const R z2 = kF32 ? (R)t.qf[2] : (R)t.p[2];
 #pragma unroll
                 for (int i = 0; i < N; ++i) { h[i][0] += z0; h[i][1] += z1; h[i][2] += z2; }
                 break;
@@ -404,6 +416,29 @@ inline void prepare_run4(TermList& tl, const Geom& g, double Ms) {
                 t.q[0] = -2.0 * t.p[0] / mu0Ms;
                 t.q[1] = -2.0 * t.p[1] / mu0Ms;
                 t.q[2] = -4.0 * t.p[2] / mu0Ms;
+                break;
+            default: break;
+        }
+        // FP32 copies in the order runN_fields reads them
+        auto f = [](double v) { return (float)v; };
+        switch (t.kind) {
+            case TK_EXCHANGE:
+                for (int k = 0; k < 3; ++k) t.qf[k] = f(t.q[k]);
+                break;
+            case TK_DMI:
+                for (int k = 0; k < 4; ++k) t.qf[k] = f(t.q[k]);
+                for (int k = 0; k < 3; ++k) t.qf[4 + k] = f(t.p[1 + k]);
+                break;
+            case TK_UNIAXIAL:
+                t.qf[0] = f(t.q[0]);
+                for (int k = 0; k < 3; ++k) t.qf[1 + k] = f(t.p[1 + k]);
+                break;
+            case TK_CUBIC:
+                for (int k = 0; k < 3; ++k) t.qf[k] = f(t.q[k]);
+                for (int k = 3; k < 12; ++k) t.qf[k] = f(t.p[k]);
+                break;
+            case TK_ZEEMAN:
+                for (int k = 0; k < 3; ++k) t.qf[k] = f(t.p[k]);
                 break;
             default: break;
         }

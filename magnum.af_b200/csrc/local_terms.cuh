@@ -37,6 +37,7 @@ struct TermDesc {
     int kind = TK_DEMAG;
     double p[12] = {};          // kind-specific parameters (see make_* in field.cu)
     double q[4] = {};           // per-launch constants of the fast run epilogue (prepare_run4)
+    float qf[16] = {};          // the run epilogue's constants rounded to FP32 once on the host (prepare_run4)
     const double* f0 = nullptr;  // optional per-cell scalar field (Ku1, D) or vector field (Zeeman) [3][N]
     const double* f1 = nullptr;  // optional per-cell axis field [3][N]
 };

@@ -258,7 +258,7 @@ class State:
                                      float("nan"), _dptr(msf), _dptr(mf), prec))
 
     def __del__(self):
-        if getattr(self, "_h", None) and getattr(self, "_owned", True):
+        if getattr(self, "_h", None) and getattr(self, "_owned", True) and lib is not None:
             lib.maf_state_destroy(self._h)
         self._h = None
 
@@ -385,7 +385,7 @@ class FieldTerm:
     _h = None
 
     def __del__(self):
-        if getattr(self, "_h", None):
+        if getattr(self, "_h", None) and lib is not None:
             lib.maf_term_destroy(self._h)
             self._h = None
 
@@ -701,7 +701,7 @@ class LLGIntegrator:
                                    mode.encode(), hmin, hmax, atol, rtol, int(bool(dissipation_term_only))))
 
     def __del__(self):
-        if getattr(self, "_h", None):
+        if getattr(self, "_h", None) and lib is not None:
             lib.maf_llg_destroy(self._h)
             self._h = None
 
@@ -876,7 +876,7 @@ class LBFGS_Minimizer:
         _ck(lib.maf_lbfgs_create(C.byref(self._h), arr, len(self._terms), float(tol), int(maxiter)))
 
     def __del__(self):
-        if getattr(self, "_h", None):
+        if getattr(self, "_h", None) and lib is not None:
             lib.maf_lbfgs_destroy(self._h)
             self._h = None
 
@@ -914,7 +914,7 @@ class ConvNet:
             self.dilation = d
 
     def __del__(self):
-        if getattr(self, "_h", None):
+        if getattr(self, "_h", None) and lib is not None:
             lib.maf_cnn_destroy(self._h)
             self._h = None
 
@@ -979,7 +979,7 @@ class StochasticBatch:
         return bool(v.value)
 
     def __del__(self):
-        if getattr(self, "_h", None):
+        if getattr(self, "_h", None) and lib is not None:
             lib.maf_stoch_batch_destroy(self._h)
             self._h = None
 
@@ -1012,7 +1012,7 @@ class StringMethod:
         self.n_interp = int(n_interp)
 
     def __del__(self):
-        if getattr(self, "_h", None):
+        if getattr(self, "_h", None) and lib is not None:
             lib.maf_string_destroy(self._h)
             self._h = None
 
@@ -1073,7 +1073,7 @@ class Stochastic_LLG:
                                           str(smode).encode(), int(seed), int(member)))
 
     def __del__(self):
-        if getattr(self, "_h", None):
+        if getattr(self, "_h", None) and lib is not None:
             lib.maf_stochastic_llg_destroy(self._h)
             self._h = None
 
