@@ -202,9 +202,11 @@ int maf_llg_heff_pipeline_m32(maf_llg l, maf_state s, const float* const* m_host
  * up to rounding. */
 int maf_llg_autotune(maf_llg l, maf_state s, int reps, int choices[3], double* pass_ms);
 /* The autotuner's full search: four configurations of the passes are timed (defaults; all alternatives;
- * and two mixed ones), and the y passes' column tile, pipelining and radix sequence (16 16 R or 16 R 16)
- * are chosen jointly, the z convolution and the x-inverse run length per pass.  choices[5] = {cols_wide,
- * convz_reg, xinv_run, cols_pipe, cols_plan}; pass_ms (optional) receives 4 x 5 per-pass times; the
+ * and two mixed ones); the y passes' column tile is chosen for both, then the forward pass's pipelining
+ * and radix sequence and the inverse pass's radix sequence each from the configurations with that tile,
+ * the z convolution and the x-inverse run length per pass.  choices[5] = {cols_wide, convz_reg, xinv_run,
+ * cols_pipe, cols_plan}, cols_plan: 0 both y passes 16 16 R, 1 both 16 R 16, 2 the inverse only, 3 the
+ * forward only; pass_ms (optional) receives 4 x 5 per-pass times; the
  * result is cached per (mesh, precision, term kinds) for the process, and *cached (optional) reports a
  * cache hit (no timing then). */
 int maf_llg_autotune_ex(maf_llg l, maf_state s, int reps, int choices[5], double* pass_ms, int* cached);

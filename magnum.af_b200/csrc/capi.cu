@@ -1651,12 +1651,27 @@ int maf_llg_autotune_ex(maf_llg l, maf_state s, int reps, int choices[5], double
                 for (int c = 0; c < 4; ++c) t[c] = run(cfg[c]);
                 best = cfg[0];
                 if (st.md.nz > 1 && t[0].size() == 5) {
-                    int by = 0;  // y passes: the whole (tile, pipelining, plan) triple of the fastest configuration
-                    for (int c = 1; c < 4; ++c)
-                        if (t[c].size() == 5 && t[c][1] + t[c][3] < t[by][1] + t[by][3]) by = c;
-                    best.cols_wide = cfg[by].cols_wide;
-                    best.cols_pipe = cfg[by].cols_pipe;
-                    best.cols_plan = cfg[by].cols_plan;
+                    // y passes: per column tile width (shared by both passes), the fastest
+                    // forward (pipelining, plan) and the fastest inverse plan among the
+                    // configurations with that width; then the faster width
+                    double best_y = 0;
+                    for (int wide = 0; wide < 2; ++wide) {
+                        int bf = -1, bi = -1;
+                        for (int c = 0; c < 4; ++c) {
+                            if (cfg[c].cols_wide != wide || t[c].size() != 5) continue;
+                            if (bf < 0 || t[c][1] < t[bf][1]) bf = c;
+                            if (bi < 0 || t[c][3] < t[bi][3]) bi = c;
+                        }
+                        if (bf < 0) continue;
+                        const double ty = t[bf][1] + t[bi][3];
+                        if (wide == 0 || ty < best_y) {
+                            best_y = ty;
+                            best.cols_wide = wide;
+                            best.cols_pipe = cfg[bf].cols_pipe;
+                            const bool pf = cfg[bf].cols_plan == 1, pi = cfg[bi].cols_plan == 1;
+                            best.cols_plan = pf && pi ? 1 : pf ? 3 : pi ? 2 : 0;
+                        }
+                    }
                     best.convz_reg = (t[0][2] + t[2][2]) <= (t[1][2] + t[3][2]) ? 1 : 0;
                     best.xinv_run = (t[0][4] + t[2][4]) <= (t[1][4] + t[3][4]) ? 2 : 4;
                 } else if (t[0].size() == 3) {
@@ -1715,8 +1730,8 @@ int maf_term_demag_set_tune_ex(maf_term t, const int choices[5]) {
               "maf_term_demag_set_tune_ex: not a DemagField");
         check((choices[0] == 0 || choices[0] == 1) && (choices[1] == 0 || choices[1] == 1) &&
                   (choices[2] == 0 || choices[2] == 2 || choices[2] == 4) && (choices[3] == 0 || choices[3] == 1) &&
-                  (choices[4] == 0 || choices[4] == 1),
-              "maf_term_demag_set_tune_ex: choices are {0|1, 0|1, 0|2|4, 0|1, 0|1}");
+                  (choices[4] >= 0 && choices[4] <= 3),
+              "maf_term_demag_set_tune_ex: choices are {0|1, 0|1, 0|2|4, 0|1, 0..3}");
         TuneChoice& c = t->t->demag->tune;
         c.cols_wide = choices[0];
         c.convz_reg = choices[1];

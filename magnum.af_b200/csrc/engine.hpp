@@ -135,7 +135,8 @@ struct TuneChoice {
     int convz_reg = 1;
     int xinv_run = 0;
     int cols_pipe = 1;  // forward y pass: persistent kernel staging the next tile's input (cp.async)
-    int cols_plan = 0;  // y passes: radix sequence 16 16 R (0) or 16 R 16 (1)
+    int cols_plan = 0;  // y passes' radix sequences: 0 both 16 16 R, 1 both 16 R 16, 2 inverse only 16 R 16,
+                        // 3 forward only 16 R 16
     int generic = 0;    // 1: the run-time-plan kernels for every pass (as the batched passes run)
 };
 

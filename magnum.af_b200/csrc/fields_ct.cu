@@ -971,13 +971,16 @@ bool ct_cols(const cplx_t<R>* in, cplx_t<R>* out, int L, int n_in, int n_out, in
     // the row stride bounds the column tiles the pipelined kernel copies whole
     const int pitch = (int)std::min<int64_t>(in_si, 1 << 30);
     if (!hin && !hout && !f64) return false;
+    // radix plan of this pass (TuneChoice::cols_plan: 0 both 16 16 R, 1 both 16 R 16,
+    // 2 only the inverse pass 16 R 16, 3 only the forward pass 16 R 16)
+    const bool alt = DIR < 0 ? (tc.cols_plan == 1 || tc.cols_plan == 3) : (tc.cols_plan == 1 || tc.cols_plan == 2);
 #define C3(N, T, HI, HO, V)                                                                                \
     cols_L<R, DIR, N, T, HI, HO, V>(in, out, n_in, n_out, ncols, in_si, out_si, in_sbat, out_sbat, nbat,     \
                                     ct_tw<N, V>(tw, f64), tc.cols_pipe, pitch, st)
 #define C2(N, T, HI, HO)               \
     do {                               \
         if constexpr (N >= 512 && (N & (N - 1)) == 0) {  \
-            if (tc.cols_plan)          \
+            if (alt)                   \
                 C3(N, T, HI, HO, 1);   \
             else                       \
                 C3(N, T, HI, HO, 0);   \

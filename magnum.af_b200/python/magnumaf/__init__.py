@@ -514,7 +514,8 @@ class DemagField(FieldTerm):
 
     @property
     def tune_ex(self):
-        """All kernel choices: (cols_wide, convz_reg, xinv_run, cols_pipe, cols_plan)."""
+        """All kernel choices: (cols_wide, convz_reg, xinv_run, cols_pipe, cols_plan); cols_plan 0: both
+        y passes radix 16 16 R, 1: both 16 R 16, 2: the inverse only, 3: the forward only."""
         ch = (_I * 5)()
         _ck(lib.maf_term_demag_get_tune_ex(self._h, ch))
         return tuple(ch)

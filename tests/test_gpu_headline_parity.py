@@ -57,7 +57,8 @@ def _case(shape, seed):
 
 # (cols_wide, convz_reg, xinv_run, cols_pipe, cols_plan): the defaults first, then
 # every alternative of each pass
-VARIANTS = [(0, 1, 2, 1, 0), (1, 1, 2, 1, 0), (0, 0, 4, 1, 0), (1, 0, 4, 0, 1), (0, 1, 2, 0, 1), (0, 1, 2, 1, 1)]
+VARIANTS = [(0, 1, 2, 1, 0), (1, 1, 2, 1, 0), (0, 0, 4, 1, 0), (1, 0, 4, 0, 1), (0, 1, 2, 0, 1), (0, 1, 2, 1, 1),
+            (0, 1, 2, 1, 2), (0, 1, 2, 0, 3)]
 
 
 @pytest.mark.parametrize("shape", [(1024, 1024, 2), (256, 256, 16)])
