@@ -827,6 +827,8 @@ def main():
     ap.add_argument("--warm-start-samples", type=int, default=16, help="held-out samples of the warm-start gain")
     ap.add_argument("--kernel-sweep", action="store_true",
                     help="launch every kernel family once or twice (for profiler captures) and exit")
+    ap.add_argument("--ensemble-only", action="store_true",
+                    help="time only the batched 64-member Heun ensemble (--heun-steps steps; for profiler captures)")
     ap.add_argument("--mesh", type=int, nargs=3, default=None, metavar=("NX", "NY", "NZ"),
                     help="smaller mesh for profiling captures (the reported metric is defined at 1024 1024 16)")
     args = ap.parse_args()
@@ -837,6 +839,10 @@ def main():
         run_reference(args)
     elif args.kernel_sweep:
         kernel_sweep(args)
+    elif args.ensemble_only:
+        import magnumaf as M
+
+        print(json.dumps({"heun_ensemble_64": heun_ensemble(M, args.heun_steps, fused_only=True)}), flush=True)
     else:
         run_ours(args)
 
