@@ -592,6 +592,8 @@ struct maf_lbfgs_s {
     double tolerance = 1e-6;
     size_t maxIter = 230;
     DevBuf sV[5], yV[5], q, s, y, grad, grad_old, x_old, wa, red;
+    DevBuf coef;           // device scalars: alpha[5] of the two-loop recursion, its current dot product, 3 more
+    double rho[5] = {};    // 1 / (s . y) of each stored pair
     unsigned long long fevals = 0, iterations = 0;
     double last_gradnorm = 0;
 };
@@ -797,6 +799,14 @@ double lbfgs_minimize(maf_lbfgs_s* h, maf_state_s* st) {
         h->yV[i].ensure(sizeof(double) * n3);
     }
     h->red.ensure(sizeof(double) * (red_blocks() + 8));
+    h->coef.ensure(sizeof(double) * 10);
+    double* alpha_d = h->coef.as<double>();  // alpha[0..4]
+    double* dot_d = alpha_d + 5;             // the dot product of the current recursion step
+    double* trio_d = alpha_d + 6;            // up to three reductions read back with one synchronisation
+    auto read_back = [&](int k, double* out) {
+        MAF_CUDA(cudaMemcpyAsync(out, trio_d, sizeof(double) * k, cudaMemcpyDeviceToHost, S.stream));
+        MAF_CUDA(cudaStreamSynchronize(S.stream));
+    };
     LbfgsCtx c{h, st, n3, S.md.N(), S.stream};
     const double eps = 2.22e-16, eps2 = std::sqrt(eps), epsr = std::pow(eps, 0.9);
     const double tolf2 = std::sqrt(h->tolerance), tolf3 = std::pow(h->tolerance, 0.3333333333333333333333333);
@@ -806,7 +816,6 @@ double lbfgs_minimize(maf_lbfgs_s* h, maf_state_s* st) {
     h->last_gradnorm = gradNorm;
     if (gradNorm < (epsr * (1 + std::fabs(f)))) return f;
     const size_t m = 5;
-    double alpha[5] = {0, 0, 0, 0, 0};
     size_t iter = 0, globIter = 0;
     double H0k = 1;
     int order[5] = {0, 1, 2, 3, 4};  // logical slot -> buffer (std::rotate of the reference)
@@ -816,20 +825,24 @@ double lbfgs_minimize(maf_lbfgs_s* h, maf_state_s* st) {
         MAF_CUDA(cudaMemcpyAsync(h->grad_old.p, h->grad.p, sizeof(double) * n3, cudaMemcpyDeviceToDevice, S.stream));
         MAF_CUDA(cudaMemcpyAsync(h->q.p, h->grad.p, sizeof(double) * n3, cudaMemcpyDeviceToDevice, S.stream));
         const int k = (int)std::min(m, iter);
+        // the two-loop recursion stays on the device: alpha_i = rho_i (s_i . q) and
+        // beta = rho_i (y_i . q) are formed by the kernels that use them, with the
+        // host arithmetic's operations in the same order (rho_i = 1 / (s_i . y_i)
+        // is kept from when the pair was stored: the same value as recomputing it)
         for (int i = k - 1; i >= 0; --i) {
             const DevBuf& sv = h->sV[order[i]];
             const DevBuf& yv = h->yV[order[i]];
-            const double rho = 1.0 / c.dot(sv, yv);
-            alpha[i] = rho * c.dot(sv, h->q);
-            axpby(h->q.as<double>(), 1.0, h->q.as<double>(), -alpha[i], yv.as<double>(), n3, S.stream);
+            dot_dev(sv.as<double>(), h->q.as<double>(), n3, c.red(), dot_d, S.stream);
+            axpby_rho(h->q.as<double>(), yv.as<double>(), dot_d, h->rho[order[i]], nullptr, alpha_d + i, n3,
+                      S.stream);
         }
         axpby(h->q.as<double>(), H0k, h->q.as<double>(), 0.0, nullptr, n3, S.stream);
         for (int i = 0; i < k; ++i) {
             const DevBuf& sv = h->sV[order[i]];
             const DevBuf& yv = h->yV[order[i]];
-            const double rho = 1.0 / c.dot(sv, yv);
-            const double beta = rho * c.dot(yv, h->q);
-            axpby(h->q.as<double>(), 1.0, h->q.as<double>(), alpha[i] - beta, sv.as<double>(), n3, S.stream);
+            dot_dev(yv.as<double>(), h->q.as<double>(), n3, c.red(), dot_d, S.stream);
+            axpby_rho(h->q.as<double>(), sv.as<double>(), dot_d, h->rho[order[i]], alpha_d + i, nullptr, n3,
+                      S.stream);
         }
         const double phiPrime0 = -c.dot(h->grad, h->q);
         if (phiPrime0 > 0) {
@@ -848,12 +861,20 @@ double lbfgs_minimize(maf_lbfgs_s* h, maf_state_s* st) {
             return f;
         }
         axpby(h->s.as<double>(), 1.0, S.m64.as<double>(), -1.0, h->x_old.as<double>(), n3, S.stream);
-        const double smax = c.maxabs(h->s.as<double>());
-        const double mmax = c.maxabs(S.m64.as<double>());
+        double mx[2];
+        reduce_dev(h->s.as<double>(), nullptr, n3, 1, c.red(), trio_d, S.stream);
+        reduce_dev(S.m64.as<double>(), nullptr, n3, 1, c.red(), trio_d + 1, S.stream);
+        read_back(2, mx);
+        const double smax = mx[0], mmax = mx[1];
         if (((f_old - f) < (h->tolerance * f1)) && (smax < (tolf2 * (1 + mmax))) && (gradNorm <= (tolf3 * f1))) break;
         axpby(h->y.as<double>(), 1.0, h->grad.as<double>(), -1.0, h->grad_old.as<double>(), n3, S.stream);
-        const double ys = c.dot(h->y, h->s);
-        if (ys <= eps2 * std::sqrt(c.dot(h->y, h->y)) * std::sqrt(c.dot(h->s, h->s))) {
+        double d3[3];
+        dot_dev(h->y.as<double>(), h->s.as<double>(), n3, c.red(), trio_d, S.stream);
+        dot_dev(h->y.as<double>(), h->y.as<double>(), n3, c.red(), trio_d + 1, S.stream);
+        dot_dev(h->s.as<double>(), h->s.as<double>(), n3, c.red(), trio_d + 2, S.stream);
+        read_back(3, d3);
+        const double ys = d3[0], yy = d3[1];
+        if (ys <= eps2 * std::sqrt(yy) * std::sqrt(d3[2])) {
             // Dennis, Schnabel 9.4.1: skip the update
         } else {
             int slot;
@@ -867,7 +888,8 @@ double lbfgs_minimize(maf_lbfgs_s* h, maf_state_s* st) {
             }
             MAF_CUDA(cudaMemcpyAsync(h->sV[slot].p, h->s.p, sizeof(double) * n3, cudaMemcpyDeviceToDevice, S.stream));
             MAF_CUDA(cudaMemcpyAsync(h->yV[slot].p, h->y.p, sizeof(double) * n3, cudaMemcpyDeviceToDevice, S.stream));
-            H0k = ys / c.dot(h->y, h->y);
+            h->rho[slot] = 1.0 / ys;  // = 1 / (s . y): the products commute exactly, same partial-sum order
+            H0k = ys / yy;
             iter++;
         }
         globIter++;

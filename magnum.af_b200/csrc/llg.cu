@@ -449,6 +449,19 @@ double dot_host(const double* a, const double* b, int64_t n, double* scratch, cu
     return reduce_host(a, b, n, 0, scratch, st);
 }
 
+void reduce_dev(const double* a, const double* b, int64_t n, int mode, double* scratch, double* out, cudaStream_t st) {
+    const int nred = red_blocks();
+    const int blocks = (int)std::min<int64_t>(ceil_div(n, 256), nred);
+    k_red_partials<<<blocks, 256, 0, st>>>(a, b, n, mode, scratch);
+    MAF_LAUNCH_CHECK();
+    k_red_final<<<1, 32, 0, st>>>(scratch, blocks, mode, out);
+    MAF_LAUNCH_CHECK();
+}
+
+void dot_dev(const double* a, const double* b, int64_t n, double* scratch, double* out, cudaStream_t st) {
+    reduce_dev(a, b, n, 0, scratch, out, st);
+}
+
 double maxabs_host(const double* a, int64_t n, double* scratch, cudaStream_t st) {
     return reduce_host(a, nullptr, n, 1, scratch, st);
 }
@@ -490,6 +503,27 @@ __global__ void k_axpby(double* out, double a, const double* x, double b, const 
 void axpby(double* out, double a, const double* x, double b, const double* y, int64_t n, cudaStream_t st) {
     const int64_t blocks = std::min<int64_t>(ceil_div(n, 256), (int64_t)sm_count() * 16);
     k_axpby<<<(unsigned)blocks, 256, 0, st>>>(out, a, x, b, y, n);
+    MAF_LAUNCH_CHECK();
+}
+
+// k_axpby with a = 1 and the coefficient formed on the device from the dot
+// product *d (every thread forms the same value)
+__global__ void k_axpby_rho(double* q, const double* __restrict__ y, const double* __restrict__ d, double rho,
+                            const double* __restrict__ alpha_in, double* __restrict__ alpha_out, int64_t n) {
+    const double t = rho * *d;
+    const double b = alpha_in ? *alpha_in - t : -t;
+    if (alpha_out && blockIdx.x == 0 && threadIdx.x == 0) *alpha_out = t;
+    const double a = 1.0;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double v = a * q[i];
+        q[i] = v + b * y[i];
+    }
+}
+
+void axpby_rho(double* q, const double* y, const double* d, double rho, const double* alpha_in, double* alpha_out,
+               int64_t n, cudaStream_t st) {
+    const int64_t blocks = std::min<int64_t>(ceil_div(n, 256), (int64_t)sm_count() * 16);
+    k_axpby_rho<<<(unsigned)blocks, 256, 0, st>>>(q, y, d, rho, alpha_in, alpha_out, n);
     MAF_LAUNCH_CHECK();
 }
 

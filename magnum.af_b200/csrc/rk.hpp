@@ -27,6 +27,15 @@ int red_blocks();
 double dot_host(const double* a, const double* b, int64_t n, double* scratch, cudaStream_t st);
 double maxabs_host(const double* a, int64_t n, double* scratch, cudaStream_t st);
 void axpby(double* out, double a, const double* x, double b, const double* y, int64_t n, cudaStream_t st);
+// Device-resident steps of the LBFGS two-loop recursion (no host synchronisation):
+// *out = a . b (the same partial sums and order as dot_host), and
+// q = 1 q + c y with c = -(rho *d) (alpha_out: t = rho *d, written by one thread)
+// or c = *alpha_in - rho *d -- the arithmetic of axpby with a host coefficient.
+void dot_dev(const double* a, const double* b, int64_t n, double* scratch, double* out, cudaStream_t st);
+// reduce_host's mode (0 dot, 1 NaN-propagating max |a|, 2 squared difference) into a device scalar
+void reduce_dev(const double* a, const double* b, int64_t n, int mode, double* scratch, double* out, cudaStream_t st);
+void axpby_rho(double* q, const double* y, const double* d, double rho, const double* alpha_in, double* alpha_out,
+               int64_t n, cudaStream_t st);
 void normalize_combine(double* m, const double* wa, double stp, const double* s, int64_t N, cudaStream_t st);
 // string method: sum (a-b)^2 over n values (synchronises), out = a + (c1 (b - a)) / c2
 double sqdiff_host(const double* a, const double* b, int64_t n, double* scratch, cudaStream_t st);
