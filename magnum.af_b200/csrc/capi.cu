@@ -612,6 +612,28 @@ struct LbfgsCtx {
     double maxabs(const double* a) const { return maxabs_host(a, n3, red(), stream); }
 };
 
+// EnergyAndGradient of the state's current m and the directional derivative g . s,
+// read back with one synchronisation (the energy scaled as eval_terms scales it)
+void lbfgs_egrad_dg(const LbfgsCtx& c, DevBuf& g, const DevBuf& s, double& f, double& dg) {
+    std::vector<Term*> terms;
+    for (auto& t : c.h->terms) terms.push_back(t.get());
+    double* two = c.h->coef.as<double>() + 6;
+    EpilogueArgs ep;
+    ep.kind = EPI_EGRAD;
+    ep.out = g.p;
+    ep.llg.m64 = c.st->s.m64.as<double>();
+    ep.energy_dev = two;
+    eval_on_state(c.st, terms, ep, nullptr);
+    c.h->fevals++;
+    dot_dev(g.as<double>(), s.as<double>(), c.n3, c.red(), two + 1, c.stream);
+    double v[2];
+    MAF_CUDA(cudaMemcpyAsync(v, two, sizeof(v), cudaMemcpyDeviceToHost, c.stream));
+    MAF_CUDA(cudaStreamSynchronize(c.stream));
+    const MeshDims& md = c.st->s.md;
+    f = v[0] * md.dx * md.dy * md.dz;
+    dg = v[1];
+}
+
 // EnergyAndGradient (lbfgs_minimizer.cpp:38-42) of the state's current m
 double lbfgs_egrad(const LbfgsCtx& c, DevBuf& g) {
     std::vector<Term*> terms;
@@ -752,9 +774,9 @@ void cvsrch(const LbfgsCtx& c, const DevBuf& wa, double& f, DevBuf& g, double& s
             stp = stx;
         normalize_combine(S.m64.as<double>(), wa.as<double>(), stp, s.as<double>(), S.md.N(), c.stream);
         c.st->m32_valid = false;
-        f = lbfgs_egrad(c, g);
+        double dg;
+        lbfgs_egrad_dg(c, g, s, f, dg);
         nfev++;
-        const double dg = c.dot(g, s);
         const double ftest1 = finit + stp * dgtest;
         const double ftest2 = finit + eps * std::fabs(finit);
         const double ft = 2 * ftol - 1;
@@ -827,8 +849,8 @@ double lbfgs_minimize(maf_lbfgs_s* h, maf_state_s* st) {
         const int k = (int)std::min(m, iter);
         // the two-loop recursion stays on the device: alpha_i = rho_i (s_i . q) and
         // beta = rho_i (y_i . q) are formed by the kernels that use them, with the
-        // host arithmetic's operations in the same order (rho_i = 1 / (s_i . y_i)
-        // is kept from when the pair was stored: the same value as recomputing it)
+        // reference's operations in its order (rho_i = 1 / (s_i . y_i) is kept from when
+        // the pair was stored: the same value as recomputing it); no host synchronisation
         for (int i = k - 1; i >= 0; --i) {
             const DevBuf& sv = h->sV[order[i]];
             const DevBuf& yv = h->yV[order[i]];

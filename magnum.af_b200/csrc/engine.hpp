@@ -101,6 +101,8 @@ struct EpilogueArgs {
     double* partials = nullptr;    // EPI_EDENS: one double per CTA
     LLGParams llg;
     int edge_exchange = 1;         // EPI_EDENS: exchange energy uses h_withedges
+    double* energy_dev = nullptr;  // EPI_EDENS/EGRAD: leave the summed energy density (before the cell
+                                   // volume) on the device here instead of reading it back
 };
 
 // Optional CUDA-event marks recorded after every pass kernel of a field

@@ -663,9 +663,10 @@ void eval_terms(const std::vector<Term*>& terms, const MeshDims& md, const R* m,
         if (marks) marks->mark(st, "local");
     }
     if (ep.kind == EPI_EDENS || ep.kind == EPI_EGRAD) {
-        double* dst = ep.partials + nblocks;
+        double* dst = ep_in.energy_dev ? ep_in.energy_dev : ep.partials + nblocks;
         k_sum_partials<<<1, 256, 0, st>>>(ep.partials, nblocks, dst);
         MAF_LAUNCH_CHECK();
+        if (ep_in.energy_dev) return;  // the caller reads it back
         double e = 0;
         MAF_CUDA(cudaMemcpyAsync(&e, dst, sizeof(double), cudaMemcpyDeviceToHost, st));
         MAF_CUDA(cudaStreamSynchronize(st));

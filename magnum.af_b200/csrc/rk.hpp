@@ -30,7 +30,8 @@ void axpby(double* out, double a, const double* x, double b, const double* y, in
 // Device-resident steps of the LBFGS two-loop recursion (no host synchronisation):
 // *out = a . b (the same partial sums and order as dot_host), and
 // q = 1 q + c y with c = -(rho *d) (alpha_out: t = rho *d, written by one thread)
-// or c = *alpha_in - rho *d -- the arithmetic of axpby with a host coefficient.
+// or c = *alpha_in - rho *d (the reference's operations; the multiply-add may round
+// differently in the last bit from axpby's).
 void dot_dev(const double* a, const double* b, int64_t n, double* scratch, double* out, cudaStream_t st);
 // reduce_host's mode (0 dot, 1 NaN-propagating max |a|, 2 squared difference) into a device scalar
 void reduce_dev(const double* a, const double* b, int64_t n, int mode, double* scratch, double* out, cudaStream_t st);
