@@ -745,13 +745,15 @@ void cstep(double& stx, double& fx, double& dx, double& sty, double& fy, double&
 }
 
 // cvsrch (lbfgs_minimizer.cpp:213-360): wa = x_old, s = search direction (device)
-void cvsrch(const LbfgsCtx& c, const DevBuf& wa, double& f, DevBuf& g, double& stp, const DevBuf& s, double tolf) {
+// (dginit_known: g . s when the caller has it already, else NaN)
+void cvsrch(const LbfgsCtx& c, const DevBuf& wa, double& f, DevBuf& g, double& stp, const DevBuf& s, double tolf,
+            double dginit_known) {
     int infoc = 1;
     const double xtol = 1e-15, ftol = 1.0e-4, gtol = 0.9, eps = tolf;
     const double stpmin = 1e-15, stpmax = 1e15, xtrapf = 4;
     const int maxfev = 20;
     int nfev = 0;
-    const double dginit = c.dot(g, s);
+    const double dginit = std::isnan(dginit_known) ? c.dot(g, s) : dginit_known;
     if (dginit >= 0.0) return;  // no descent
     bool brackt = false, stage1 = true;
     const double finit = f, dgtest = ftol * dginit;
@@ -874,20 +876,25 @@ double lbfgs_minimize(maf_lbfgs_s* h, maf_state_s* st) {
         // search direction -q (held in s until the step is known)
         axpby(h->s.as<double>(), -1.0, h->q.as<double>(), 0.0, nullptr, n3, S.stream);
         double rate = 1.0;
-        cvsrch(c, h->x_old, f, h->grad, rate, h->s, h->tolerance);
+        // with s = -q exactly (a negation), grad . s = -(grad . q) = phiPrime0 to the bit
+        cvsrch(c, h->x_old, f, h->grad, rate, h->s, h->tolerance,
+               phiPrime0 > 0 ? std::numeric_limits<double>::quiet_NaN() : phiPrime0);
         const double f1 = 1 + std::fabs(f);
-        gradNorm = c.maxabs(h->grad.as<double>());
+        // max|grad|, and ahead of the convergence test the step s = m - x_old with
+        // max|s| and max|m| (unused if the gradient test ends the run): one synchronisation
+        axpby(h->s.as<double>(), 1.0, S.m64.as<double>(), -1.0, h->x_old.as<double>(), n3, S.stream);
+        double mx[3];
+        reduce_dev(h->grad.as<double>(), nullptr, n3, 1, c.red(), trio_d, S.stream);
+        reduce_dev(h->s.as<double>(), nullptr, n3, 1, c.red(), trio_d + 1, S.stream);
+        reduce_dev(S.m64.as<double>(), nullptr, n3, 1, c.red(), trio_d + 2, S.stream);
+        read_back(3, mx);
+        gradNorm = mx[0];
         h->last_gradnorm = gradNorm;
         if (gradNorm < (epsr * f1)) {
             h->iterations = globIter;
             return f;
         }
-        axpby(h->s.as<double>(), 1.0, S.m64.as<double>(), -1.0, h->x_old.as<double>(), n3, S.stream);
-        double mx[2];
-        reduce_dev(h->s.as<double>(), nullptr, n3, 1, c.red(), trio_d, S.stream);
-        reduce_dev(S.m64.as<double>(), nullptr, n3, 1, c.red(), trio_d + 1, S.stream);
-        read_back(2, mx);
-        const double smax = mx[0], mmax = mx[1];
+        const double smax = mx[1], mmax = mx[2];
         if (((f_old - f) < (h->tolerance * f1)) && (smax < (tolf2 * (1 + mmax))) && (gradNorm <= (tolf3 * f1))) break;
         axpby(h->y.as<double>(), 1.0, h->grad.as<double>(), -1.0, h->grad_old.as<double>(), n3, S.stream);
         double d3[3];
