@@ -405,7 +405,7 @@ def heun_ensemble(M, steps, fused_only=False, shapes=None):
     return res
 
 
-def other_configs(M, stream):
+def other_configs(M, stream, film_steps=10000):
     """Simulated ns per hour of wall time on the two other single-mesh
     configurations (short runs, seeded inputs):
     strip   100x25x1 cells of 5x5x3 nm, demag + exchange, Ms 8e5, A 1.3e-11,
@@ -413,7 +413,8 @@ def other_configs(M, stream):
             <m> sampled every 10 ps for 0.2 ns (FP64 form, the configuration's);
     film    512x512x4 cells of 2x2x1 nm, demag + exchange (1.6e-11) + interface DMI
             (3e-3) + uniaxial Ku 1e6 along z, Ms 1.1e6, alpha 0.1, m = +z with 20
-            reversed discs of radius 5-15 cells, RKF45, 200 steps in both forms."""
+            reversed discs of radius 5-15 cells, RKF45, film_steps steps in both forms (10^4, the
+            configuration's run length, by default)."""
     import torch
 
     rng = np.random.default_rng(SEED + 1)
@@ -450,10 +451,12 @@ def other_configs(M, stream):
         torch.cuda.synchronize()
         t_start = st.t
         t0 = time.perf_counter()
-        llg.steps(st, 200)
+        llg.steps(st, film_steps)
+        torch.cuda.synchronize()
         wall = time.perf_counter() - t0
         out["film_512x512x4_" + prec] = {"sim_ns_per_hour": (st.t - t_start) * 1e9 / wall * 3600.0,
-                                         "steps_per_s": 200 / wall, "sim_s": st.t - t_start}
+                                         "steps": film_steps, "steps_per_s": film_steps / wall,
+                                         "sim_s": st.t - t_start}
         del st
     return out
 
@@ -626,7 +629,7 @@ def run_ours(args):
         traj["scheme"] = "DP45 (alpha 0.01, default controller), <m> sampled every %g s" % (TRAJ_T / 10)
 
     # the other single-mesh configurations, short runs: simulated ns per hour
-    cfgs = {} if args.no_trajectory else other_configs(M, stream)
+    cfgs = {} if args.no_trajectory else other_configs(M, stream, args.film_steps)
     if not args.no_trajectory and args.heun_steps > 0:
         cfgs["heun_ensemble_64"] = heun_ensemble(M, args.heun_steps)
         # the same with 64 small members (64 x 64): launch-bound, where one launch per pass pays
@@ -822,7 +825,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default kernel variants")
-    ap.add_argument("--rk-steps", type=int, default=300, help="DP45 steps of the plain step loop per form")
+    ap.add_argument("--rk-steps", type=int, default=1000, help="DP45 steps of the plain step loop per form")
+    ap.add_argument("--film-steps", type=int, default=10000, help="RKF45 steps of the 512x512x4 film per form")
     ap.add_argument("--heun-steps", type=int, default=1000, help="steps of the 64-member Heun ensemble")
     ap.add_argument("--warm-start-samples", type=int, default=16, help="held-out samples of the warm-start gain")
     ap.add_argument("--kernel-sweep", action="store_true",
