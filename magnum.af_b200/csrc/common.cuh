@@ -56,41 +56,6 @@ template <typename C> __host__ __device__ __forceinline__ C cconj(C a) { return 
 template <typename C, typename R> __host__ __device__ __forceinline__ C cscale(C a, R s) {
     return mk(a.x * s, a.y * s);
 }
-// Complex add / subtract of the FFT butterflies: in FP32 device code one packed
-// add.rn.f32x2 / sub.rn.f32x2 (each lane rounded as the scalar operation would be,
-// so the results are the same) instead of two instructions; a build option.
-#ifndef MAF_PACKED_F32
-#define MAF_PACKED_F32 1
-#endif
-template <typename C> __host__ __device__ __forceinline__ C badd(C a, C b) { return cadd(a, b); }
-template <typename C> __host__ __device__ __forceinline__ C bsub(C a, C b) { return csub(a, b); }
-#if MAF_PACKED_F32
-template <> __host__ __device__ __forceinline__ float2 badd<float2>(float2 a, float2 b) {
-#ifdef __CUDA_ARCH__
-    float2 r;
-    asm("{\n\t.reg .b64 pa, pb, pd;\n\tmov.b64 pa, {%2, %3};\n\tmov.b64 pb, {%4, %5};\n\t"
-        "add.rn.f32x2 pd, pa, pb;\n\tmov.b64 {%0, %1}, pd;\n\t}"
-        : "=f"(r.x), "=f"(r.y)
-        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
-    return r;
-#else
-    return cadd(a, b);
-#endif
-}
-template <> __host__ __device__ __forceinline__ float2 bsub<float2>(float2 a, float2 b) {
-#ifdef __CUDA_ARCH__
-    float2 r;
-    asm("{\n\t.reg .b64 pa, pb, pd;\n\tmov.b64 pa, {%2, %3};\n\tmov.b64 pb, {%4, %5};\n\t"
-        "sub.rn.f32x2 pd, pa, pb;\n\tmov.b64 {%0, %1}, pd;\n\t}"
-        : "=f"(r.x), "=f"(r.y)
-        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
-    return r;
-#else
-    return csub(a, b);
-#endif
-}
-#endif
-
 // multiply by -i (forward) or +i (inverse): dir = -1 -> -i, dir = +1 -> +i
 template <int DIR, typename C> __host__ __device__ __forceinline__ C cmul_i(C a) {
     return DIR < 0 ? mk(a.y, -a.x) : mk(-a.y, a.x);

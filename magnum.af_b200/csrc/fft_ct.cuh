@@ -62,9 +62,9 @@ template <int DIR, typename R> __host__ __device__ __forceinline__ void bfly16_h
     for (int n2 = 0; n2 < 4; ++n2) {
         const C p = v[n2], q = v[4 + n2];
         const C iq = cmul_i<DIR>(q);
-        a[n2][0] = badd(p, q);
+        a[n2][0] = cadd(p, q);
         a[n2][1] = cadd(p, iq);
-        a[n2][2] = bsub(p, q);
+        a[n2][2] = csub(p, q);
         a[n2][3] = csub(p, iq);
     }
     const R sd = (R)DIR;

@@ -54,18 +54,18 @@ template <bool BFAST> struct SLay {
 // ---------------------------------------------------------------------------
 template <int DIR, typename C> __host__ __device__ __forceinline__ void bfly2(C& a, C& b) {
     C t = a;
-    a = badd(t, b);
-    b = bsub(t, b);
+    a = cadd(t, b);
+    b = csub(t, b);
 }
 
 template <int DIR, typename C> __host__ __device__ __forceinline__ void bfly4(C* v) {
-    C t0 = badd(v[0], v[2]);
-    C t1 = bsub(v[0], v[2]);
-    C t2 = badd(v[1], v[3]);
-    C t3 = cmul_i<DIR>(bsub(v[1], v[3]));
-    v[0] = badd(t0, t2);
-    v[2] = bsub(t0, t2);
-    v[1] = cadd(t1, t3);  // t3 is a lane swap with a negation: two scalar operations fold it
+    C t0 = cadd(v[0], v[2]);
+    C t1 = csub(v[0], v[2]);
+    C t2 = cadd(v[1], v[3]);
+    C t3 = cmul_i<DIR>(csub(v[1], v[3]));
+    v[0] = cadd(t0, t2);
+    v[2] = csub(t0, t2);
+    v[1] = cadd(t1, t3);
     v[3] = csub(t1, t3);
 }
 
@@ -82,14 +82,14 @@ template <int DIR, typename R> __host__ __device__ __forceinline__ void bfly8(cp
     C o1 = cmul(o[1], w1);
     C o2 = cmul_i<DIR>(o[2]);
     C o3 = cmul(o[3], w3);
-    v[0] = badd(e[0], o[0]);
-    v[4] = bsub(e[0], o[0]);
-    v[1] = badd(e[1], o1);
-    v[5] = bsub(e[1], o1);
+    v[0] = cadd(e[0], o[0]);
+    v[4] = csub(e[0], o[0]);
+    v[1] = cadd(e[1], o1);
+    v[5] = csub(e[1], o1);
     v[2] = cadd(e[2], o2);
     v[6] = csub(e[2], o2);
-    v[3] = badd(e[3], o3);
-    v[7] = bsub(e[3], o3);
+    v[3] = cadd(e[3], o3);
+    v[7] = csub(e[3], o3);
 }
 
 // direct DFT of odd prime size with roots W_R^m = tw[m * L / R]
