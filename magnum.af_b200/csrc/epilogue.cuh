@@ -275,6 +275,19 @@ __device__ __forceinline__ void runN_fields(const TermList& tl, const RunN<R, N>
                 }
                 const R k1 = kF32 ? (R)t.qf[0] : (R)t.q[0], k2 = kF32 ? (R)t.qf[1] : (R)t.q[1];
                 const R k3 = kF32 ? (R)t.qf[2] : (R)t.q[2];
+                if (t.qf[12] != 0.0f) {
+                    // axes x, y, z and K2 = K3 = 0 (flag set on the host): the same values
+                    // without the products by the axes' zeros and ones and the zero terms
+#pragma unroll
+                    for (int i = 0; i < N; ++i) {
+                        const R m0 = r.c[0][i], m1 = r.c[1][i], m2 = r.c[2][i];
+                        const R s1 = m0 * m0, s2 = m1 * m1, s3 = m2 * m2;
+                        h[i][0] += k1 * (s2 + s3) * m0;
+                        h[i][1] += k1 * (s1 + s3) * m1;
+                        h[i][2] += k1 * (s1 + s2) * m2;
+                    }
+                    break;
+                }
 #pragma unroll
                 for (int i = 0; i < N; ++i) {
                     const R m0 = r.c[0][i], m1 = r.c[1][i], m2 = r.c[2][i];
@@ -433,10 +446,16 @@ inline void prepare_run4(TermList& tl, const Geom& g, double Ms) {
                 t.qf[0] = f(t.q[0]);
                 for (int k = 0; k < 3; ++k) t.qf[1 + k] = f(t.p[1 + k]);
                 break;
-            case TK_CUBIC:
+            case TK_CUBIC: {
                 for (int k = 0; k < 3; ++k) t.qf[k] = f(t.q[k]);
                 for (int k = 3; k < 12; ++k) t.qf[k] = f(t.p[k]);
+                // axes exactly x, y, z and only K1: the epilogue's short form
+                const double id[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+                bool fast = t.p[1] == 0.0 && t.p[2] == 0.0;
+                for (int k = 0; k < 9; ++k) fast = fast && t.p[3 + k] == id[k];
+                t.qf[12] = fast ? 1.0f : 0.0f;
                 break;
+            }
             case TK_ZEEMAN:
                 for (int k = 0; k < 3; ++k) t.qf[k] = f(t.p[k]);
                 break;
