@@ -36,14 +36,15 @@ def test_variants_agree_and_autotune_picks_valid(precision, tol, shape):
 
 @pytest.mark.parametrize("shape", [(64, 256, 4), (32, 1024, 2)])
 def test_full_search_variants_agree_and_cache(shape):
-    """Every radix sequence / pipelining / tile choice of the y passes gives the
-    field of the defaults to rounding, and the full search is cached per shape."""
+    """Every radix sequence (both y passes, or only one of them) / pipelining / tile
+    choice gives the field of the defaults to rounding, and the full search is
+    cached per shape."""
     mesh = M.Mesh(*shape, 3e-9, 3e-9, 3e-9)
     d = M.DemagField(mesh)
     llg = M.LLGIntegrator(0.01, [d, M.ExchangeField(1.3e-11)])
     s = M.State(mesh, 8.6e5, random_m(shape, 4), precision="fp32_field")
     H0 = np.asarray(llg.H_in_Apm_f32(s), dtype=np.float64)
-    for choice in [(0, 1, 2, 1, 1), (1, 1, 2, 0, 1), (0, 0, 4, 0, 0), (1, 0, 2, 1, 1)]:
+    for choice in [(0, 1, 2, 1, 1), (1, 1, 2, 0, 1), (0, 0, 4, 0, 0), (1, 0, 2, 1, 1), (0, 1, 2, 1, 2), (1, 0, 4, 0, 3)]:
         d.tune_ex = choice
         assert d.tune_ex == choice
         H = np.asarray(llg.H_in_Apm_f32(s), dtype=np.float64)
@@ -55,3 +56,5 @@ def test_full_search_variants_agree_and_cache(shape):
     llg2 = M.LLGIntegrator(0.01, [d2, M.ExchangeField(1.3e-11)])
     res2 = llg2.autotune_ex(s, reps=2)
     assert res2["cached"] and d2.tune_ex == d.tune_ex
+    with pytest.raises(M.MafError):
+        d.tune_ex = (0, 1, 2, 1, 4)  # cols_plan is 0..3
