@@ -27,9 +27,13 @@ constexpr int kMinBlocks = (sizeof(R) == 4 ? T32 : T64) / NT > 1 ? (sizeof(R) ==
 constexpr int kRunCells = MAF_RUN_CELLS;
 static_assert(kRunCells == 2 || kRunCells == 4, "run length");
 // resident threads per SM the x-inverse kernels are compiled for (register caps; build options):
-// FP64 two 192-thread CTAs (168 registers, no spill), FP32 576 threads
+// FP64 two 192-thread CTAs (168 registers, no spill); FP32 four 192-thread CTAs (80 registers:
+// the power-of-two lengths up to 1024) and 576 threads for the other CTA sizes
 #ifndef MAF_XINV_THREADS_F64
 #define MAF_XINV_THREADS_F64 384
+#endif
+#ifndef MAF_XINV_THREADS_192
+#define MAF_XINV_THREADS_192 768
 #endif
 #ifndef MAF_XINV_THREADS
 #define MAF_XINV_THREADS 576
@@ -640,7 +644,7 @@ __device__ __forceinline__ void xinv_ct_tile(const cplx_t<R>* __restrict__ S1, i
 }
 
 template <typename R, int EPI, int LC, int NBR, int NT, int RN>
-__global__ void __launch_bounds__(NT, (kMinBlocks<R, NT, (RN == 2 ? MAF_XINV_THREADS : 384), MAF_XINV_THREADS_F64>)) k_xinv_ct(const cplx_t<R>* __restrict__ S1, int pitch,
+__global__ void __launch_bounds__(NT, (kMinBlocks<R, NT, (RN == 2 ? (NT == 192 ? MAF_XINV_THREADS_192 : MAF_XINV_THREADS) : 384), MAF_XINV_THREADS_F64>)) k_xinv_ct(const cplx_t<R>* __restrict__ S1, int pitch,
                                                 const cplx_t<R>* __restrict__ tw, const cplx_t<R>* __restrict__ twP,
                                                 Geom g, R scale, const R* __restrict__ m, MsInfo ms, TermList tl,
                                                 EpilogueArgs ep, int run4) {
@@ -667,7 +671,7 @@ __global__ void __launch_bounds__(NT) kbt_convy(const CtConvyItem<R>* __restrict
 }
 
 template <typename R, int LC, int NBR, int NT, int RN>
-__global__ void __launch_bounds__(NT, (kMinBlocks<R, NT, (RN == 2 ? MAF_XINV_THREADS : 384), MAF_XINV_THREADS_F64>))
+__global__ void __launch_bounds__(NT, (kMinBlocks<R, NT, (RN == 2 ? (NT == 192 ? MAF_XINV_THREADS_192 : MAF_XINV_THREADS) : 384), MAF_XINV_THREADS_F64>))
     kbt_xinv(const CtXinvItem<R>* __restrict__ items, const int2* __restrict__ work, const cplx_t<R>* __restrict__ tw,
              const cplx_t<R>* __restrict__ twP) {
     const int2 w = work[blockIdx.x];
