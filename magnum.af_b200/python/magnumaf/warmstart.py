@@ -5,7 +5,7 @@ own CUDA kernels) maps an initial magnetisation and the material/field
 parameters to a proposal for the relaxed state; LBFGS then finishes from the
 proposal.  Plain LBFGS from the user's initial state stays both the fallback
 (a proposal with non-finite values or a higher energy than the initial state
-is discarded) and the judge: the minimiser's own stopping criteria decide when
+is discarded) and the arbiter: the minimiser's own stopping criteria decide when
 a state is relaxed, and the final energy and residual torque max|m x H|/Ms are
 reported for both starts.
 

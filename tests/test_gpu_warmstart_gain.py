@@ -1,5 +1,5 @@
 """What the trained warm start gains over plain LBFGS (the reference's
-LBFGS_Minimizer, lbfgs_minimizer.cpp:55-198, is both fallback and judge): the
+LBFGS_Minimizer, lbfgs_minimizer.cpp:55-198, is both fallback and arbiter): the
 pretrained U-net (magnumaf/data/warmstart_unet_128.npz, trained by the
 library's own tensor-core kernels on GPU-LBFGS relaxations) proposes relaxed
 states for held-out 128 x 128 samples of the configuration (seeds never used in
