@@ -549,7 +549,7 @@ __device__ __forceinline__ void convy_ct_tile(cplx_t<R>* S, const R* __restrict_
 }
 
 template <typename R, int L, int NB, int NT>
-__global__ void __launch_bounds__(NT, (sizeof(R) == 4 && NT == 384) ? 2 : 1) k_convy_ct(cplx_t<R>* S, const R* __restrict__ Nred, int ny, int nxh, int pitch,
+__global__ void __launch_bounds__(NT) k_convy_ct(cplx_t<R>* S, const R* __restrict__ Nred, int ny, int nxh, int pitch,
                                                  const cplx_t<R>* __restrict__ tw) {
     convy_ct_tile<R, L, NB, NT>(S, Nred, ny, nxh, pitch, tw, blockIdx.x);
 }
@@ -663,7 +663,7 @@ __global__ void __launch_bounds__(NT) kbt_xfwd(const CtXfwdItem<R>* __restrict__
 }
 
 template <typename R, int L, int NB, int NT>
-__global__ void __launch_bounds__(NT, (sizeof(R) == 4 && NT == 384) ? 2 : 1) kbt_convy(const CtConvyItem<R>* __restrict__ items, const int2* __restrict__ work,
+__global__ void __launch_bounds__(NT) kbt_convy(const CtConvyItem<R>* __restrict__ items, const int2* __restrict__ work,
                                                 const cplx_t<R>* __restrict__ tw) {
     const int2 w = work[blockIdx.x];
     const CtConvyItem<R> d = items[w.x];
