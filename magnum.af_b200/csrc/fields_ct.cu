@@ -802,8 +802,10 @@ static void convz_L(cplx_t<R>* S, const R* Nred, int nz, int ny, int nxh, int pi
     static_assert(NT <= kMaxFftThreads, "CTA size");
     const size_t smem = sizeof(cplx_t<R>) * (size_t)6 * NB * ((L - 1) + ((L - 1) >> 4) + 1);
     if constexpr (L <= 32 && REG) {
-        // transforms in registers: one thread per column, NB columns of kx
-        constexpr int NBR = sizeof(R) == 4 ? 32 : 16;
+        // transforms in registers: one thread per column, 16 columns of kx per CTA
+        // (96 threads; at nz = 16 in FP32, 96 registers and 31 KB of shared memory:
+        // seven CTAs per SM, where 32-column CTAs fit three)
+        constexpr int NBR = 16;
         // spectra [L][6 NBR] plus the tensor slice [6][L/2 + 1][NBR]
         constexpr size_t smem_r = sizeof(cplx_t<R>) * (size_t)L * 6 * NBR + sizeof(R) * (size_t)6 * (L / 2 + 1) * NBR;
         auto kr = k_convz_reg<R, L / 2, NBR>;
