@@ -130,10 +130,15 @@ __global__ void __launch_bounds__(NT) k_xfwd_ct(const R* __restrict__ in, int n_
 // while the current tile's transform runs (issued right after the first stage,
 // the staging buffer's only reader).  For a scalar Ms, n_in <= LC (zero-padded
 // half pruned) and rows of whole 16-byte chunks; the same arithmetic as k_xfwd_ct.
+// CTAs per SM the kernel is compiled for: 1024 (FP32) / 512 (FP64) resident threads for
+// power-of-two lengths, 576 / 288 for three times a power of two, whose radix-3 stage
+// holds more values per thread
+template <typename R, int NT>
+constexpr int kXfwdPipeBlocks = ((sizeof(R) == 4 ? (NT % 3 == 0 ? 576 : 1024) : (NT % 3 == 0 ? 288 : 512)) / NT > 1)
+                                    ? (sizeof(R) == 4 ? (NT % 3 == 0 ? 576 : 1024) : (NT % 3 == 0 ? 288 : 512)) / NT
+                                    : 1;
 template <typename R, int LC, int NB, int NT>
-// (four 256-thread CTAs per SM for power-of-two lengths; three 192-thread CTAs for
-// three times a power of two, whose radix-3 stage holds more values per thread)
-__global__ void __launch_bounds__(NT, (NT % 3 == 0 ? 3 : 4)) k_xfwd_pipe(const R* __restrict__ in, int n_in, int64_t rows, R ms,
+__global__ void __launch_bounds__(NT, (kXfwdPipeBlocks<R, NT>)) k_xfwd_pipe(const R* __restrict__ in, int n_in, int64_t rows, R ms,
                                                   cplx_t<R>* __restrict__ out, int pitch,
                                                   const cplx_t<R>* __restrict__ tw,
                                                   const cplx_t<R>* __restrict__ twP) {
@@ -688,6 +693,11 @@ template <typename K> static void ct_smem(K kernel, size_t bytes) {
 // tile widths: about 4096 (FP32) / 2048 (FP64) complex values per CTA for the
 // x passes, 8192 / 4096 for the column passes (a 32-byte row segment at least)
 template <typename R> constexpr int kTileX = sizeof(R) == 4 ? 4096 : 2048;
+// the pipelined x forward: about 1024 values per tile (one row at length 1024, so
+// 64-thread CTAs, sixteen per SM in FP32): the small CTAs keep more tiles in different
+// phases per SM than 4-row tiles at the same resident warps (0.172 -> 0.158 ms FP32,
+// 0.348 -> 0.338 ms FP64 at 1024x1024x16)
+template <typename R> constexpr int kTileXP = 1024;
 template <typename R> constexpr int kTileC = sizeof(R) == 4 ? 8192 : 4096;
 // complex values per CTA tile of the y passes (columns x length); a build option
 #ifndef MAF_COLS_TILE_F32
@@ -729,6 +739,8 @@ static void xfwd_L(const R* in, int n_in, int64_t rows, int64_t rows_pc, const R
     const size_t smem = sizeof(cplx_t<R>) * (size_t)NB * SB;
     if constexpr (HIN) {
         // the pipelined persistent kernel: scalar Ms, rows of whole 16-byte chunks
+        constexpr int NB = pow2floor(cmax(1, kTileXP<R> / LC));
+        constexpr int NT = LC * NB / kE;
         constexpr int E16 = 16 / (int)sizeof(R);
         if (!msf && n_in % E16 == 0 && (uintptr_t)in % 16 == 0) {
             auto kp = k_xfwd_pipe<R, LC, NB, NT>;
